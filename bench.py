@@ -1,0 +1,342 @@
+"""Benchmark: PFC Misfit time steps per second at 1024^2, FP32 fused path, batched.
+
+Workload (one GPU): B Misfit runs of 1024 x 1024 x 1 (the single-run GPU
+configuration: FP32 complex FFT path with the FP64 k = 0 mode), seeds 1000+i,
+u0/con0 = reference defaults, advanced together.  One "step" advances every run
+of the batch by one time step; `value` is run-steps per second over all GPUs.
+The batch's resident state (B x ~26 MB of row-space arrays) is larger than the
+126 MB L2, so timed steps stream from HBM.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl ours|reference]
+
+N > 1 runs one process per GPU under torchrun (weak scaling: each rank owns its
+own batch, no data-path collective; timing is the max over ranks).
+`--impl reference` times the reference program's own CPU implementation of the
+step (the unmodified sources compiled by oracle/Makefile) on this host's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import glob
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "pfc-exp-gui_b200"))
+
+GRID = 1024
+METRIC = "PFC Misfit steps/s at 1024^2 (FP32 fused step, batched; run-steps/s)"
+UNIT = "steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--grid", type=int, default=GRID)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (torch.distributed over NCCL: barrier and max-over-ranks)
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self, n):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            import torch
+            t = torch.zeros(1, device=f"cuda:{self.local}")
+            self.pg.all_reduce(t)
+            torch.cuda.synchronize()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
+        self.pg.all_reduce(t)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        j = json.load(open(p))
+        return float(j["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(grid, batch):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, scaled to this batch."""
+    p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if not os.path.exists(p):
+        return None
+    j = json.load(open(p))
+    per_run = j.get("col_kernel_dram_bytes_per_run", {}).get(str(grid))
+    return None if per_run is None else per_run * batch
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference program (or the oracle port) on this host's cores
+# ---------------------------------------------------------------------------
+def ref_binary(grid):
+    p = os.path.join(ROOT, "oracle", "_ref", f"pfc-exp-cli-{grid}x{grid}x1")
+    return p if os.path.exists(p) else None
+
+
+def time_reference_process(exe, steps, outdir):
+    t0 = time.perf_counter()
+    subprocess.run([exe, "--model", "misfit", "--steps", str(steps), "--mod", str(steps), "--outdir", outdir],
+                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, check=True)
+    return time.perf_counter() - t0
+
+
+def cpu_steps_per_s(grid, nproc, extra_steps):
+    """Per-step throughput of `nproc` concurrent single-threaded reference processes.
+
+    Each process runs once with 1 step and once with 1+extra_steps steps (same init
+    and the same single checkpoint), so the difference is exactly extra_steps steps."""
+    import tempfile
+    exe = ref_binary(grid)
+    kind = "reference"
+    if exe is None:
+        kind = "port"
+    with tempfile.TemporaryDirectory() as tmp:
+        def phase(steps):
+            if exe is not None:
+                procs = []
+                t0 = time.perf_counter()
+                for i in range(nproc):
+                    procs.append(subprocess.Popen([exe, "--model", "misfit", "--steps", str(steps), "--mod",
+                                                   str(steps), "--outdir", os.path.join(tmp, f"r{i}_{steps}")],
+                                                  stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
+                for p in procs:
+                    p.wait()
+                return time.perf_counter() - t0
+            # oracle port (bit-identical restatement of the reference step), one process per core
+            code = ("import sys; sys.path.insert(0, %r); import oracle as O; "
+                    "r = O.Run(O.default_params(0, L=%d, M=%d)); r.step(%d)") % (os.path.join(ROOT, "oracle"), grid,
+                                                                                 grid, steps)
+            t0 = time.perf_counter()
+            procs = [subprocess.Popen([sys.executable, "-c", code]) for _ in range(nproc)]
+            for p in procs:
+                p.wait()
+            return time.perf_counter() - t0
+        ta = phase(1)
+        tb = phase(1 + extra_steps)
+    dt = max(tb - ta, 1e-9)
+    return nproc * extra_steps / dt, kind
+
+
+def cpu_baseline(grid):
+    v, kind = cpu_steps_per_s(grid, 1, 2)
+    what = "reference pfc-exp-cli built from its sources" if kind == "reference" else "oracle port of the reference step"
+    return {"value": round(v, 4), "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"2 Misfit {grid}^2 FP64 steps of one run ({what}; FFTW unavailable, "
+                      "project FFTW-API shim FFT), 1 core; time(1+2 steps) - time(1 step)"}
+
+
+def run_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    nproc = os.cpu_count() or 1
+    v, kind = cpu_steps_per_s(args.grid, nproc, 2)
+    sample = (f"each step: {nproc} concurrent single-threaded processes x 2 Misfit {args.grid}^2 FP64 steps "
+              f"({'reference pfc-exp-cli built from its sources' if kind == 'reference' else 'oracle port'}; "
+              "FFTW unavailable, project FFTW-API shim FFT)")
+    line = {"metric": METRIC, "value": round(v, 4), "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000.0 / v, 3) if v else None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"Misfit {args.grid}x{args.grid}x1, reference CPU step (seed 20200604, "
+                                   "u0 0.05, con0 0.2)", "grid": [args.grid, args.grid, 1]},
+            "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": nproc, "kind": kind, "sample": sample},
+            "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    dist = Dist(args.gpus)
+    import numpy as np
+    import pfc_b200 as P
+    dev = dist.local
+    G, B = args.grid, args.batch
+    runs = []
+    for i in range(B):
+        p = P.default_params(P.MODEL_MISFIT, L=G, M=G, N=1, seed=1000 + i + 100000 * dist.rank, device=dev)
+        runs.append(P.Run(p))
+    batch = P.Batch(runs)
+    batch.advance(max(3, args.warmup))
+    dist.barrier()
+    clocks = Clocks(dev)
+    clocks.start()
+    ms = batch.advance_timed(args.steps)
+    clk = clocks.stop()
+    ms_max = dist.max(ms)
+    total_run_steps = dist.sum(B * args.steps)
+    value = total_run_steps / (ms_max / 1000.0)
+
+    # per-kernel roofline (dominant kernel), timed with events on the library stream
+    row_ms, col_ms = batch.kernel_times(20)
+    H1 = G // 2 + 1
+    bytes_row = B * G * H1 * 8 * 6   # 4 row-space arrays read, 2 written
+    bytes_col = B * G * H1 * 8 * 8   # 4 read, 4 written
+    if col_ms >= row_ms:
+        dom, dom_ms, dom_bytes = "k_col_step", col_ms, bytes_col
+    else:
+        dom, dom_ms, dom_bytes = "k_row_step", row_ms, bytes_row
+    peak, peak_kind = measured_peak()
+    achieved = dom_bytes / (dom_ms / 1000.0) / 1e9
+    traffic = profiled_traffic(G, B) if dom == "k_col_step" else None
+
+    # end to end through the public API: host initial fields in, B runs x K steps, host fields out
+    phi0, con0 = runs[0].fields()
+    host_phi = [np.ascontiguousarray(phi0) for _ in range(B)]
+    host_con = [np.ascontiguousarray(con0) for _ in range(B)]
+    dist.barrier()
+    t0 = time.perf_counter()
+    for r, a, c in zip(runs, host_phi, host_con):
+        r.set_fields(a, c)
+    batch.advance(args.steps)
+    outs = [r.fields_f32() for r in runs]
+    e2e_s = time.perf_counter() - t0
+    e2e_s = dist.max(e2e_s)
+    e2e_value = total_run_steps / e2e_s
+    P_pts = G * G
+    h2d = B * P_pts * 16 / args.steps
+    d2h = B * P_pts * 8 / args.steps
+    del outs
+
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": round(ms_max / args.steps, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 k=0 mode, FP64 denominators)",
+        "data": "synthetic (reference INITIAL_dis seeded polycrystal, seeds 1000+i)",
+        "config": {"workload": f"Misfit {G}x{G}x1 FP32 fused step, {B} runs per GPU advanced together "
+                               "(graph-captured row/column sweeps)",
+                   "grid": [G, G, 1], "runs_per_gpu": B, "parallelism": f"replicas x{dist.world}",
+                   "l2": "inputs larger than L2 (resident state ~26 MB/run x batch)"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes,
+                     "launch_ms": round(dom_ms, 5), "row_ms": round(row_ms, 5), "col_ms": round(col_ms, 5)},
+        "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h),
+                "what": "pfc_run_set_fields (host FP64 fields) + pfc_batch_advance(K) + pfc_run_get_fields_f32"},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk,
+    }
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(G)
+        except Exception as e:  # noqa: BLE001
+            line["cpu_baseline"] = {"value": None, "error": str(e)}
+    batch.close()
+    for r in runs:
+        r.close()
+    if dist.rank == 0:
+        print(json.dumps(line), flush=True)
+    dist.close()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,147 @@
+/*
+ * pfc_b200.h -- C ABI of libpfc_b200.so, the B200 (sm_100a) engine for the
+ * pfc-exp-cli hot path of zhiqing0205/PFC-Exp-GUI.
+ *
+ * Plain C types only: pointers, sizes and status codes.  Every function returns
+ * PFC_OK (0) on success or a negative PFC_E_* code, and pfc_last_error() then
+ * describes the failure (thread-local).  Nothing here calls exit().
+ *
+ * Reference interfaces replaced (paths within zhiqing0205/PFC-Exp-GUI):
+ *   src/experiment/main_cli.cpp:24-88          main() / --model dispatch
+ *   src/experiment/pfc_common.h:348-350        int run_misfit/run_cvd/run_elastic(int, char**)
+ *   src/experiment/misfit_uniform_time_seed_fftw_early.cpp:464-501   INITIAL_dis + one time step
+ *   src/experiment/cvd.cpp:377-422             INITIAL_C2 + one time step
+ *   src/experiment/misfit_uniform_time_seed_fftw_early.cpp:1043-1092 ENERGYC2
+ *   src/experiment/misfit_uniform_time_seed_fftw_early.cpp:3261-3556 phimax_atmposi (Misfit)
+ *   src/experiment/elastic.cpp:2802-2921       phimax_atmposi (Elastic)
+ *   src/experiment/elastic.cpp:3586-3729       elastic3D
+ *   src/experiment/elastic.cpp:3013-3319       cryst_order
+ *   src/experiment/misfit_uniform_time_seed_fftw_early.cpp:438-452   fftw_plan_dft_3d / fftw_execute
+ */
+#ifndef PFC_B200_H
+#define PFC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PFC_OK 0
+#define PFC_E_INVALID (-1)   /* bad argument or unsupported size */
+#define PFC_E_CUDA (-2)      /* CUDA runtime error */
+#define PFC_E_NOMEM (-3)     /* device or host allocation failed */
+#define PFC_E_IO (-4)        /* file read/write failure */
+#define PFC_E_STATE (-5)     /* call not valid in the object's current state */
+
+#define PFC_MODEL_MISFIT 0
+#define PFC_MODEL_CVD 1
+
+#define PFC_PRECISION_FP32 0 /* fused FP32 path, FP64 k=0 mode and reductions */
+#define PFC_PRECISION_FP64 1 /* plain FP64 path with the reference's float roundings */
+#define PFC_PRECISION_FP64_PURE 2 /* plain FP64 path, every intermediate in double */
+
+/* Parameters of one run.  Field meanings and defaults follow the reference CLI
+ * (misfit_uniform_time_seed_fftw_early.cpp:17-35, 125-143; cvd.cpp:111-125, 33-53). */
+typedef struct pfc_run_params {
+    int model;      /* PFC_MODEL_MISFIT or PFC_MODEL_CVD */
+    int L, M, N;    /* grid; L, M powers of two in [32, 2048]; N = 1 (2-D) */
+    float u0, con0, sig, dt, dx, axx;
+    int grainx, grainy, grainz; /* Misfit initial grains */
+    uint32_t seed;
+    int precision;  /* PFC_PRECISION_FP32 or PFC_PRECISION_FP64 */
+    int device;     /* CUDA device ordinal */
+} pfc_run_params;
+
+typedef struct pfc_run pfc_run;
+typedef struct pfc_batch pfc_batch;
+
+/* Last error message of the calling thread ("" if none). */
+const char *pfc_last_error(void);
+
+/* Fill *p with the reference defaults of `model` (grid 256 x 256 x 1, FP32). */
+int pfc_default_params(int model, pfc_run_params *p);
+
+/* Allocate a run on the device and set its initial condition (INITIAL_dis for
+ * Misfit, MIS:610-682; INITIAL_C2 for CVD, CVD:587-642). */
+int pfc_run_create(const pfc_run_params *p, pfc_run **out);
+int pfc_run_destroy(pfc_run *r);
+
+/* Advance nsteps time steps (MIS:475-501 / CVD:389-422).  With analysis != 0 the
+ * last step also prepares the checkpoint analysis (real fields, energy, mass). */
+int pfc_run_advance(pfc_run *r, int nsteps, int analysis);
+
+/* Steps taken so far. */
+int pfc_run_steps(const pfc_run *r, int *steps);
+
+/* Real fields of the current state in the reference layout n + N*(m + M*l)
+ * (double, P = L*M*N each); either pointer may be NULL. */
+int pfc_run_get_fields(pfc_run *r, double *phi, double *con);
+/* Same, as the FP32 values the checkpoint writer stores. */
+int pfc_run_get_fields_f32(pfc_run *r, float *phi, float *con);
+/* Replace the state with the given real fields (double, reference layout). */
+int pfc_run_set_fields(pfc_run *r, const double *phi, const double *con);
+
+/* ENERGYC2 of the current state: sum(e)/L/M/N and sum(phi)/L/M/N as written to
+ * energy.txt (MIS:1081-1085).  Valid after pfc_run_advance(..., analysis=1). */
+int pfc_run_energy(pfc_run *r, double *e_over_p, double *mass_over_p);
+
+/* FP64 k = 0 modes of phi and con divided by P (the conserved means). */
+int pfc_run_means(const pfc_run *r, double *phi_mean, double *con_mean);
+
+/* Batched execution: runs of any of the supported grid sizes advanced together
+ * (one launch per size class per sweep).  Runs must be FP32 and on one device;
+ * the batch does not own them. */
+int pfc_batch_create(pfc_run *const *runs, int nruns, pfc_batch **out);
+int pfc_batch_destroy(pfc_batch *b);
+/* Advance every run of the batch by nsteps (captured once into a CUDA graph). */
+int pfc_batch_advance(pfc_batch *b, int nsteps);
+
+/* Same as pfc_batch_advance, bracketed by CUDA events on the batch's stream;
+ * *ms receives the device time of the nsteps.  (Measurement hook; no reference
+ * counterpart.) */
+int pfc_batch_advance_timed(pfc_batch *b, int nsteps, float *ms);
+
+/* Advance reps steps with each sweep's kernels launched individually and timed
+ * with CUDA events; *row_ms and *col_ms receive the mean device time of the row
+ * and column kernel launches of one step.  (Measurement hook; no reference
+ * counterpart.) */
+int pfc_batch_kernel_times(pfc_batch *b, int reps, double *row_ms, double *col_ms);
+
+/* Misfit peak finder (MIS:3261-3556) on a 2-D field (N = 1, layout m + M*l).
+ * Writes up to cap atoms as 5 doubles (x, y, z, phimax, con) in the reference's
+ * emission order; *count receives the number of atoms (the global-maximum
+ * fallback counts as one). */
+int pfc_phimax_misfit(const float *phi, const float *con, int L, int M, float dx, float con0, double *out5, int cap,
+                      int *count);
+
+/* Elastic peak finder (ELA:2802-2921) on a field read from a VTI (layout
+ * n + N*(m + M*l)); writes up to cap atoms as 4 doubles (x, y, z, phimax). */
+int pfc_phimax_elastic(const float *phi, int L, int M, int N, float dx, double *out4, int cap, int *count);
+
+/* elastic3D (ELA:3586-3729): per-atom strain magnitude and neighbour count
+ * (0.7 < r < benchel, first 16 neighbours in ascending index contribute). */
+int pfc_elastic3d(const double *x, const double *y, const double *z, int n, int L, int M, int N, float dx,
+                  float benchel, double *strain, uint32_t *nb);
+
+/* cryst_order (ELA:3013-3319): per-atom q4 and q6 as written to q4q6_<kd>.txt. */
+int pfc_cryst_order(const double *x, const double *y, const double *z, int n, int L, int M, int N, float dx,
+                    double *q4, double *q6);
+
+/* 3-D complex-double DFT with FFTW's conventions (row-major, n2 fastest,
+ * sign -1 = forward exp(-2 pi i jk/n), +1 = backward, unnormalised): the transform
+ * the reference obtains from fftw_plan_dft_3d + fftw_execute (MIS:438-452).
+ * in/out: host arrays of n0*n1*n2 interleaved (re, im) doubles. */
+int pfc_dft3d(const double *in, double *out, int n0, int n1, int n2, int sign);
+
+/* The pfc-exp-cli process interface (main_cli.cpp:24-88): same flags, files,
+ * progress lines and exit codes, plus the additive --grid LxMxN and
+ * --precision fp32|fp64 options.  Returns the process exit code. */
+int pfc_run_cli(int argc, char **argv);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,751 @@
+// engine.cu -- run objects, batching and the C ABI of libpfc_b200.so.
+//
+// Host-side restatement of the reference's setup (model constants, k-vectors,
+// correlation-kernel parameters, grain seeding) feeding the device kernels.
+// Reference: src/experiment/misfit_uniform_time_seed_fftw_early.cpp:116-179 (constants,
+// RecomputeDerivedParams), :455-466 (k-vectors, INITIAL_dis, C2AK/C2BK), and
+// src/experiment/cvd.cpp:26-53, 351-377.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "pfc_b200.h"
+#include "pfc_engine.h"
+#include "pfc_internal.h"
+
+namespace pfc {
+
+cudaError_t launch_init_misfit(float *psi, float *con, int L, int M, int N, float u0, float con0, float dx,
+                               const void *grains, int ngrains, double limx, double limy, const float *costab,
+                               int xmin, int ntab, float A1x2, float A2x4, cudaStream_t s);
+cudaError_t launch_init_cvd(float *psi, float *con, int L, int M, int N, float u0, float con0, const float *tab,
+                            float A1x2, float A2x4, cudaStream_t s);
+cudaError_t launch_sum_f32(const float *a, long n, double *scratch, int blocks, double *out, cudaStream_t s);
+cudaError_t launch_reduce_fixed(const double *partials, int count, int stride, int width, double *out,
+                                cudaStream_t s);
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_error(cudaError_t e, const char *what) {
+    return set_error(PFC_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define PFC_CUDA_TRY(expr)                                   \
+    do {                                                     \
+        cudaError_t _e = (expr);                             \
+        if (_e != cudaSuccess) return cuda_error(_e, #expr); \
+    } while (0)
+
+static constexpr double PI_REF = 3.1415926;  // pfc_common.h:152
+
+// ---------------------------------------------------------------------------
+// Per-device context: stream and twiddle tables.
+// ---------------------------------------------------------------------------
+static std::mutex g_ctx_mu;
+static std::map<int, Context *> g_ctx;
+
+int get_context(int device, Context **out) {
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    auto it = g_ctx.find(device);
+    if (it != g_ctx.end()) {
+        *out = it->second;
+        return PFC_OK;
+    }
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return set_error(PFC_E_CUDA, std::string("no CUDA device available: ") + cudaGetErrorString(e));
+    if (device < 0 || device >= ndev) return set_error(PFC_E_INVALID, "device ordinal out of range");
+    PFC_CUDA_TRY(cudaSetDevice(device));
+    Context *c = new Context();
+    c->device = device;
+    PFC_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    // twiddles: for n = 2^1 .. 2^11, exp(-2 pi i j / n), j < n, in double, rounded once for FP32
+    size_t total = 0;
+    for (int lg = 1; lg <= 11; ++lg) total += (size_t)1 << lg;
+    std::vector<double2> h64(total);
+    std::vector<float2> h32(total);
+    size_t off = 0;
+    for (int lg = 1; lg <= 11; ++lg) {
+        const int n = 1 << lg;
+        for (int j = 0; j < n; ++j) {
+            const double a = 2.0 * M_PI * (double)j / (double)n;
+            h64[off + j] = make_double2(std::cos(a), -std::sin(a));
+            h32[off + j] = make_float2((float)std::cos(a), (float)-std::sin(a));
+        }
+        off += n;
+    }
+    char *mem = nullptr;
+    PFC_CUDA_TRY(cudaMalloc(&mem, total * (sizeof(double2) + sizeof(float2))));
+    PFC_CUDA_TRY(cudaMemcpy(mem, h64.data(), total * sizeof(double2), cudaMemcpyHostToDevice));
+    PFC_CUDA_TRY(cudaMemcpy(mem + total * sizeof(double2), h32.data(), total * sizeof(float2), cudaMemcpyHostToDevice));
+    c->tw_mem = mem;
+    off = 0;
+    for (int lg = 1; lg <= 11; ++lg) {
+        c->tw.f64[lg] = reinterpret_cast<const double2 *>(mem) + off;
+        c->tw.f32[lg] = reinterpret_cast<const float2 *>(mem + total * sizeof(double2)) + off;
+        off += (size_t)1 << lg;
+    }
+    c->tw.f64[0] = c->tw.f64[1];
+    c->tw.f32[0] = c->tw.f32[1];
+    g_ctx[device] = c;
+    *out = c;
+    return PFC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Model constants (MIS:116-143, CVD:26-53) and derived parameters.
+// ---------------------------------------------------------------------------
+void model_coefs(int model, ModelCoefs *k) {
+    const float a_lattice = 1.0f;
+    k->gaa1 = 0.8f;
+    k->gaa2 = (float)(k->gaa1 * std::sqrt(2.));
+    k->gab1 = 0.8f;
+    k->gab2 = (float)(k->gaa2 * std::sqrt(2.));
+    k->niu = 1.4f;
+    k->ksi = 1.f;
+    k->ka0 = (float)(2.0 * PI_REF / a_lattice);
+    k->ka1 = (float)(2.0 * PI_REF);
+    k->ka2 = (float)(std::sqrt(2.0) * k->ka1);
+    k->sigMa1 = k->sigMa2 = k->sigMb1 = k->sigMb2 = 0.55f;
+    k->para_c0 = 0.5f;
+    k->para_alpha = 0.5f;
+    k->para_w = 0.02f;
+    if (model == MODEL_CVD) {
+        const float b_lattice = (float)(std::sqrt(3.0) / 2.0);
+        k->kb0 = (float)(2.5 * PI_REF / b_lattice);
+        k->kb1 = (float)(5.0 * PI_REF / std::sqrt(3.0));
+        k->kb2 = (float)(k->kb1 * std::sqrt(2.0));
+        k->dynamic_mn = 1.f;
+        k->dynamic_mc = 1.f;
+    } else {
+        const float b_lattice = 0.88f;
+        k->kb0 = (float)(2.0 * PI_REF / b_lattice);
+        k->kb1 = k->kb0;
+        k->kb2 = (float)(k->kb1 * std::sqrt(2.0));
+        k->dynamic_mn = 0.1f;
+        k->dynamic_mc = 10.f;
+    }
+}
+
+// Crossover |k| of the two Gaussian peaks, float arithmetic of MIS:702-706.
+float c2_kc(float sig, float g1, float g2, float k1, float k2, float s1, float s2) {
+    const float aa1 = (float)std::pow(sig / s1, 2);
+    const float aa2 = (float)std::pow(sig / s2, 2);
+    const float bb1 = (float)(1. / (2. * g1 * g1));
+    const float bb2 = (float)(1. / (2. * g2 * g2));
+    const float D = bb1 * k1 - bb2 * k2;
+    const float E = aa1 - aa2 + bb1 * k1 * k1 - bb2 * k2 * k2;
+    float kc = (float)(((double)D + std::sqrt(std::pow((double)D, 2) - (double)((bb1 - bb2) * E))) / (double)(bb1 - bb2));
+    if (g1 == g2) kc = (aa2 - aa1 + bb1 * (k2 * k2 - k1 * k1)) / (2 * bb1 * (k2 - k1));
+    return kc;
+}
+
+static C2Params c2_params(float sig, float g1, float g2, float k1, float k2, float s1, float s2) {
+    C2Params p;
+    p.kc = c2_kc(sig, g1, g2, k1, k2, s1, s2);
+    p.e1 = (float)std::exp(-std::pow((double)(sig / s1), 2));
+    p.e2 = (float)std::exp(-std::pow((double)(sig / s2), 2));
+    p.k1 = k1;
+    p.k2 = k2;
+    p.i1 = (float)(1.0 / (double)(2 * g1 * g1));
+    p.i2 = (float)(1.0 / (double)(2 * g2 * g2));
+    return p;
+}
+
+// k-vectors exactly as MIS:455-462 (float storage, double arithmetic).
+void kref_table(int n, float dx, std::vector<float> &k) {
+    k.resize(n);
+    const double len = (double)((float)n * dx);
+    for (int i = 0; i < n / 2 + 1; i++) k[i] = (float)((double)i * 2.0 * PI_REF / len);
+    for (int i = n / 2 + 1; i < n; i++) k[i] = (float)((double)(i - n) * 2.0 * PI_REF / len);
+}
+
+static uint64_t splitmix64_next(uint64_t &state) {  // pfc_common.h:165-170
+    uint64_t z = (state += 0x9e3779b97f4a7c15ULL);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+static double rng_u01(uint64_t &state) {  // pfc_common.h:172-176
+    return (double)(splitmix64_next(state) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+bool is_supported_len(int n) { return n >= 32 && n <= 2048 && (n & (n - 1)) == 0; }
+
+static int round_up(int x, int a) { return (x + a - 1) / a * a; }
+
+}  // namespace pfc
+
+using namespace pfc;
+
+// ---------------------------------------------------------------------------
+// Run objects
+// ---------------------------------------------------------------------------
+struct GrainHost {
+    float center_x, center_y, center_z;
+    float cth;
+    double cother;
+};
+static_assert(sizeof(GrainHost) == 24, "grain layout");
+
+int pfc_run_init_state(pfc_run *r);
+
+extern "C" const char *pfc_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" int pfc_default_params(int model, pfc_run_params *p) {
+    if (!p) return set_error(PFC_E_INVALID, "null params");
+    std::memset(p, 0, sizeof(*p));
+    p->model = model;
+    p->L = 256;
+    p->M = 256;
+    p->N = 1;
+    p->seed = 20200604u;
+    p->dt = 0.05f;
+    p->dx = 0.125f;
+    p->con0 = 0.2f;
+    p->axx = 0.0f;
+    p->precision = PFC_PRECISION_FP32;
+    p->device = 0;
+    if (model == PFC_MODEL_CVD) {
+        p->u0 = 0.01f;
+        p->sig = 0.03f;
+        p->grainx = p->grainy = p->grainz = 1;
+    } else if (model == PFC_MODEL_MISFIT) {
+        p->u0 = 0.05f;
+        p->sig = 0.05f;
+        p->grainx = 16;
+        p->grainy = 16;
+        p->grainz = 1;
+    } else {
+        return set_error(PFC_E_INVALID, "unknown model");
+    }
+    return PFC_OK;
+}
+
+static void free_run(pfc_run *r) {
+    if (!r) return;
+    if (r->dev_mem) cudaFree(r->dev_mem);
+    if (r->f64) fp64_destroy(r->f64);
+    delete r;
+}
+
+extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) {
+    if (!p || !out) return set_error(PFC_E_INVALID, "null argument");
+    *out = nullptr;
+    if (p->model != PFC_MODEL_MISFIT && p->model != PFC_MODEL_CVD) return set_error(PFC_E_INVALID, "unknown model");
+    if (!is_supported_len(p->L) || !is_supported_len(p->M))
+        return set_error(PFC_E_INVALID, "L and M must be powers of two in [32, 2048]");
+    if (p->N < 1 || p->N > 2048 || (p->N & (p->N - 1)) != 0) return set_error(PFC_E_INVALID, "N must be a power of two <= 2048");
+    if (p->N != 1 && p->precision == PFC_PRECISION_FP32)
+        return set_error(PFC_E_INVALID, "the FP32 path supports 2-D grids (N = 1); use an FP64 precision for 3-D");
+    if (p->N != 1 && p->model == PFC_MODEL_MISFIT) return set_error(PFC_E_INVALID, "Misfit runs are 2-D (N = 1)");
+    if (!(p->dt > 0.0f) || !(p->dx > 0.0f)) return set_error(PFC_E_INVALID, "dt and dx must be > 0");
+    if (p->precision != PFC_PRECISION_FP32 && p->precision != PFC_PRECISION_FP64 && p->precision != PFC_PRECISION_FP64_PURE)
+        return set_error(PFC_E_INVALID, "unknown precision");
+    if (p->model == PFC_MODEL_MISFIT &&
+        (p->grainx <= 0 || p->grainy <= 0 || p->grainz <= 0 || p->grainx > p->L || p->grainy > p->M || p->grainz > p->N))
+        return set_error(PFC_E_INVALID, "grain counts must be in [1, grid extent]");
+    Context *ctx = nullptr;
+    int rc = get_context(p->device, &ctx);
+    if (rc != PFC_OK) return rc;
+    PFC_CUDA_TRY(cudaSetDevice(p->device));
+
+    pfc_run *r = new pfc_run();
+    r->p = *p;
+    r->ctx = ctx;
+    r->stream = ctx->stream;
+    r->L = p->L;
+    r->M = p->M;
+    r->N = p->N;
+    r->P = (long)p->L * p->M * p->N;
+    r->Hp = round_up(p->M / 2 + 1, 16);
+    model_coefs(p->model, &r->k);
+    const ModelCoefs &k = r->k;
+    r->c2a = c2_params(p->sig, k.gaa1, k.gaa2, k.ka1, k.ka2, k.sigMa1, k.sigMa2);
+    r->c2b = c2_params(p->sig, k.gab1, k.gab2, k.kb1, k.kb2, k.sigMb1, k.sigMb2);
+    kref_table(p->L, p->dx, r->krefl);
+    kref_table(p->M, p->dx, r->krefm);
+    kref_table(p->N, p->dx, r->krefn);
+    r->b0 = (p->dx > 0.0f && p->dt > 0.0f && p->axx >= 0.0f) ? (float)std::sqrt(p->axx / p->dx / p->dx / p->dx / p->dt)
+                                                              : 0.0f;
+
+    // device memory: 8 row-space arrays + 2 real fields + k tables + partials + result
+    const size_t rs = (size_t)r->L * r->Hp * sizeof(float2);
+    const size_t real = (size_t)r->P * sizeof(float);
+    const int nparts = analysis_partials(r->L, r->M);
+    r->nparts = nparts;
+    const size_t ktab = (size_t)(r->L + r->M + r->N) * sizeof(float);
+    const size_t parts = (size_t)(2 * nparts + 4096) * sizeof(double);
+    size_t bytes = 0;
+    const bool fp32 = p->precision == PFC_PRECISION_FP32;
+    if (fp32) bytes += 8 * rs;
+    bytes += 2 * real + round_up((int)ktab, 256) + parts + sizeof(RunDesc) + 1024;
+    cudaError_t e = cudaMalloc(&r->dev_mem, bytes);
+    if (e != cudaSuccess) {
+        free_run(r);
+        return set_error(PFC_E_NOMEM, std::string("cudaMalloc run state: ") + cudaGetErrorString(e));
+    }
+    cudaMemsetAsync(r->dev_mem, 0, bytes, r->stream);
+    char *m = (char *)r->dev_mem;
+    RunDesc &d = r->desc;
+    std::memset(&d, 0, sizeof(d));
+    if (fp32) {
+        float2 **arrs[8] = {&d.psi, &d.con, &d.ca, &d.cb, &d.inn, &d.inc, &d.gx, &d.gy};
+        for (int i = 0; i < 8; ++i) {
+            *arrs[i] = (float2 *)m;
+            m += rs;
+        }
+    }
+    d.psi_real = (float *)m;
+    m += real;
+    d.con_real = (float *)m;
+    m += real;
+    float *kt = (float *)m;
+    m += round_up((int)ktab, 256);
+    d.krefl = kt;
+    d.krefm = kt + r->L;
+    r->d_krefn = kt + r->L + r->M;
+    d.partials = (double *)m;
+    r->d_scratch = (double *)m + 2 * nparts;
+    m += parts;
+    r->d_desc = (RunDesc *)m;
+    cudaMemcpyAsync(kt, r->krefl.data(), r->L * sizeof(float), cudaMemcpyHostToDevice, r->stream);
+    cudaMemcpyAsync(kt + r->L, r->krefm.data(), r->M * sizeof(float), cudaMemcpyHostToDevice, r->stream);
+    cudaMemcpyAsync(kt + r->L + r->M, r->krefn.data(), r->N * sizeof(float), cudaMemcpyHostToDevice, r->stream);
+    d.L = r->L;
+    d.M = r->M;
+    d.N = r->N;
+    d.Hp = r->Hp;
+    d.model = p->model;
+    d.dt = p->dt;
+    d.k = r->k;
+    d.c2a = r->c2a;
+    d.c2b = r->c2b;
+
+    if (!fp32) {
+        rc = fp64_create(r);
+        if (rc != PFC_OK) {
+            free_run(r);
+            return rc;
+        }
+    }
+    rc = pfc_run_init_state(r);
+    if (rc != PFC_OK) {
+        free_run(r);
+        return rc;
+    }
+    *out = r;
+    return PFC_OK;
+}
+
+// Initial condition into d.psi_real / d.con_real (FP32, exact reference values).
+static int init_real_fields(pfc_run *r) {
+    const pfc_run_params &p = r->p;
+    const ModelCoefs &k = r->k;
+    RunDesc &d = r->desc;
+    if (p.model == PFC_MODEL_MISFIT) {
+        // INITIAL_dis (MIS:610-682)
+        const int dnx = p.L / p.grainx, dny = p.M / p.grainy, dnz = p.N / p.grainz;
+        std::vector<GrainHost> grains;
+        for (int iii = 0; iii < p.grainx; iii++)
+            for (int jjj = 0; jjj < p.grainy; jjj++)
+                for (int kkk = 0; kkk < p.grainz; kkk++) {
+                    GrainHost g;
+                    g.center_x = (float)(dnx * iii + dnx / 2);
+                    g.center_y = (float)(dny * jjj + dny / 2);
+                    g.center_z = (float)(dnz * kkk + dnz / 2);
+                    const unsigned int center_sum =
+                        (unsigned int)((dnx * iii + dnx / 2) + (dny * jjj + dny / 2) + (dnz * kkk + dnz / 2));
+                    uint64_t st = (uint64_t)(p.seed ^ (center_sum * 2654435761u));
+                    const double v1 = 80.0 * (rng_u01(st) - 0.5);
+                    (void)rng_u01(st);
+                    const float theta = (float)(v1 * PI_REF / 180);
+                    g.cth = cosf(theta);
+                    g.cother = std::cos(PI_REF / 2 - (double)theta - (double)(iii + jjj + kkk) * PI_REF);
+                    grains.push_back(g);
+                }
+        const float kk = (1 - p.con0) * k.ka0 + p.con0 * k.kb0;
+        const int ext = p.L + p.M + 4;
+        const int xmin = -ext, ntab = 2 * ext + 1;
+        std::vector<float> costab(ntab);
+        for (int i = 0; i < ntab; ++i) {
+            const int X = xmin + i;
+            costab[i] = cosf(kk * (float)X * p.dx);
+        }
+        const double limx = (double)((float)p.L * p.dx / (float)p.grainx) / 2. - 0.2;
+        const double limy = (double)((float)p.M * p.dx / (float)p.grainy) / 2. - 0.2;
+        const size_t gbytes = grains.size() * sizeof(GrainHost), tbytes = costab.size() * sizeof(float);
+        char *tmp = nullptr;
+        PFC_CUDA_TRY(cudaMalloc(&tmp, gbytes + tbytes + 256));
+        PFC_CUDA_TRY(cudaMemcpyAsync(tmp, grains.data(), gbytes, cudaMemcpyHostToDevice, r->stream));
+        PFC_CUDA_TRY(cudaMemcpyAsync(tmp + round_up((int)gbytes, 256), costab.data(), tbytes, cudaMemcpyHostToDevice,
+                                     r->stream));
+        const float A1 = 0.1427f, A2 = 0.106f;
+        PFC_CUDA_TRY(launch_init_misfit(d.psi_real, d.con_real, p.L, p.M, p.N, p.u0, p.con0, p.dx, tmp,
+                                        (int)grains.size(), limx, limy, (const float *)(tmp + round_up((int)gbytes, 256)),
+                                        xmin, ntab, 2 * A1, 4 * A2, r->stream));
+        PFC_CUDA_TRY(cudaStreamSynchronize(r->stream));
+        cudaFree(tmp);
+    } else {
+        // INITIAL_C2 (CVD:587-642), rotation w3 = 0
+        const float w3 = (float)(0. * PI_REF / 180);
+        const float cw = cosf(w3), sw = sinf(w3);
+        std::vector<float> tab(2 * (p.L + p.M));
+        for (int pass = 0; pass < 2; ++pass) {
+            const float kx = pass == 0 ? k.ka0 : k.kb0;
+            float *tl = tab.data() + pass * (p.L + p.M);
+            float *tm = tl + p.L;
+            for (int l = 0; l < p.L; ++l) {
+                const float x = (float)(0 - p.L / 2 + l) * p.dx;
+                tl[l] = cosf(kx * x * cw + kx * 0.0f * sw);
+            }
+            for (int mm = 0; mm < p.M; ++mm) {
+                const float y = (float)(mm - p.M / 2) * p.dx;
+                tm[mm] = cosf(-0.0f * kx * sw + kx * y * cw);
+            }
+        }
+        float *tmp = nullptr;
+        PFC_CUDA_TRY(cudaMalloc(&tmp, tab.size() * sizeof(float)));
+        PFC_CUDA_TRY(cudaMemcpyAsync(tmp, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice, r->stream));
+        const float A1 = 0.15f, A2 = 0.106f;
+        PFC_CUDA_TRY(launch_init_cvd(d.psi_real, d.con_real, p.L, p.M, p.N, p.u0, p.con0, tmp, 2 * A1, 4 * A2, r->stream));
+        PFC_CUDA_TRY(cudaStreamSynchronize(r->stream));
+        cudaFree(tmp);
+    }
+    return PFC_OK;
+}
+
+// Means of the real fields (FP64), then row space and the c2a/c2b arrays.
+static int fp32_from_real(pfc_run *r, bool means_from_device) {
+    RunDesc &d = r->desc;
+    if (means_from_device) {
+        const int blocks = 256;
+        PFC_CUDA_TRY(launch_sum_f32(d.psi_real, r->P, r->d_scratch, blocks, r->d_scratch + blocks, r->stream));
+        PFC_CUDA_TRY(launch_sum_f32(d.con_real, r->P, r->d_scratch, blocks, r->d_scratch + blocks + 1, r->stream));
+        double sums[2];
+        PFC_CUDA_TRY(cudaMemcpyAsync(sums, r->d_scratch + blocks, sizeof(sums), cudaMemcpyDeviceToHost, r->stream));
+        PFC_CUDA_TRY(cudaStreamSynchronize(r->stream));
+        r->psi_mean = sums[0] / (double)r->P;
+        r->con_mean = sums[1] / (double)r->P;
+    }
+    d.psi_mean = r->psi_mean;
+    d.con_mean = r->con_mean;
+    d.psi_mean_f = (float)r->psi_mean;
+    d.con_mean_f = (float)r->con_mean;
+    PFC_CUDA_TRY(cudaMemcpyAsync(r->d_desc, &d, sizeof(RunDesc), cudaMemcpyHostToDevice, r->stream));
+    PFC_CUDA_TRY(launch_row_forward(r->d_desc, 1, r->L, r->M, r->ctx->tw, r->stream));
+    PFC_CUDA_TRY(launch_col_step(r->d_desc, 1, r->L, r->M, COL_PREPARE, r->ctx->tw, r->stream));
+    PFC_CUDA_TRY(cudaStreamSynchronize(r->stream));
+    r->fields_valid = true;
+    r->energy_valid = false;
+    return PFC_OK;
+}
+
+int pfc_run_init_state(pfc_run *r) {
+    PFC_CUDA_TRY(cudaSetDevice(r->p.device));
+    int rc = init_real_fields(r);
+    if (rc != PFC_OK) return rc;
+    r->t = 0;
+    if (r->p.precision != PFC_PRECISION_FP32) return fp64_init_from_real(r, true);
+    return fp32_from_real(r, true);
+}
+
+extern "C" int pfc_run_destroy(pfc_run *r) {
+    if (!r) return PFC_OK;
+    cudaSetDevice(r->p.device);
+    cudaStreamSynchronize(r->stream);
+    free_run(r);
+    return PFC_OK;
+}
+
+static int fp32_advance(pfc_run *r, int nsteps, int analysis) {
+    for (int i = 0; i < nsteps; ++i) {
+        const bool last = i == nsteps - 1;
+        PFC_CUDA_TRY(launch_row_step(r->d_desc, 1, r->L, r->M, r->ctx->tw, r->stream));
+        PFC_CUDA_TRY(launch_col_step(r->d_desc, 1, r->L, r->M, (last && analysis) ? COL_STEP_CHECKPOINT : COL_STEP,
+                                     r->ctx->tw, r->stream));
+    }
+    r->t += nsteps;
+    r->fields_valid = false;
+    r->energy_valid = false;
+    if (analysis) {
+        PFC_CUDA_TRY(launch_row_analysis(r->d_desc, 1, r->L, r->M, r->ctx->tw, r->stream));
+        PFC_CUDA_TRY(launch_reduce_fixed(r->desc.partials, r->nparts, 2, 2, r->d_scratch, r->stream));
+        r->fields_valid = true;
+        r->energy_valid = true;
+    }
+    return PFC_OK;
+}
+
+extern "C" int pfc_run_advance(pfc_run *r, int nsteps, int analysis) {
+    if (!r || nsteps < 0) return set_error(PFC_E_INVALID, "bad run or step count");
+    if (nsteps == 0) return PFC_OK;
+    PFC_CUDA_TRY(cudaSetDevice(r->p.device));
+    if (r->p.precision != PFC_PRECISION_FP32) return fp64_advance(r, nsteps);
+    return fp32_advance(r, nsteps, analysis);
+}
+
+extern "C" int pfc_run_steps(const pfc_run *r, int *steps) {
+    if (!r || !steps) return set_error(PFC_E_INVALID, "null argument");
+    *steps = r->t;
+    return PFC_OK;
+}
+
+// Make d.psi_real / d.con_real hold the current state.
+static int materialize(pfc_run *r) {
+    if (r->p.precision != PFC_PRECISION_FP32) return fp64_materialize(r);
+    if (r->fields_valid) return PFC_OK;
+    PFC_CUDA_TRY(launch_row_analysis(r->d_desc, 1, r->L, r->M, r->ctx->tw, r->stream));
+    r->fields_valid = true;
+    return PFC_OK;
+}
+
+extern "C" int pfc_run_get_fields_f32(pfc_run *r, float *phi, float *con) {
+    if (!r) return set_error(PFC_E_INVALID, "null run");
+    PFC_CUDA_TRY(cudaSetDevice(r->p.device));
+    int rc = materialize(r);
+    if (rc != PFC_OK) return rc;
+    if (phi) PFC_CUDA_TRY(cudaMemcpyAsync(phi, r->desc.psi_real, r->P * sizeof(float), cudaMemcpyDeviceToHost, r->stream));
+    if (con) PFC_CUDA_TRY(cudaMemcpyAsync(con, r->desc.con_real, r->P * sizeof(float), cudaMemcpyDeviceToHost, r->stream));
+    PFC_CUDA_TRY(cudaStreamSynchronize(r->stream));
+    return PFC_OK;
+}
+
+extern "C" int pfc_run_get_fields(pfc_run *r, double *phi, double *con) {
+    if (!r) return set_error(PFC_E_INVALID, "null run");
+    if (r->p.precision != PFC_PRECISION_FP32) return fp64_get_fields(r, phi, con);
+    std::vector<float> a(phi ? r->P : 0), b(con ? r->P : 0);
+    int rc = pfc_run_get_fields_f32(r, phi ? a.data() : nullptr, con ? b.data() : nullptr);
+    if (rc != PFC_OK) return rc;
+    for (long i = 0; phi && i < r->P; ++i) phi[i] = a[i];
+    for (long i = 0; con && i < r->P; ++i) con[i] = b[i];
+    return PFC_OK;
+}
+
+extern "C" int pfc_run_set_fields(pfc_run *r, const double *phi, const double *con) {
+    if (!r || !phi || !con) return set_error(PFC_E_INVALID, "null argument");
+    PFC_CUDA_TRY(cudaSetDevice(r->p.device));
+    if (r->p.precision != PFC_PRECISION_FP32) return fp64_set_fields(r, phi, con);
+    std::vector<float> a(r->P), b(r->P);
+    double sa = 0.0, sb = 0.0;
+    for (long i = 0; i < r->P; ++i) {
+        a[i] = (float)phi[i];
+        b[i] = (float)con[i];
+        sa += phi[i];
+        sb += con[i];
+    }
+    r->psi_mean = sa / (double)r->P;
+    r->con_mean = sb / (double)r->P;
+    PFC_CUDA_TRY(cudaMemcpyAsync(r->desc.psi_real, a.data(), r->P * sizeof(float), cudaMemcpyHostToDevice, r->stream));
+    PFC_CUDA_TRY(cudaMemcpyAsync(r->desc.con_real, b.data(), r->P * sizeof(float), cudaMemcpyHostToDevice, r->stream));
+    return fp32_from_real(r, false);
+}
+
+extern "C" int pfc_run_energy(pfc_run *r, double *e_over_p, double *mass_over_p) {
+    if (!r) return set_error(PFC_E_INVALID, "null run");
+    PFC_CUDA_TRY(cudaSetDevice(r->p.device));
+    if (r->p.precision != PFC_PRECISION_FP32) return fp64_energy(r, e_over_p, mass_over_p);
+    if (!r->energy_valid) return set_error(PFC_E_STATE, "energy is available after pfc_run_advance(..., analysis=1)");
+    double s[2];
+    PFC_CUDA_TRY(cudaMemcpyAsync(s, r->d_scratch, sizeof(s), cudaMemcpyDeviceToHost, r->stream));
+    PFC_CUDA_TRY(cudaStreamSynchronize(r->stream));
+    if (e_over_p) *e_over_p = s[0] / r->L / r->M / r->N;
+    if (mass_over_p) *mass_over_p = s[1] / r->L / r->M / r->N;
+    return PFC_OK;
+}
+
+extern "C" int pfc_run_means(const pfc_run *r, double *phi_mean, double *con_mean) {
+    if (!r) return set_error(PFC_E_INVALID, "null run");
+    if (phi_mean) *phi_mean = r->psi_mean;
+    if (con_mean) *con_mean = r->con_mean;
+    return PFC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batches: runs grouped by grid size, one launch per size class per sweep,
+// captured once into a CUDA graph per step count.
+// ---------------------------------------------------------------------------
+struct SizeClass {
+    int L, M;
+    std::vector<pfc_run *> runs;
+    RunDesc *d_descs = nullptr;
+};
+
+struct pfc_batch {
+    std::vector<SizeClass> classes;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    Context *ctx = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+};
+
+extern "C" int pfc_batch_create(pfc_run *const *runs, int nruns, pfc_batch **out) {
+    if (!runs || nruns <= 0 || !out) return set_error(PFC_E_INVALID, "empty batch");
+    *out = nullptr;
+    const int dev = runs[0]->p.device;
+    for (int i = 0; i < nruns; ++i) {
+        if (!runs[i]) return set_error(PFC_E_INVALID, "null run in batch");
+        if (runs[i]->p.precision != PFC_PRECISION_FP32) return set_error(PFC_E_INVALID, "batches hold FP32 runs only");
+        if (runs[i]->p.device != dev) return set_error(PFC_E_INVALID, "batch runs must share one device");
+    }
+    PFC_CUDA_TRY(cudaSetDevice(dev));
+    pfc_batch *b = new pfc_batch();
+    b->device = dev;
+    b->ctx = runs[0]->ctx;
+    b->stream = runs[0]->stream;
+    for (int i = 0; i < nruns; ++i) {
+        SizeClass *sc = nullptr;
+        for (auto &c : b->classes)
+            if (c.L == runs[i]->L && c.M == runs[i]->M) sc = &c;
+        if (!sc) {
+            b->classes.push_back(SizeClass{runs[i]->L, runs[i]->M, {}, nullptr});
+            sc = &b->classes.back();
+        }
+        sc->runs.push_back(runs[i]);
+    }
+    for (auto &c : b->classes) {
+        std::vector<RunDesc> h;
+        for (auto *r : c.runs) h.push_back(r->desc);
+        cudaError_t e = cudaMalloc(&c.d_descs, h.size() * sizeof(RunDesc));
+        if (e != cudaSuccess) {
+            pfc_batch_destroy(b);
+            return cuda_error(e, "cudaMalloc batch descriptors");
+        }
+        cudaMemcpy(c.d_descs, h.data(), h.size() * sizeof(RunDesc), cudaMemcpyHostToDevice);
+    }
+    *out = b;
+    return PFC_OK;
+}
+
+extern "C" int pfc_batch_destroy(pfc_batch *b) {
+    if (!b) return PFC_OK;
+    cudaSetDevice(b->device);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (auto &c : b->classes)
+        if (c.d_descs) cudaFree(c.d_descs);
+    delete b;
+    return PFC_OK;
+}
+
+static int batch_enqueue(pfc_batch *b, int nsteps) {
+    for (int i = 0; i < nsteps; ++i) {
+        for (auto &c : b->classes)
+            PFC_CUDA_TRY(launch_row_step(c.d_descs, (int)c.runs.size(), c.L, c.M, b->ctx->tw, b->stream));
+        for (auto &c : b->classes)
+            PFC_CUDA_TRY(launch_col_step(c.d_descs, (int)c.runs.size(), c.L, c.M, COL_STEP, b->ctx->tw, b->stream));
+    }
+    return PFC_OK;
+}
+
+// Event-timed advance on the batch's stream: *ms = device time of the nsteps.
+extern "C" int pfc_batch_advance_timed(pfc_batch *b, int nsteps, float *ms) {
+    if (!b || !ms) return set_error(PFC_E_INVALID, "null argument");
+    PFC_CUDA_TRY(cudaSetDevice(b->device));
+    cudaEvent_t e0, e1;
+    PFC_CUDA_TRY(cudaEventCreate(&e0));
+    PFC_CUDA_TRY(cudaEventCreate(&e1));
+    int rc = PFC_OK;
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, b->stream);
+    if (e == cudaSuccess) rc = pfc_batch_advance(b, nsteps);
+    if (e == cudaSuccess && rc == PFC_OK) e = cudaEventRecord(e1, b->stream);
+    if (e == cudaSuccess && rc == PFC_OK) e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess && rc == PFC_OK) e = cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != PFC_OK) return rc;
+    if (e != cudaSuccess) return cuda_error(e, "pfc_batch_advance_timed");
+    return PFC_OK;
+}
+
+// Per-kernel device times: reps steps, each row-kernel and column-kernel launch
+// (all size classes) bracketed by events; averages in milliseconds per launch set.
+extern "C" int pfc_batch_kernel_times(pfc_batch *b, int reps, double *row_ms, double *col_ms) {
+    if (!b || reps <= 0 || !row_ms || !col_ms) return set_error(PFC_E_INVALID, "bad argument");
+    PFC_CUDA_TRY(cudaSetDevice(b->device));
+    std::vector<cudaEvent_t> ev(3 * reps);
+    for (auto &x : ev) PFC_CUDA_TRY(cudaEventCreate(&x));
+    PFC_CUDA_TRY(cudaStreamSynchronize(b->stream));
+    for (int i = 0; i < reps; ++i) {
+        PFC_CUDA_TRY(cudaEventRecord(ev[3 * i], b->stream));
+        for (auto &c : b->classes)
+            PFC_CUDA_TRY(launch_row_step(c.d_descs, (int)c.runs.size(), c.L, c.M, b->ctx->tw, b->stream));
+        PFC_CUDA_TRY(cudaEventRecord(ev[3 * i + 1], b->stream));
+        for (auto &c : b->classes)
+            PFC_CUDA_TRY(launch_col_step(c.d_descs, (int)c.runs.size(), c.L, c.M, COL_STEP, b->ctx->tw, b->stream));
+        PFC_CUDA_TRY(cudaEventRecord(ev[3 * i + 2], b->stream));
+    }
+    PFC_CUDA_TRY(cudaStreamSynchronize(b->stream));
+    double rs = 0.0, cs = 0.0;
+    for (int i = 0; i < reps; ++i) {
+        float a = 0.f, c = 0.f;
+        PFC_CUDA_TRY(cudaEventElapsedTime(&a, ev[3 * i], ev[3 * i + 1]));
+        PFC_CUDA_TRY(cudaEventElapsedTime(&c, ev[3 * i + 1], ev[3 * i + 2]));
+        rs += a;
+        cs += c;
+    }
+    for (auto &x : ev) cudaEventDestroy(x);
+    for (auto &c : b->classes)
+        for (auto *r : c.runs) {
+            r->t += reps;
+            r->fields_valid = false;
+            r->energy_valid = false;
+        }
+    *row_ms = rs / reps;
+    *col_ms = cs / reps;
+    return PFC_OK;
+}
+
+extern "C" int pfc_batch_advance(pfc_batch *b, int nsteps) {
+    if (!b || nsteps < 0) return set_error(PFC_E_INVALID, "bad batch or step count");
+    if (nsteps == 0) return PFC_OK;
+    PFC_CUDA_TRY(cudaSetDevice(b->device));
+    // one graph covers `chunk` steps; replay it and enqueue the remainder directly
+    const int chunk = nsteps < 16 ? nsteps : 16;
+    if (!b->graph || b->graph_steps != chunk) {
+        if (b->graph) {
+            cudaGraphExecDestroy(b->graph);
+            b->graph = nullptr;
+        }
+        // kernel attribute setup (max dynamic shared memory) happens outside the capture
+        for (auto &c : b->classes) PFC_CUDA_TRY(prepare_size(c.L, c.M));
+        int rc = PFC_OK;
+        cudaGraph_t g = nullptr;
+        PFC_CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        rc = batch_enqueue(b, chunk);
+        cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+        if (rc != PFC_OK) return rc;
+        if (e != cudaSuccess) return cuda_error(e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&b->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_error(e, "cudaGraphInstantiate");
+        b->graph_steps = chunk;
+    }
+    int done = 0;
+    while (nsteps - done >= chunk) {
+        PFC_CUDA_TRY(cudaGraphLaunch(b->graph, b->stream));
+        done += chunk;
+    }
+    int rc = batch_enqueue(b, nsteps - done);
+    if (rc != PFC_OK) return rc;
+    for (auto &c : b->classes)
+        for (auto *r : c.runs) {
+            r->t += nsteps;
+            r->fields_valid = false;
+            r->energy_valid = false;
+        }
+    return PFC_OK;
+}

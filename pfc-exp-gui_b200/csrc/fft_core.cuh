@@ -1,0 +1,251 @@
+// fft_core.cuh -- shared-memory Stockham FFT building blocks for sm_100a.
+//
+// The reference transforms every field with FFTW's complex 3-D DFT
+// (src/experiment/misfit_uniform_time_seed_fftw_early.cpp:438-452, FFTW_ESTIMATE,
+// unnormalised, exp(-2 pi i jk/n) forward).  Here the transforms are written from
+// scratch: a batch of NB interleaved sequences of length N lives in shared memory
+// (element e of sequence b at s[e*NB + b], so consecutive threads touch consecutive
+// words), and each Stockham stage has every thread load a fixed number of complex
+// values into registers, run radix-2/4/8/16 butterflies there, and store them to
+// their autosorted positions.  Natural order in, natural order out; no bit reversal.
+//
+// Twiddles come from a per-length table tw[j] = exp(-2 pi i j / N) computed on the
+// host in double and rounded once to the working precision.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pfc {
+
+// ---------------------------------------------------------------------------
+// complex helpers (float2 / double2)
+// ---------------------------------------------------------------------------
+template <typename T> struct cplx_traits;
+template <> struct cplx_traits<float> { typedef float2 C; };
+template <> struct cplx_traits<double> { typedef double2 C; };
+
+__device__ __forceinline__ float2 mk(float x, float y) { return make_float2(x, y); }
+__device__ __forceinline__ double2 mk(double x, double y) { return make_double2(x, y); }
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// multiply by conj(b)
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+    return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {
+    return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+
+// multiply by -i (forward) or +i (inverse)
+template <bool FWD, typename C> __device__ __forceinline__ C mul_mi(C a) {
+    return FWD ? mk(a.y, -a.x) : mk(-a.y, a.x);
+}
+
+// ---------------------------------------------------------------------------
+// Radix butterflies (in registers).  FWD uses exp(-2 pi i / R), inverse exp(+).
+// ---------------------------------------------------------------------------
+template <bool FWD, typename C> __device__ __forceinline__ void dft2(C &a0, C &a1) {
+    C t = a0;
+    a0 = cadd(t, a1);
+    a1 = csub(t, a1);
+}
+
+template <bool FWD, typename C> __device__ __forceinline__ void dft4(C &a0, C &a1, C &a2, C &a3) {
+    C t0 = cadd(a0, a2), t1 = csub(a0, a2);
+    C t2 = cadd(a1, a3), t3 = mul_mi<FWD>(csub(a1, a3));
+    a0 = cadd(t0, t2);
+    a2 = csub(t0, t2);
+    a1 = cadd(t1, t3);
+    a3 = csub(t1, t3);
+}
+
+template <typename R> struct kconst;
+template <> struct kconst<float> {
+    static __device__ __forceinline__ float h() { return 0.70710678118654752f; }
+    static __device__ __forceinline__ float c8() { return 0.92387953251128674f; }
+    static __device__ __forceinline__ float s8() { return 0.38268343236508977f; }
+};
+template <> struct kconst<double> {
+    static __device__ __forceinline__ double h() { return 0.70710678118654752440; }
+    static __device__ __forceinline__ double c8() { return 0.92387953251128675613; }
+    static __device__ __forceinline__ double s8() { return 0.38268343236508977173; }
+};
+
+template <typename C> struct real_of;
+template <> struct real_of<float2> { typedef float T; };
+template <> struct real_of<double2> { typedef double T; };
+
+// multiply by w8^k for k = 1, 2, 3 where w8 = exp(-+2 pi i / 8)
+template <bool FWD, typename C> __device__ __forceinline__ C w8_1(C a) {
+    typedef typename real_of<C>::T R;
+    const R h = kconst<R>::h();
+    // FWD: (h, -h);  INV: (h, +h)
+    return FWD ? mk(h * (a.x + a.y), h * (a.y - a.x)) : mk(h * (a.x - a.y), h * (a.x + a.y));
+}
+template <bool FWD, typename C> __device__ __forceinline__ C w8_3(C a) {
+    typedef typename real_of<C>::T R;
+    const R h = kconst<R>::h();
+    // FWD: (-h, -h); INV: (-h, +h)
+    return FWD ? mk(h * (a.y - a.x), -h * (a.x + a.y)) : mk(-h * (a.x + a.y), h * (a.x - a.y));
+}
+
+template <bool FWD, typename C> __device__ __forceinline__ void dft8(C *a) {
+    // radix-2 DIT over two length-4 DFTs
+    C e0 = a[0], e1 = a[2], e2 = a[4], e3 = a[6];
+    C o0 = a[1], o1 = a[3], o2 = a[5], o3 = a[7];
+    dft4<FWD>(e0, e1, e2, e3);
+    dft4<FWD>(o0, o1, o2, o3);
+    o1 = w8_1<FWD>(o1);
+    o2 = mul_mi<FWD>(o2);
+    o3 = w8_3<FWD>(o3);
+    a[0] = cadd(e0, o0);
+    a[4] = csub(e0, o0);
+    a[1] = cadd(e1, o1);
+    a[5] = csub(e1, o1);
+    a[2] = cadd(e2, o2);
+    a[6] = csub(e2, o2);
+    a[3] = cadd(e3, o3);
+    a[7] = csub(e3, o3);
+}
+
+// multiply by w16^j (j = n2*k1 in 0..9), w16 = exp(-+2 pi i / 16)
+template <bool FWD, typename C> __device__ __forceinline__ C w16(C a, int j) {
+    typedef typename real_of<C>::T R;
+    const R c1 = kconst<R>::c8(), s1 = kconst<R>::s8(), h = kconst<R>::h();
+    R c, s;  // exp(-i theta) = c - i s with theta = 2 pi j / 16
+    switch (j) {
+        case 0: return a;
+        case 1: c = c1; s = s1; break;
+        case 2: c = h; s = h; break;
+        case 3: c = s1; s = c1; break;
+        case 4: return mul_mi<FWD>(a);
+        case 5: c = -s1; s = c1; break;
+        case 6: c = -h; s = h; break;
+        case 7: c = -c1; s = s1; break;
+        case 8: return mk(-a.x, -a.y);
+        default: c = -c1; s = -s1; break;  // 9
+    }
+    if (!FWD) s = -s;
+    // (a.x + i a.y)(c - i s)
+    return mk(a.x * c + a.y * s, a.y * c - a.x * s);
+}
+
+template <bool FWD, typename C> __device__ __forceinline__ void dft16(C *a) {
+    // 16 = 4 x 4: X[k1 + 4 k2] = sum_n2 w4^(n2 k2) w16^(n2 k1) sum_n1 a[4 n1 + n2] w4^(n1 k1)
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) dft4<FWD>(a[n2], a[n2 + 4], a[n2 + 8], a[n2 + 12]);
+    // now a[n2 + 4*k1] holds the inner DFT output k1 of column n2
+#pragma unroll
+    for (int n2 = 1; n2 < 4; ++n2)
+#pragma unroll
+        for (int k1 = 1; k1 < 4; ++k1) a[n2 + 4 * k1] = w16<FWD>(a[n2 + 4 * k1], n2 * k1);
+    C b[16];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+        C x0 = a[0 + 4 * k1], x1 = a[1 + 4 * k1], x2 = a[2 + 4 * k1], x3 = a[3 + 4 * k1];
+        dft4<FWD>(x0, x1, x2, x3);
+        b[k1 + 0] = x0;
+        b[k1 + 4] = x1;
+        b[k1 + 8] = x2;
+        b[k1 + 12] = x3;
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) a[i] = b[i];
+}
+
+template <int R, bool FWD, typename C> __device__ __forceinline__ void dftR(C *a) {
+    if (R == 2) dft2<FWD>(a[0], a[1]);
+    else if (R == 4) dft4<FWD>(a[0], a[1], a[2], a[3]);
+    else if (R == 8) dft8<FWD>(a);
+    else if (R == 16) dft16<FWD>(a);
+}
+
+// ---------------------------------------------------------------------------
+// Radix plan: N = 16^a * r with r in {1, 2, 4, 8}; the small radix comes last.
+// ---------------------------------------------------------------------------
+template <int N> struct radix_plan {
+    static constexpr int log2n = (N <= 1) ? 0 : 1 + radix_plan<N / 2>::log2n;
+    static constexpr int n16 = log2n / 4;
+    static constexpr int tail = 1 << (log2n % 4);  // 1, 2, 4 or 8
+    static constexpr int stages = n16 + (tail > 1 ? 1 : 0);
+};
+template <> struct radix_plan<1> {
+    static constexpr int log2n = 0;
+    static constexpr int n16 = 0;
+    static constexpr int tail = 1;
+    static constexpr int stages = 0;
+};
+
+// One Stockham stage of radix R on NB interleaved sequences of length N in shared
+// memory, in place.  Each of the NT threads owns PER_T = NB*N/(R*NT) butterflies.
+// tw: table of exp(-2 pi i j / N), j < N.
+template <int N, int NB, int NT, int R, bool FWD, typename C>
+__device__ __forceinline__ void stockham_stage(C *s, const C *__restrict__ tw, int Ns) {
+    constexpr int ITEMS = NB * (N / R);
+    constexpr int PER_T = (ITEMS + NT - 1) / NT;
+    const int tid = threadIdx.x;
+    C v[PER_T][R];
+#pragma unroll
+    for (int q = 0; q < PER_T; ++q) {
+        const int w = tid + q * NT;
+        if (ITEMS % NT == 0 || w < ITEMS) {
+            const int b = w % NB, j = w / NB;
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[q][r] = s[(j + r * (N / R)) * NB + b];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < PER_T; ++q) {
+        const int w = tid + q * NT;
+        if (ITEMS % NT == 0 || w < ITEMS) {
+            const int b = w % NB, j = w / NB;
+            const int k = j % Ns;
+            if (Ns > 1) {
+                // twiddle w^(r*k) with w = exp(-+2 pi i/(Ns*R)); table step N/(Ns*R)
+                const int step = N / (Ns * R);
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    const C t = tw[(r * k * step) & (N - 1)];
+                    v[q][r] = FWD ? cmul(v[q][r], t) : cmulc(v[q][r], t);
+                }
+            }
+            dftR<R, FWD>(v[q]);
+            const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) s[(base + r * Ns) * NB + b] = v[q][r];
+        }
+    }
+    __syncthreads();
+}
+
+// Full in-place FFT of NB interleaved length-N sequences in shared memory.
+// Caller must __syncthreads() before (data written) -- the routine syncs after.
+template <int N, int NB, int NT, bool FWD, typename C>
+__device__ __forceinline__ void fft_smem(C *s, const C *__restrict__ tw) {
+    typedef radix_plan<N> P;
+    int Ns = 1;
+    if constexpr (P::n16 > 0) {
+#pragma unroll
+        for (int st = 0; st < P::n16; ++st) {
+            stockham_stage<N, NB, NT, 16, FWD>(s, tw, Ns);
+            Ns *= 16;
+        }
+    }
+    if constexpr (P::tail > 1) stockham_stage<N, NB, NT, P::tail, FWD>(s, tw, Ns);
+}
+
+}  // namespace pfc

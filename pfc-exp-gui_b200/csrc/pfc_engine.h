@@ -1,0 +1,67 @@
+// pfc_engine.h -- host-side run object shared by engine.cu, step_fp64.cu and cli.cpp.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "pfc_b200.h"
+#include "pfc_internal.h"
+
+namespace pfc {
+struct Fp64State;
+
+// Per-device context: one non-blocking stream and the twiddle tables.
+struct Context {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    TwiddleSet tw{};
+    void *tw_mem = nullptr;
+};
+
+int set_error(int code, const std::string &msg);
+int cuda_error(cudaError_t e, const char *what);
+int get_context(int device, Context **out);
+void model_coefs(int model, ModelCoefs *k);
+void kref_table(int n, float dx, std::vector<float> &k);
+float c2_kc(float sig, float g1, float g2, float k1, float k2, float s1, float s2);
+bool is_supported_len(int n);
+}  // namespace pfc
+
+struct pfc_run {
+    pfc_run_params p;
+    pfc::Context *ctx = nullptr;
+    cudaStream_t stream = nullptr;
+    int L = 0, M = 0, N = 0, Hp = 0;
+    long P = 0;
+    int nparts = 0;
+    pfc::ModelCoefs k;
+    pfc::C2Params c2a, c2b;
+    std::vector<float> krefl, krefm, krefn;
+    float b0 = 0.0f;
+    void *dev_mem = nullptr;
+    pfc::RunDesc desc;
+    pfc::RunDesc *d_desc = nullptr;
+    float *d_krefn = nullptr;
+    double *d_scratch = nullptr;
+    double psi_mean = 0.0, con_mean = 0.0;
+    int t = 0;
+    bool fields_valid = false;
+    bool energy_valid = false;
+    pfc::Fp64State *f64 = nullptr;
+};
+
+namespace pfc {
+// Plain FP64 path (step_fp64.cu).
+int fp64_create(pfc_run *r);
+void fp64_destroy(Fp64State *s);
+int fp64_init_from_real(pfc_run *r, bool from_device_real);
+int fp64_advance(pfc_run *r, int nsteps);
+int fp64_materialize(pfc_run *r);
+int fp64_get_fields(pfc_run *r, double *phi, double *con);
+int fp64_set_fields(pfc_run *r, const double *phi, const double *con);
+int fp64_energy(pfc_run *r, double *e_over_p, double *mass_over_p);
+// Kernel attribute setup for one grid size (must precede graph capture).
+cudaError_t prepare_size(int L, int M);
+}  // namespace pfc

@@ -1,0 +1,73 @@
+// pfc_internal.h -- device-side run descriptors and internal launch interfaces.
+//
+// A "run" is one Misfit or CVD simulation.  Its FP32 state lives in row space:
+// every field f[l][m] (m fastest, the reference's n + N*(m + M*l) layout with N = 1,
+// misfit_uniform_time_seed_fftw_early.cpp:600) is stored as its unnormalised DFT
+// along m, bins 0..M/2 (Hermitian half), in a row of Hp >= M/2 + 1 complex floats.
+// The k = 0 mode of phi and con is held separately in FP64 and kept out of the
+// FP32 arrays (their DC bin is zero), so the mass is conserved exactly.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pfc {
+
+enum Model : int { MODEL_MISFIT = 0, MODEL_CVD = 1 };
+
+// Model coefficients of the reference (float statics at
+// misfit_uniform_time_seed_fftw_early.cpp:116-143 and cvd.cpp:26-53).
+struct ModelCoefs {
+    float niu, ksi, para_w, para_c0, para_alpha, dynamic_mn, dynamic_mc;
+    float gaa1, gaa2, gab1, gab2;
+    float ka0, ka1, ka2, kb0, kb1, kb2;
+    float sigMa1, sigMa2, sigMb1, sigMb2;
+};
+
+// Two-peak correlation kernel parameters (misfit_uniform_time_seed_fftw_early.cpp:700-750):
+// C2(k) = e1 * exp(-(|k| - k1)^2 * i1) for |k| <= kc, else e2 * exp(-(|k| - k2)^2 * i2).
+struct C2Params {
+    float kc, e1, e2, k1, k2, i1, i2;
+};
+
+struct RunDesc {
+    int L, M, N;      // grid (N = 1 for 2-D)
+    int Hp;           // row stride of row-space arrays, in complex elements
+    int model;
+    // row-space arrays, [L][Hp] float2 each
+    float2 *psi, *con, *ca, *cb, *inn, *inc, *gx, *gy;
+    // real-space checkpoint outputs, [L][M] float
+    float *psi_real, *con_real;
+    // reference k-vectors (float), lengths L and M
+    const float *krefl, *krefm;
+    // FP64 means of phi and con (the k = 0 modes / P), and their float roundings
+    double psi_mean, con_mean;
+    float psi_mean_f, con_mean_f;
+    float dt;
+    ModelCoefs k;
+    C2Params c2a, c2b;
+    // per-CTA partial sums written by the analysis row kernel: [2 * L] doubles
+    double *partials;
+};
+
+// Twiddle tables exp(-2 pi i j / n) for n = 2^1 .. 2^11, FP32 and FP64.
+struct TwiddleSet {
+    const float2 *f32[12];
+    const double2 *f64[12];
+};
+
+// FP32 fused step (step_fp32.cu).  All runs of one call share (L, M).
+cudaError_t launch_row_step(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw, cudaStream_t s);
+cudaError_t launch_col_step(const RunDesc *d_runs, int nruns, int L, int M, int mode, const TwiddleSet &tw,
+                            cudaStream_t s);
+cudaError_t launch_row_forward(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw, cudaStream_t s);
+cudaError_t launch_row_analysis(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw,
+                                cudaStream_t s);
+
+// column-kernel modes
+enum ColMode : int { COL_STEP = 0, COL_PREPARE = 1, COL_STEP_CHECKPOINT = 2 };
+
+// Number of partial-sum slots the analysis kernel writes per run (2 doubles each).
+int analysis_partials(int L, int M);
+
+}  // namespace pfc

@@ -1,0 +1,527 @@
+// step_fp32.cu -- fused FP32 semi-implicit spectral step (2-D Misfit / CVD).
+//
+// Restates, as two fused sweeps, one time step of the reference
+// (src/experiment/misfit_uniform_time_seed_fftw_early.cpp:479-501 and
+// src/experiment/cvd.cpp:400-422):
+//
+//   row kernel (one CTA per RPC rows l):
+//     inverse row FFTs of psi+i*con and c2a+i*c2b   (p2/p7 and p10/p11 of the reference)
+//     pointwise UPDATEINN3 + UPDATEINFMIX + UPDATEINFCMIX tail + UPDATEINC2MIX(C)
+//       (MIS:773-874) -> inn, inc
+//     forward row FFT of inn+i*inc                  (first half of p8/p9)
+//   column kernel (one CTA per C packed columns km):
+//     forward column FFTs of psi, inn, con, inc     (second half of p1/p8/p6/p9)
+//     semi-implicit update MAINEQUATIONC2_NOI/C2MIX (MIS:983-1014, CVD:865-886) with
+//       the denominators built in FP64 and rounded, k = 0 held out in FP64
+//     C2A/C2B multiply (MIS:807-810) and inverse column FFTs of psi', c2a, c2b, con'
+//
+// Compulsory HBM traffic: row kernel reads 4 and writes 2 row-space arrays, column
+// kernel reads 4 and writes 4; a row-space array is 4 bytes per grid point, so one
+// step moves 56 bytes per point.
+#include "fft_core.cuh"
+#include "pfc_internal.h"
+
+namespace pfc {
+
+constexpr int TILE = 8192;  // complex elements per CTA tile in shared memory (64 KB in FP32)
+
+template <int M> struct RowCfg {
+    static constexpr int RPC = (TILE / 2) / M >= 1 ? (TILE / 2) / M : 1;  // rows per CTA
+    static constexpr int NB = 2 * RPC;
+    static constexpr int NT = (NB * M / 16) < 512 ? (NB * M / 16) : 512;
+};
+
+template <int L> struct ColCfg {
+    static constexpr int C = (TILE / L) > 16 ? 16 : (TILE / L);  // packed columns per CTA
+    static constexpr int NT = (C * L / 16) < 512 ? (C * L / 16) : 512;
+    static constexpr int PER = (C * L) / NT;  // complex values each thread parks
+};
+
+__device__ __forceinline__ float c2eval(const C2Params &p, float ks) {
+    const float s = sqrtf(ks);
+    if (s <= p.kc) {
+        const float d = s - p.k1;
+        return p.e1 * expf(-d * d * p.i1);
+    }
+    const float d = s - p.k2;
+    return p.e2 * expf(-d * d * p.i2);
+}
+
+// Nonlinear chemical-potential terms at one grid point (MIS:773-874), FP32.
+struct PointTerms {
+    float inn, inc;
+};
+__device__ __forceinline__ PointTerms point_terms(const ModelCoefs &k, float inv_c0, float inv_1mc0, float psi,
+                                                   float c, float a, float b) {
+    const float psi2 = psi * psi;
+    const float in1 = -k.niu * psi2 * 0.5f + k.ksi * psi2 * psi * (1.0f / 3.0f);
+    const float lc = logf(c * inv_c0);
+    const float omc = 1.0f - c;
+    const float l1c = logf(omc * inv_1mc0);
+    const float in2 = k.para_w * (c * lc + omc * l1c);
+    const float c2 = c * c, omc2 = omc * omc;
+    const float in3 = -(1.0f - 3.0f * c2 + 2.0f * c2 * c) * a - (1.0f - 3.0f * omc2 + 2.0f * omc2 * omc) * b;
+    const float wp = k.para_w * (psi + 1.0f);
+    PointTerms t;
+    t.inn = in1 + in2 + in3;
+    t.inc = wp * (lc - l1c) - 3.0f * psi * (a - b) * (c2 - c);
+    return t;
+}
+
+// Hermitian separation of Z = FFT(x + i y) into X[k], Y[k] (k = 0..M/2).
+__device__ __forceinline__ void separate(float2 zk, float2 zm, float2 &X, float2 &Y) {
+    X = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+    Y = make_float2(0.5f * (zk.y + zm.y), 0.5f * (zm.x - zk.x));
+}
+
+// Write Z[k], Z[M-k] of Z = IFFT-input for real pair (x, y) from half spectra X, Y.
+__device__ __forceinline__ void build_pair(float2 *s, int NB, int b, int k, int M, float2 X, float2 Y) {
+    const int H = M / 2;
+    if (k == 0 || k == H) {
+        s[k * NB + b] = make_float2(X.x, Y.x);
+    } else {
+        s[k * NB + b] = make_float2(X.x - Y.y, X.y + Y.x);
+        s[(M - k) * NB + b] = make_float2(X.x + Y.y, Y.x - X.y);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Row kernel: 4 row-space arrays in, 2 out.
+// ---------------------------------------------------------------------------
+template <int M>
+__global__ void __launch_bounds__(RowCfg<M>::NT) k_row_step(const RunDesc *__restrict__ runs,
+                                                             const float2 *__restrict__ tw) {
+    constexpr int RPC = RowCfg<M>::RPC, NB = RowCfg<M>::NB, NT = RowCfg<M>::NT, H = M / 2;
+    extern __shared__ float2 s[];
+    const RunDesc &d = runs[blockIdx.y];
+    const int L = d.L, Hp = d.Hp;
+    const int l0 = blockIdx.x * RPC;
+    for (int w = threadIdx.x; w < RPC * (H + 1); w += NT) {
+        const int r = w / (H + 1), k = w - r * (H + 1), l = l0 + r;
+        float2 P = make_float2(0.f, 0.f), Cc = P, A = P, B = P;
+        if (l < L) {
+            const size_t o = (size_t)l * Hp + k;
+            P = d.psi[o];
+            Cc = d.con[o];
+            A = d.ca[o];
+            B = d.cb[o];
+        }
+        build_pair(s, NB, 2 * r, k, M, P, Cc);
+        build_pair(s, NB, 2 * r + 1, k, M, A, B);
+    }
+    __syncthreads();
+    fft_smem<M, NB, NT, false>(s, tw);
+
+    constexpr int PTS = (RPC * M + NT - 1) / NT;
+    const float invM = 1.0f / (float)M;
+    const float inv_c0 = 1.0f / d.k.para_c0, inv_1mc0 = 1.0f / (1.0f - d.k.para_c0);
+    float2 out[PTS];
+#pragma unroll
+    for (int q = 0; q < PTS; ++q) {
+        const int w = threadIdx.x + q * NT;
+        if (w < RPC * M) {
+            const int r = w % RPC, m = w / RPC;
+            const float2 z1 = s[m * NB + 2 * r], z2 = s[m * NB + 2 * r + 1];
+            const float psi = z1.x * invM + d.psi_mean_f, c = z1.y * invM + d.con_mean_f;
+            const PointTerms t = point_terms(d.k, inv_c0, inv_1mc0, psi, c, z2.x * invM, z2.y * invM);
+            out[q] = make_float2(t.inn, t.inc);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < PTS; ++q) {
+        const int w = threadIdx.x + q * NT;
+        if (w < RPC * M) s[w] = out[q];  // w = m*RPC + r: interleaved layout with NB' = RPC
+    }
+    __syncthreads();
+    fft_smem<M, RPC, NT, true>(s, tw);
+    for (int w = threadIdx.x; w < RPC * (H + 1); w += NT) {
+        const int r = w / (H + 1), k = w - r * (H + 1), l = l0 + r;
+        if (l >= L) continue;
+        float2 X, Y;
+        separate(s[k * RPC + r], s[((M - k) & (M - 1)) * RPC + r], X, Y);
+        const size_t o = (size_t)l * Hp + k;
+        d.inn[o] = X;
+        d.inc[o] = Y;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Row forward: real psi/con (FP32, [L][M]) minus their FP64 means -> row space.
+// ---------------------------------------------------------------------------
+template <int M>
+__global__ void __launch_bounds__(RowCfg<M>::NT) k_row_forward(const RunDesc *__restrict__ runs,
+                                                                const float2 *__restrict__ tw) {
+    constexpr int RPC = RowCfg<M>::RPC, NT = RowCfg<M>::NT, H = M / 2;
+    extern __shared__ float2 s[];
+    const RunDesc &d = runs[blockIdx.y];
+    const int L = d.L, Hp = d.Hp;
+    const int l0 = blockIdx.x * RPC;
+    for (int w = threadIdx.x; w < RPC * M; w += NT) {
+        const int r = w % RPC, m = w / RPC, l = l0 + r;
+        float2 z = make_float2(0.f, 0.f);
+        if (l < L) {
+            const size_t o = (size_t)l * M + m;
+            z = make_float2((float)((double)d.psi_real[o] - d.psi_mean), (float)((double)d.con_real[o] - d.con_mean));
+        }
+        s[w] = z;
+    }
+    __syncthreads();
+    fft_smem<M, RPC, NT, true>(s, tw);
+    for (int w = threadIdx.x; w < RPC * (H + 1); w += NT) {
+        const int r = w / (H + 1), k = w - r * (H + 1), l = l0 + r;
+        if (l >= L) continue;
+        float2 X, Y;
+        separate(s[k * RPC + r], s[((M - k) & (M - 1)) * RPC + r], X, Y);
+        const size_t o = (size_t)l * Hp + k;
+        d.psi[o] = X;
+        d.con[o] = Y;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Column kernel.
+// ---------------------------------------------------------------------------
+template <int L, int C, int NT>
+__device__ __forceinline__ void tile_load(float2 *s, const float2 *__restrict__ g, int Hp, int c0) {
+    for (int e = threadIdx.x; e < L * C; e += NT) {
+        const int l = e / C, c = e % C;
+        s[e] = g[(size_t)l * Hp + c0 + c];
+    }
+}
+template <int L, int C, int NT>
+__device__ __forceinline__ void tile_store(const float2 *s, float2 *__restrict__ g, int Hp, int c0, int H) {
+    for (int e = threadIdx.x; e < L * C; e += NT) {
+        const int l = e / C, c = e % C;
+        if (c0 + c <= H) g[(size_t)l * Hp + c0 + c] = s[e];
+    }
+}
+
+template <int L, int MODE>
+__global__ void __launch_bounds__(ColCfg<L>::NT) k_col_step(const RunDesc *__restrict__ runs,
+                                                             const float2 *__restrict__ tw) {
+    constexpr int C = ColCfg<L>::C, NT = ColCfg<L>::NT, PER = ColCfg<L>::PER;
+    extern __shared__ float2 s[];
+    const RunDesc &d = runs[blockIdx.y];
+    const int Hp = d.Hp, H = d.M / 2;
+    const int c0 = blockIdx.x * C;
+    const float invL = 1.0f / (float)L;
+    const float mn_dt = d.k.dynamic_mn * d.dt, mc_dt = d.k.dynamic_mc * d.dt;
+    const float mc_dt_alpha = mc_dt * d.k.para_alpha;
+    float2 park[PER];
+
+    // ---- phi: forward column FFT ----
+    tile_load<L, C, NT>(s, d.psi, Hp, c0);
+    __syncthreads();
+    fft_smem<L, C, NT, true>(s, tw);
+#pragma unroll
+    for (int i = 0; i < PER; ++i) park[i] = s[threadIdx.x + i * NT];
+    __syncthreads();
+    if (MODE != COL_PREPARE) {
+        tile_load<L, C, NT>(s, d.inn, Hp, c0);
+        __syncthreads();
+        fft_smem<L, C, NT, true>(s, tw);
+    }
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        const int e = threadIdx.x + i * NT, l = e / C, km = c0 + e % C;
+        float2 v = park[i];
+        if (MODE != COL_PREPARE) {
+            const float kl = d.krefl[l], kmv = km <= H ? d.krefm[km] : 0.0f;
+            const float ks = kl * kl + kmv * kmv;
+            const float an = mn_dt * ks;
+            const float den = (float)(1.0 / (1.0 + (double)an));
+            const float2 nh = s[e];
+            v = make_float2((v.x - an * nh.x) * den, (v.y - an * nh.y) * den);
+        }
+        if (l == 0 && km == 0) v = make_float2(0.f, 0.f);
+        park[i] = cscale(v, invL);
+    }
+    if (MODE != COL_PREPARE) {
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < PER; ++i) s[threadIdx.x + i * NT] = park[i];
+        __syncthreads();
+        fft_smem<L, C, NT, false>(s, tw);
+        tile_store<L, C, NT>(s, d.psi, Hp, c0, H);
+    }
+    // ---- c2a, c2b ----
+#pragma unroll
+    for (int pass = 0; pass < 2; ++pass) {
+        __syncthreads();
+        const C2Params &cp = pass == 0 ? d.c2a : d.c2b;
+#pragma unroll
+        for (int i = 0; i < PER; ++i) {
+            const int e = threadIdx.x + i * NT, l = e / C, km = c0 + e % C;
+            const float kl = d.krefl[l], kmv = km <= H ? d.krefm[km] : 0.0f;
+            s[e] = cscale(park[i], c2eval(cp, kl * kl + kmv * kmv));
+        }
+        __syncthreads();
+        fft_smem<L, C, NT, false>(s, tw);
+        tile_store<L, C, NT>(s, pass == 0 ? d.ca : d.cb, Hp, c0, H);
+    }
+    if (MODE == COL_PREPARE) return;
+
+    // ---- con ----
+    __syncthreads();
+    tile_load<L, C, NT>(s, d.con, Hp, c0);
+    __syncthreads();
+    fft_smem<L, C, NT, true>(s, tw);
+#pragma unroll
+    for (int i = 0; i < PER; ++i) park[i] = s[threadIdx.x + i * NT];
+    __syncthreads();
+    tile_load<L, C, NT>(s, d.inc, Hp, c0);
+    __syncthreads();
+    fft_smem<L, C, NT, true>(s, tw);
+#pragma unroll
+    for (int i = 0; i < PER; ++i) {
+        const int e = threadIdx.x + i * NT, l = e / C, km = c0 + e % C;
+        const float kl = d.krefl[l], kmv = km <= H ? d.krefm[km] : 0.0f;
+        const float ks = kl * kl + kmv * kmv;
+        const float ac = mc_dt * ks;
+        const float dc = mc_dt_alpha * ks * ks;
+        const float den = (float)(1.0 / (1.0 + (double)dc));
+        const float2 ih = s[e];
+        float2 v = make_float2((park[i].x - ac * ih.x) * den, (park[i].y - ac * ih.y) * den);
+        if (l == 0 && km == 0) v = make_float2(0.f, 0.f);
+        park[i] = cscale(v, invL);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < PER; ++i) s[threadIdx.x + i * NT] = park[i];
+    __syncthreads();
+    fft_smem<L, C, NT, false>(s, tw);
+    tile_store<L, C, NT>(s, d.con, Hp, c0, H);
+    if (MODE == COL_STEP_CHECKPOINT) {
+        // gradient of con: -i k con^ along l (gra1) and m (gra2), MIS:884-889
+#pragma unroll
+        for (int pass = 0; pass < 2; ++pass) {
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < PER; ++i) {
+                const int e = threadIdx.x + i * NT, l = e / C, km = c0 + e % C;
+                const float kv = pass == 0 ? d.krefl[l] : (km <= H ? d.krefm[km] : 0.0f);
+                s[e] = make_float2(kv * park[i].y, -kv * park[i].x);
+            }
+            __syncthreads();
+            fft_smem<L, C, NT, false>(s, tw);
+            tile_store<L, C, NT>(s, pass == 0 ? d.gx : d.gy, Hp, c0, H);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Analysis row kernel (checkpoints): real fields, energy density and mass.
+// ENERGYC2 (MIS:1043-1092): float energy terms, double accumulation.
+// ---------------------------------------------------------------------------
+template <int M>
+__global__ void __launch_bounds__(RowCfg<M>::NT) k_row_analysis(const RunDesc *__restrict__ runs,
+                                                                 const float2 *__restrict__ tw) {
+    constexpr int RPC = RowCfg<M>::RPC, NT = RowCfg<M>::NT, H = M / 2;
+    constexpr int NB = 3 * RPC;
+    extern __shared__ float2 s[];
+    __shared__ double red[2][32];
+    const RunDesc &d = runs[blockIdx.y];
+    const int L = d.L, Hp = d.Hp;
+    const int l0 = blockIdx.x * RPC;
+    for (int w = threadIdx.x; w < RPC * (H + 1); w += NT) {
+        const int r = w / (H + 1), k = w - r * (H + 1), l = l0 + r;
+        float2 z[6];
+#pragma unroll
+        for (int j = 0; j < 6; ++j) z[j] = make_float2(0.f, 0.f);
+        if (l < L) {
+            const size_t o = (size_t)l * Hp + k;
+            z[0] = d.psi[o];
+            z[1] = d.con[o];
+            z[2] = d.ca[o];
+            z[3] = d.cb[o];
+            z[4] = d.gx[o];
+            z[5] = d.gy[o];
+        }
+        build_pair(s, NB, 3 * r, k, M, z[0], z[1]);
+        build_pair(s, NB, 3 * r + 1, k, M, z[2], z[3]);
+        build_pair(s, NB, 3 * r + 2, k, M, z[4], z[5]);
+    }
+    __syncthreads();
+    fft_smem<M, NB, NT, false>(s, tw);
+    const float invM = 1.0f / (float)M;
+    const ModelCoefs &k = d.k;
+    const float inv_c0 = 1.0f / k.para_c0, inv_1mc0 = 1.0f / (1.0f - k.para_c0);
+    double acc_e = 0.0, acc_m = 0.0;
+    for (int w = threadIdx.x; w < RPC * M; w += NT) {
+        const int r = w % RPC, m = w / RPC, l = l0 + r;
+        if (l >= L) continue;
+        const float2 z1 = s[m * NB + 3 * r], z2 = s[m * NB + 3 * r + 1], z3 = s[m * NB + 3 * r + 2];
+        const float psi = z1.x * invM + d.psi_mean_f, c = z1.y * invM + d.con_mean_f;
+        const float a = z2.x * invM, b = z2.y * invM, gx = z3.x * invM, gy = z3.y * invM;
+        d.psi_real[(size_t)l * M + m] = psi;
+        d.con_real[(size_t)l * M + m] = c;
+        const float psi2 = psi * psi;
+        const float e_id = psi2 * 0.5f - k.niu * psi2 * psi * (1.0f / 6.0f) + k.ksi * psi2 * psi2 * (1.0f / 12.0f);
+        const float lc = logf(c * inv_c0), omc = 1.0f - c, l1c = logf(omc * inv_1mc0);
+        const float e_mix = (psi + 1.0f) * k.para_w * (c * lc + omc * l1c);
+        const float c2 = c * c, omc2 = omc * omc;
+        const float in3 = -(1.0f - 3.0f * c2 + 2.0f * c2 * c) * a - (1.0f - 3.0f * omc2 + 2.0f * omc2 * omc) * b;
+        const float e_ex = 0.5f * psi * in3 + k.para_alpha * (gx * gx + gy * gy + gy * gy);
+        acc_e += (double)(e_id + e_mix + e_ex);
+        acc_m += (double)psi;
+    }
+    // deterministic block reduction
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        acc_e += __shfl_down_sync(0xffffffffu, acc_e, off);
+        acc_m += __shfl_down_sync(0xffffffffu, acc_m, off);
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        red[0][warp] = acc_e;
+        red[1][warp] = acc_m;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double se = 0.0, sm = 0.0;
+        for (int i = 0; i < NT / 32; ++i) {
+            se += red[0][i];
+            sm += red[1][i];
+        }
+        d.partials[2 * blockIdx.x] = se;
+        d.partials[2 * blockIdx.x + 1] = sm;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+static int log2i(int n) {
+    int l = 0;
+    while ((1 << l) < n) ++l;
+    return l;
+}
+
+// Opt in to more than 48 KB of dynamic shared memory, once per kernel and device
+// (the attribute call is not a stream operation, so it is also done before any
+// graph capture through prepare_size()).
+template <typename K> static cudaError_t set_smem(K kernel, size_t bytes, unsigned &mask) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (mask & (1u << dev)) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) mask |= 1u << dev;
+    return e;
+}
+
+template <int M>
+static cudaError_t row_step_impl(const RunDesc *d_runs, int nruns, int L, const TwiddleSet &tw, cudaStream_t st) {
+    constexpr int RPC = RowCfg<M>::RPC, NT = RowCfg<M>::NT;
+    const size_t smem = sizeof(float2) * RowCfg<M>::NB * M;
+    static unsigned mask = 0;
+    cudaError_t e = set_smem(k_row_step<M>, smem, mask);
+    if (nruns == 0) return e;
+    if (e != cudaSuccess) return e;
+    dim3 grid((L + RPC - 1) / RPC, nruns);
+    k_row_step<M><<<grid, NT, smem, st>>>(d_runs, tw.f32[log2i(M)]);
+    return cudaGetLastError();
+}
+
+template <int M>
+static cudaError_t row_forward_impl(const RunDesc *d_runs, int nruns, int L, const TwiddleSet &tw, cudaStream_t st) {
+    constexpr int RPC = RowCfg<M>::RPC, NT = RowCfg<M>::NT;
+    const size_t smem = sizeof(float2) * RPC * M;
+    static unsigned mask = 0;
+    cudaError_t e = set_smem(k_row_forward<M>, smem, mask);
+    if (nruns == 0) return e;
+    if (e != cudaSuccess) return e;
+    dim3 grid((L + RPC - 1) / RPC, nruns);
+    k_row_forward<M><<<grid, NT, smem, st>>>(d_runs, tw.f32[log2i(M)]);
+    return cudaGetLastError();
+}
+
+template <int M>
+static cudaError_t row_analysis_impl(const RunDesc *d_runs, int nruns, int L, const TwiddleSet &tw,
+                                     cudaStream_t st) {
+    constexpr int RPC = RowCfg<M>::RPC, NT = RowCfg<M>::NT;
+    const size_t smem = sizeof(float2) * 3 * RPC * M;
+    static unsigned mask = 0;
+    cudaError_t e = set_smem(k_row_analysis<M>, smem, mask);
+    if (nruns == 0) return e;
+    if (e != cudaSuccess) return e;
+    dim3 grid((L + RPC - 1) / RPC, nruns);
+    k_row_analysis<M><<<grid, NT, smem, st>>>(d_runs, tw.f32[log2i(M)]);
+    return cudaGetLastError();
+}
+
+template <int L, int MODE>
+static cudaError_t col_impl(const RunDesc *d_runs, int nruns, int M, const TwiddleSet &tw, cudaStream_t st) {
+    constexpr int C = ColCfg<L>::C, NT = ColCfg<L>::NT;
+    const size_t smem = sizeof(float2) * C * L;
+    static unsigned mask = 0;
+    cudaError_t e = set_smem(k_col_step<L, MODE>, smem, mask);
+    if (nruns == 0) return e;
+    if (e != cudaSuccess) return e;
+    const int H = M / 2;
+    dim3 grid((H + 1 + C - 1) / C, nruns);
+    k_col_step<L, MODE><<<grid, NT, smem, st>>>(d_runs, tw.f32[log2i(L)]);
+    return cudaGetLastError();
+}
+
+#define PFC_SIZE_SWITCH(n, FN, ...)             \
+    switch (n) {                                \
+        case 32: return FN<32>(__VA_ARGS__);    \
+        case 64: return FN<64>(__VA_ARGS__);    \
+        case 128: return FN<128>(__VA_ARGS__);  \
+        case 256: return FN<256>(__VA_ARGS__);  \
+        case 512: return FN<512>(__VA_ARGS__);  \
+        case 1024: return FN<1024>(__VA_ARGS__); \
+        case 2048: return FN<2048>(__VA_ARGS__); \
+        default: return cudaErrorInvalidValue;  \
+    }
+
+cudaError_t launch_row_step(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw, cudaStream_t s) {
+    PFC_SIZE_SWITCH(M, row_step_impl, d_runs, nruns, L, tw, s)
+}
+
+cudaError_t launch_row_forward(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw, cudaStream_t s) {
+    PFC_SIZE_SWITCH(M, row_forward_impl, d_runs, nruns, L, tw, s)
+}
+
+cudaError_t launch_row_analysis(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw,
+                                cudaStream_t s) {
+    PFC_SIZE_SWITCH(M, row_analysis_impl, d_runs, nruns, L, tw, s)
+}
+
+template <int L>
+static cudaError_t col_dispatch(const RunDesc *d_runs, int nruns, int M, int mode, const TwiddleSet &tw,
+                                cudaStream_t s) {
+    switch (mode) {
+        case COL_STEP: return col_impl<L, COL_STEP>(d_runs, nruns, M, tw, s);
+        case COL_PREPARE: return col_impl<L, COL_PREPARE>(d_runs, nruns, M, tw, s);
+        case COL_STEP_CHECKPOINT: return col_impl<L, COL_STEP_CHECKPOINT>(d_runs, nruns, M, tw, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_col_step(const RunDesc *d_runs, int nruns, int L, int M, int mode, const TwiddleSet &tw,
+                            cudaStream_t s) {
+    PFC_SIZE_SWITCH(L, col_dispatch, d_runs, nruns, M, mode, tw, s)
+}
+
+cudaError_t prepare_size(int L, int M) {
+    // nruns == 0: only the shared-memory attributes are set, nothing is launched
+    TwiddleSet none{};
+    cudaError_t e;
+    if ((e = launch_row_step(nullptr, 0, L, M, none, 0)) != cudaSuccess) return e;
+    if ((e = launch_row_forward(nullptr, 0, L, M, none, 0)) != cudaSuccess) return e;
+    if ((e = launch_row_analysis(nullptr, 0, L, M, none, 0)) != cudaSuccess) return e;
+    for (int mode = 0; mode < 3; ++mode)
+        if ((e = launch_col_step(nullptr, 0, L, M, mode, none, 0)) != cudaSuccess) return e;
+    return cudaSuccess;
+}
+
+int analysis_partials(int L, int M) {
+    int rpc = (TILE / 2) / M;
+    if (rpc < 1) rpc = 1;
+    return (L + rpc - 1) / rpc;
+}
+
+}  // namespace pfc

@@ -1,0 +1,281 @@
+"""ctypes binding of libpfc_b200.so (the C ABI declared in include/pfc_b200.h).
+
+This is the Python view of the same entry points a C/C++ caller links against.
+Importing it does not need a GPU; creating a run does.  There is no fallback:
+if the shared library is missing, :func:`lib` raises, and every call that fails
+on the device raises :class:`PfcError` with the library's message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG_DIR)
+LIB_PATH = os.path.join(ROOT, "lib", "libpfc_b200.so")
+CLI_PATH = os.path.join(ROOT, "bin", "pfc-exp-cli")
+HEADER_PATH = os.path.join(os.path.dirname(ROOT), "include", "pfc_b200.h")
+
+MODEL_MISFIT = 0
+MODEL_CVD = 1
+FP32 = 0
+FP64 = 1
+FP64_PURE = 2
+
+PFC_OK = 0
+
+
+class PfcError(RuntimeError):
+    pass
+
+
+class RunParams(C.Structure):
+    _fields_ = [
+        ("model", C.c_int),
+        ("L", C.c_int),
+        ("M", C.c_int),
+        ("N", C.c_int),
+        ("u0", C.c_float),
+        ("con0", C.c_float),
+        ("sig", C.c_float),
+        ("dt", C.c_float),
+        ("dx", C.c_float),
+        ("axx", C.c_float),
+        ("grainx", C.c_int),
+        ("grainy", C.c_int),
+        ("grainz", C.c_int),
+        ("seed", C.c_uint32),
+        ("precision", C.c_int),
+        ("device", C.c_int),
+    ]
+
+
+_lib = None
+
+
+def build(jobs: int = 8) -> str:
+    """Compile the library and the CLI with this package's Makefile (sm_100a)."""
+    subprocess.run(["make", "-s", "-j", str(jobs), "-C", ROOT], check=True)
+    return LIB_PATH
+
+
+def lib():
+    """Load libpfc_b200.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise PfcError(f"libpfc_b200.so not built ({LIB_PATH}); run `make -C {ROOT}`")
+    L = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    vp, dp, fp = C.c_void_p, P(C.c_double), P(C.c_float)
+    sig = {
+        "pfc_last_error": ([], C.c_char_p),
+        "pfc_default_params": ([C.c_int, P(RunParams)], C.c_int),
+        "pfc_run_create": ([P(RunParams), P(vp)], C.c_int),
+        "pfc_run_destroy": ([vp], C.c_int),
+        "pfc_run_advance": ([vp, C.c_int, C.c_int], C.c_int),
+        "pfc_run_steps": ([vp, P(C.c_int)], C.c_int),
+        "pfc_run_get_fields": ([vp, dp, dp], C.c_int),
+        "pfc_run_get_fields_f32": ([vp, fp, fp], C.c_int),
+        "pfc_run_set_fields": ([vp, dp, dp], C.c_int),
+        "pfc_run_energy": ([vp, dp, dp], C.c_int),
+        "pfc_run_means": ([vp, dp, dp], C.c_int),
+        "pfc_batch_create": ([P(vp), C.c_int, P(vp)], C.c_int),
+        "pfc_batch_destroy": ([vp], C.c_int),
+        "pfc_batch_advance": ([vp, C.c_int], C.c_int),
+        "pfc_phimax_misfit": ([fp, fp, C.c_int, C.c_int, C.c_float, C.c_float, dp, C.c_int, P(C.c_int)], C.c_int),
+        "pfc_phimax_elastic": ([fp, C.c_int, C.c_int, C.c_int, C.c_float, dp, C.c_int, P(C.c_int)], C.c_int),
+        "pfc_elastic3d": ([dp, dp, dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, dp,
+                           P(C.c_uint32)], C.c_int),
+        "pfc_cryst_order": ([dp, dp, dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, dp, dp], C.c_int),
+        "pfc_dft3d": ([dp, dp, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
+        "pfc_batch_advance_timed": ([vp, C.c_int, P(C.c_float)], C.c_int),
+        "pfc_batch_kernel_times": ([vp, C.c_int, dp, dp], C.c_int),
+        "pfc_run_cli": ([C.c_int, P(C.c_char_p)], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def _check(rc: int, what: str):
+    if rc != PFC_OK:
+        msg = lib().pfc_last_error().decode(errors="replace")
+        raise PfcError(f"{what} failed ({rc}): {msg}")
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def default_params(model: int = MODEL_MISFIT, **kw) -> RunParams:
+    p = RunParams()
+    _check(lib().pfc_default_params(model, C.byref(p)), "pfc_default_params")
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class Run:
+    """One Misfit or CVD run resident on the GPU."""
+
+    def __init__(self, params: RunParams):
+        self.params = params
+        self.L, self.M, self.N = params.L, params.M, params.N
+        self.P = self.L * self.M * self.N
+        self.h = C.c_void_p()
+        _check(lib().pfc_run_create(C.byref(params), C.byref(self.h)), "pfc_run_create")
+
+    def close(self):
+        if self.h:
+            lib().pfc_run_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def advance(self, nsteps: int = 1, analysis: bool = False):
+        _check(lib().pfc_run_advance(self.h, nsteps, 1 if analysis else 0), "pfc_run_advance")
+
+    @property
+    def steps(self) -> int:
+        s = C.c_int()
+        _check(lib().pfc_run_steps(self.h, C.byref(s)), "pfc_run_steps")
+        return s.value
+
+    def fields(self):
+        phi = np.empty(self.P, np.float64)
+        con = np.empty(self.P, np.float64)
+        _check(lib().pfc_run_get_fields(self.h, _dp(phi), _dp(con)), "pfc_run_get_fields")
+        s = (self.L, self.M, self.N)
+        return phi.reshape(s), con.reshape(s)
+
+    def fields_f32(self):
+        phi = np.empty(self.P, np.float32)
+        con = np.empty(self.P, np.float32)
+        _check(lib().pfc_run_get_fields_f32(self.h, _fp(phi), _fp(con)), "pfc_run_get_fields_f32")
+        s = (self.L, self.M, self.N)
+        return phi.reshape(s), con.reshape(s)
+
+    def set_fields(self, phi, con):
+        phi = np.ascontiguousarray(phi, np.float64).ravel()
+        con = np.ascontiguousarray(con, np.float64).ravel()
+        _check(lib().pfc_run_set_fields(self.h, _dp(phi), _dp(con)), "pfc_run_set_fields")
+
+    def energy(self):
+        e, d = C.c_double(), C.c_double()
+        _check(lib().pfc_run_energy(self.h, C.byref(e), C.byref(d)), "pfc_run_energy")
+        return e.value, d.value
+
+    def means(self):
+        a, b = C.c_double(), C.c_double()
+        _check(lib().pfc_run_means(self.h, C.byref(a), C.byref(b)), "pfc_run_means")
+        return a.value, b.value
+
+
+class Batch:
+    """Runs advanced together, one launch per grid size per sweep (CUDA graph)."""
+
+    def __init__(self, runs):
+        self.runs = list(runs)
+        arr = (C.c_void_p * len(self.runs))(*[r.h.value for r in self.runs])
+        self.h = C.c_void_p()
+        _check(lib().pfc_batch_create(arr, len(self.runs), C.byref(self.h)), "pfc_batch_create")
+
+    def advance(self, nsteps: int):
+        _check(lib().pfc_batch_advance(self.h, nsteps), "pfc_batch_advance")
+
+    def advance_timed(self, nsteps: int) -> float:
+        """Advance and return the device time in ms (CUDA events on the batch stream)."""
+        ms = C.c_float()
+        _check(lib().pfc_batch_advance_timed(self.h, nsteps, C.byref(ms)), "pfc_batch_advance_timed")
+        return ms.value
+
+    def kernel_times(self, reps: int):
+        """Mean device ms of the row-kernel and column-kernel launches of one step."""
+        a, b = C.c_double(), C.c_double()
+        _check(lib().pfc_batch_kernel_times(self.h, reps, C.byref(a), C.byref(b)), "pfc_batch_kernel_times")
+        return a.value, b.value
+
+    def close(self):
+        if self.h:
+            lib().pfc_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def phimax_misfit(phi, con, dx=0.125, con0=0.2):
+    phi = np.ascontiguousarray(phi, np.float32)
+    con = np.ascontiguousarray(con, np.float32)
+    L, M = phi.shape[0], phi.shape[1]
+    cap = L * M + 1
+    out = np.zeros((cap, 5), np.float64)
+    n = C.c_int()
+    _check(lib().pfc_phimax_misfit(_fp(phi), _fp(con), L, M, dx, con0, _dp(out), cap, C.byref(n)), "pfc_phimax_misfit")
+    return out[: n.value].copy()
+
+
+def phimax_elastic(phi, dx=0.125):
+    phi = np.ascontiguousarray(phi, np.float32)
+    L, M, N = phi.shape
+    cap = L * M * N + 1
+    out = np.zeros((cap, 4), np.float64)
+    n = C.c_int()
+    _check(lib().pfc_phimax_elastic(_fp(phi), L, M, N, dx, _dp(out), cap, C.byref(n)), "pfc_phimax_elastic")
+    return out[: n.value].copy()
+
+
+def elastic3d(x, y, z, L, M, N, dx=0.125, benchel=1.7):
+    x, y, z = (np.ascontiguousarray(a, np.float64) for a in (x, y, z))
+    n = len(x)
+    strain = np.zeros(n, np.float64)
+    nb = np.zeros(n, np.uint32)
+    _check(lib().pfc_elastic3d(_dp(x), _dp(y), _dp(z), n, L, M, N, dx, benchel, _dp(strain),
+                               nb.ctypes.data_as(C.POINTER(C.c_uint32))), "pfc_elastic3d")
+    return strain, nb
+
+
+def cryst_order(x, y, z, L, M, N, dx=0.125):
+    x, y, z = (np.ascontiguousarray(a, np.float64) for a in (x, y, z))
+    n = len(x)
+    q4 = np.zeros(n, np.float64)
+    q6 = np.zeros(n, np.float64)
+    _check(lib().pfc_cryst_order(_dp(x), _dp(y), _dp(z), n, L, M, N, dx, _dp(q4), _dp(q6)), "pfc_cryst_order")
+    return q4, q6
+
+
+def dft3d(a, sign=-1):
+    """3-D complex-double DFT on the GPU with FFTW's conventions (unnormalised)."""
+    a = np.ascontiguousarray(a, np.complex128)
+    out = np.empty_like(a)
+    n0, n1, n2 = a.shape
+    _check(lib().pfc_dft3d(a.ctypes.data_as(C.POINTER(C.c_double)), out.ctypes.data_as(C.POINTER(C.c_double)),
+                           n0, n1, n2, sign), "pfc_dft3d")
+    return out
+
+
+def header_functions(path: str = HEADER_PATH):
+    """Names of the functions declared in include/pfc_b200.h."""
+    import re
+    txt = open(path).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(pfc_[a-z0-9_]+)\s*\(", txt)))

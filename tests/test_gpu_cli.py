@@ -1,0 +1,154 @@
+"""The pfc-exp-cli drop-in: same flags, files, progress lines and exit codes.
+
+Runs bin/pfc-exp-cli (a thin main() over pfc_run_cli) and compares its output
+directory with the reference program's (golden fixtures): text files byte for
+byte where the values are computed identically, and field values within the
+FP32 tolerance where they come from the FP32 step.
+"""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as O
+import pfc_b200 as P
+from helpers import golden_case, read_vti
+
+CLI = P.CLI_PATH
+
+
+def run_cli(args, **kw):
+    return subprocess.run([CLI, *args], capture_output=True, text=True, timeout=600, **kw)
+
+
+def test_cli_help_and_bad_args():
+    """Exit codes and dispatch need no GPU (main_cli.cpp:24-88, MIS:306-308)."""
+    r = run_cli(["--help"])
+    assert r.returncode == 0 and "Models:" in r.stderr
+    r = run_cli(["--model", "misfit", "--help"])
+    assert r.returncode == 0 and "--grainx" in r.stderr
+    r = run_cli(["--model", "nope"])
+    assert r.returncode == 2 and "Unknown model: nope" in r.stderr
+    r = run_cli(["--model", "misfit", "--bogus", "1"])
+    assert r.returncode == 2 and "Unknown option: --bogus" in r.stderr
+    r = run_cli(["--model", "misfit", "--steps", "0"])
+    assert r.returncode == 2 and "--steps must be > 0" in r.stderr
+    r = run_cli(["--model", "cvd", "--mod", "-1"])
+    assert r.returncode == 2 and "Invalid parameter values" in r.stderr
+    r = run_cli(["--model"])
+    assert r.returncode == 2
+
+
+@pytest.mark.gpu
+def test_cli_misfit_matches_reference(tmp_path):
+    d, meta, fields = golden_case("misfit_64")
+    out = tmp_path / "run"
+    r = run_cli(["--model", "misfit", "--grid", "64x64x1", *meta["args"], "--outdir", str(out)])
+    assert r.returncode == 0, r.stderr
+    # progress lines as the GUI parses them (MainWindow.cpp:3426)
+    prog = [l for l in r.stdout.splitlines() if re.match(r"^PFC_PROGRESS\s+step=(\d+)\s+total=(\d+)\s*$", l)]
+    ref_prog = [l for l in open(f"{d}/stdout.txt").read().splitlines() if l.startswith("PFC_PROGRESS")]
+    assert prog == ref_prog
+    # non-progress stdout lines: identical sequence of tags
+    tags = [re.sub(r"\d+", "#", l) for l in r.stdout.splitlines() if not l.startswith("PFC_PROGRESS")]
+    ref_tags = [re.sub(r"\d+", "#", l) for l in open(f"{d}/stdout.txt").read().splitlines()
+                if not l.startswith("PFC_PROGRESS")]
+    assert tags == ref_tags
+    assert (out / "run_config.txt").read_text() == open(f"{d}/run_config.txt").read()
+    # checkpoint files: byte-identical headers and pvti, values within the FP32 tolerance
+    for kd in (0, 25, 50):
+        for f in ("phi", "con"):
+            vals, head, nbytes = read_vti(out / f"{f}_{kd}_0.vti")
+            ref = fields[f"{f}_{kd}"]
+            if kd == 0:
+                assert np.array_equal(vals, ref)
+            else:
+                assert np.abs(vals - ref).max() <= 1e-5
+            if os.path.exists(f"{d}/{f}_{kd}_0.vti"):
+                _, rhead, rbytes = read_vti(f"{d}/{f}_{kd}_0.vti")
+                assert head == rhead and nbytes == rbytes
+                assert (out / f"{f}_{kd}.pvti").read_text() == open(f"{d}/{f}_{kd}.pvti").read()
+                raw = (out / f"{f}_{kd}_0.vti").read_bytes()
+                rraw = open(f"{d}/{f}_{kd}_0.vti", "rb").read()
+                assert len(raw) == len(rraw) and raw[-40:] == rraw[-40:]
+    # energy.txt: same lines (steps) and values within tolerance
+    got = [l.split() for l in (out / "energy.txt").read_text().splitlines()]
+    ref = [l.split() for l in open(f"{d}/energy.txt").read().splitlines()]
+    assert [g[0] for g in got] == [r_[0] for r_ in ref]
+    for g, r_ in zip(got, ref):
+        assert abs(float(g[1]) - float(r_[1])) <= 1e-5 * abs(float(r_[1]))
+        assert abs(float(g[2]) - float(r_[2])) <= 1e-6
+    # Phimax: same atoms (count, ordering) within the FP32 field tolerance
+    for kd in (25, 50):
+        a = np.loadtxt(out / f"Phimax_{kd}.txt", skiprows=2)
+        b = np.loadtxt(f"{d}/Phimax_{kd}.txt", skiprows=2)
+        assert a.shape == b.shape
+        assert np.abs(a - b).max() <= 2e-3
+    ts = (out / "checkpoint_timestamps.txt").read_text().splitlines()
+    assert ts[0].startswith("# Checkpoint timestamps") and [l.split()[1] for l in ts[1:]] == ["25", "50"]
+
+
+@pytest.mark.gpu
+def test_cli_elastic_on_reference_checkpoints(tmp_path):
+    """Elastic Analysis on the reference's own VTI files: text outputs byte-identical
+    (Phimax, strain), q4q6 within the cryst_order tolerance."""
+    d, meta, fields = golden_case("misfit_64")
+    inp = tmp_path / "in"
+    inp.mkdir()
+    # write the reference checkpoints back out with the reference's byte layout
+    for kd in (25, 50):
+        for f in ("phi", "con"):
+            arr = fields[f"{f}_{kd}"]
+            L, M, N = arr.shape
+            raw = open(f"{d}/{f}_25_0.vti", "rb").read()
+            i = raw.index(b"_", raw.index(b"<AppendedData"))
+            body = arr.transpose(2, 1, 0).astype(np.float32).tobytes()
+            (inp / f"{f}_{kd}_0.vti").write_bytes(raw[:i + 5] + body + raw[i + 5 + len(body):])
+    for k, extra in enumerate([[], ["--benchel", "1.3"]]):
+        out = tmp_path / f"el{k}"
+        r = run_cli(["--model", "elastic", "--input-dir", str(inp), "--outdir", str(out), *extra])
+        assert r.returncode == 0, r.stderr
+        assert "PFC_PROGRESS step=2 total=2" in r.stderr
+        for kd in (25, 50):
+            for f in ("Phimax", "strain"):
+                assert (out / f"{f}_{kd}.txt").read_text() == open(f"{d}/elastic{k}/{f}_{kd}.txt").read()
+            a = np.loadtxt(out / f"q4q6_{kd}.txt", skiprows=2, usecols=(1, 2, 3, 4, 5))
+            b = np.loadtxt(f"{d}/elastic{k}/q4q6_{kd}.txt", skiprows=2, usecols=(1, 2, 3, 4, 5))
+            assert a.shape == b.shape and np.abs(a - b).max() <= 1.01e-4
+
+
+@pytest.mark.gpu
+def test_cli_elastic_missing_input_exits_2(tmp_path):
+    r = run_cli(["--model", "elastic", "--input-dir", str(tmp_path / "none"), "--outdir", str(tmp_path / "o"),
+                 "--steps", "10", "--mod", "5"])
+    assert r.returncode == 2 and "can't open input file" in r.stderr
+
+
+@pytest.mark.gpu
+def test_cli_cvd_matches_reference(tmp_path):
+    d, meta, fields = golden_case("cvd_64")
+    out = tmp_path / "cvd"
+    r = run_cli(["--model", "cvd", "--grid", "64x64x1", *meta["args"], "--outdir", str(out)])
+    assert r.returncode == 0, r.stderr
+    assert r.stderr.count("PFC_PROGRESS") == 21
+    for kd in (0, 10, 20):
+        vals, _, _ = read_vti(out / f"phi_{kd}_0.vti")
+        assert np.abs(vals - fields[f"phi_{kd}"]).max() <= 1e-5
+    got = [l.split() for l in (out / "energy.txt").read_text().splitlines()]
+    ref = [l.split() for l in open(f"{d}/energy.txt").read().splitlines()]
+    assert [g[0] for g in got] == [r_[0] for r_ in ref]
+    for g, r_ in zip(got, ref):
+        assert abs(float(g[1]) - float(r_[1])) <= 1e-5 * abs(float(r_[1])) + 1e-9
+
+
+@pytest.mark.gpu
+def test_cli_fp64_precision_3d(tmp_path):
+    d, meta, fields = golden_case("cvd_32x32x8")
+    out = tmp_path / "cvd3"
+    r = run_cli(["--model", "cvd", "--grid", "32x32x8", "--precision", "fp64", *meta["args"], "--outdir", str(out)])
+    assert r.returncode == 0, r.stderr
+    for kd in (0, 5, 10):
+        vals, _, _ = read_vti(out / f"phi_{kd}_0.vti")
+        assert np.abs(vals - fields[f"phi_{kd}"]).max() <= 1e-6

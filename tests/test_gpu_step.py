@@ -1,0 +1,186 @@
+"""GPU parity of the time step, initial conditions, FFT, mass and batching.
+
+Every test calls the CUDA engine through its C ABI (pfc_b200 ctypes binding) and
+checks it against the oracle (CPU restatement) and the reference fixtures.
+
+Tolerances:
+  * initial conditions: bit-exact (Float32) with the reference;
+  * FP32 fused path: max-abs field error <= 1e-5 after 200 steps against the FP64
+    oracle and against the reference's own run (the stated target);
+  * FP64 plain path, pure mode: <= 1e-11 against the pure-FP64 oracle (FFT algorithm
+    and libm differences only); reference-exact mode: <= 1e-6, because the
+    reference's float roundings turn last-bit double differences into occasional
+    float-ulp differences;
+  * FFT: <= 1e-12 relative to numpy.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import pfc_b200 as P
+from helpers import golden_case
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_run(model, L, M, N=1, exact=1, **kw):
+    p = O.default_params(model, L=L, M=M, N=N, exact=exact, **kw)
+    return O.Run(p)
+
+
+def gpu_run(model, L, M, N=1, precision=P.FP32, **kw):
+    p = P.default_params(model, L=L, M=M, N=N, precision=precision, **kw)
+    return P.Run(p)
+
+
+@pytest.mark.parametrize("shape", [(8, 16, 1), (64, 64, 1), (32, 32, 8), (256, 128, 1), (2, 4, 2048), (2048, 2, 1)])
+def test_dft3d_matches_numpy(shape):
+    rng = np.random.default_rng(3)
+    a = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    for sign, ref in ((-1, np.fft.fftn(a)), (1, np.fft.ifftn(a) * a.size)):
+        got = P.dft3d(a, sign)
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("name", ["misfit_64", "misfit_128_s7"])
+def test_misfit_initial_condition_bitexact(name):
+    d, meta, fields = golden_case(name)
+    L, M, N = meta["grid"]
+    kv = dict(zip(meta["args"][::2], meta["args"][1::2]))
+    kw = {}
+    if "--seed" in kv:
+        kw["seed"] = int(kv["--seed"])
+    for k in ("u0", "con0"):
+        if f"--{k}" in kv:
+            kw[k] = float(np.float32(kv[f"--{k}"]))
+    r = gpu_run(P.MODEL_MISFIT, L, M, **kw)
+    phi, con = r.fields_f32()
+    assert np.array_equal(phi.view(np.uint32), fields["phi_0"].view(np.uint32))
+    assert np.array_equal(con.view(np.uint32), fields["con_0"].view(np.uint32))
+
+
+@pytest.mark.parametrize("model,L,M", [(P.MODEL_MISFIT, 256, 256), (P.MODEL_MISFIT, 1024, 512), (P.MODEL_CVD, 128, 64),
+                                       (P.MODEL_MISFIT, 64, 2048)])
+def test_initial_condition_matches_oracle(model, L, M):
+    r = gpu_run(model, L, M)
+    o = oracle_run(model, L, M)
+    phi, con = r.fields_f32()
+    ophi, ocon = o.fields()
+    assert np.array_equal(phi, ophi.astype(np.float32))
+    assert np.array_equal(con, ocon.astype(np.float32))
+
+
+@pytest.mark.parametrize("precision,exact,tol", [(P.FP64, 1, 1e-6), (P.FP64_PURE, 0, 1e-11)])
+def test_fp64_path_matches_oracle(precision, exact, tol):
+    r = gpu_run(P.MODEL_MISFIT, 64, 64, precision=precision)
+    o = oracle_run(P.MODEL_MISFIT, 64, 64, exact=exact)
+    r.advance(20)
+    o.step(20)
+    phi, con = r.fields()
+    ophi, ocon = o.fields()
+    assert np.abs(phi - ophi).max() <= tol
+    assert np.abs(con - ocon).max() <= tol
+    e, d = r.energy()
+    oe, od = o.energy()
+    assert abs(e - oe) <= 1e3 * tol * abs(oe) + 1e-12 and abs(d - od) <= 1e-12
+
+
+def test_fp64_path_cvd_3d_matches_reference():
+    d, meta, fields = golden_case("cvd_32x32x8")
+    r = gpu_run(P.MODEL_CVD, 32, 32, 8, precision=P.FP64)
+    r.advance(1)
+    phi, con = r.fields()
+    assert np.abs(phi - fields["phi_0"]).max() <= 1e-6
+    assert np.abs(con - fields["con_0"]).max() <= 1e-6
+    r.advance(10)
+    phi, con = r.fields()
+    assert np.abs(phi - fields["phi_10"]).max() <= 1e-6
+
+
+@pytest.mark.parametrize("model,L,M,steps", [(P.MODEL_MISFIT, 64, 64, 200), (P.MODEL_MISFIT, 128, 128, 200),
+                                             (P.MODEL_MISFIT, 256, 256, 200), (P.MODEL_CVD, 64, 64, 200),
+                                             (P.MODEL_MISFIT, 128, 64, 100), (P.MODEL_MISFIT, 64, 256, 100)])
+def test_fp32_path_matches_fp64_oracle(model, L, M, steps):
+    r = gpu_run(model, L, M)
+    o = oracle_run(model, L, M, exact=0)
+    r.advance(steps, analysis=True)
+    o.step(steps)
+    phi, con = r.fields()
+    ophi, ocon = o.fields()
+    err_phi = np.abs(phi - ophi).max()
+    err_con = np.abs(con - ocon).max()
+    assert err_phi <= 1e-5, err_phi
+    assert err_con <= 1e-5, err_con
+    e, d = r.energy()
+    oe, od = o.energy()
+    assert abs(e - oe) <= 1e-5 * abs(oe) + 1e-7
+    assert abs(d - od) <= 1e-7
+
+
+def test_fp32_c1_matches_reference_run():
+    """C1: Misfit 256^2, 200 steps, against the reference program's own checkpoint."""
+    d, meta, fields = golden_case("misfit_256_c1")
+    r = gpu_run(P.MODEL_MISFIT, 256, 256, seed=20200604, u0=0.05, con0=0.2)
+    r.advance(25, analysis=True)
+    phi, con = r.fields_f32()
+    assert np.abs(phi - fields["phi_25"]).max() <= 1e-5
+    r.advance(175, analysis=True)
+    phi, con = r.fields_f32()
+    assert np.abs(phi - fields["phi_200"]).max() <= 1e-5
+    assert np.abs(con - fields["con_200"]).max() <= 1e-5
+    lines = open(f"{d}/energy.txt").read().split()
+    e_ref, m_ref = float(lines[-2]), float(lines[-1])
+    e, m = r.energy()
+    assert abs(e - e_ref) <= 2e-5 * abs(e_ref)
+    assert abs(m - m_ref) <= 1e-6
+
+
+def test_mass_is_conserved():
+    r = gpu_run(P.MODEL_MISFIT, 256, 256)
+    m0 = r.means()
+    r.advance(500, analysis=True)
+    assert r.means() == m0  # the FP64 k = 0 modes are exact invariants of the step
+    _, mass = r.energy()
+    assert abs(mass - m0[0]) <= 1e-9 * abs(m0[0]) + 1e-12  # FP64 reduction of the FP32 field
+
+
+def test_batch_results_equal_single_runs():
+    shapes = [(128, 128), (256, 256), (128, 128), (512, 512), (256, 128)]
+    singles, batched = [], []
+    for i, (L, M) in enumerate(shapes):
+        kw = dict(seed=1000 + i, u0=0.02 + 0.03 * (i % 4), con0=0.1 + 0.1 * (i % 4))
+        singles.append(gpu_run(P.MODEL_MISFIT, L, M, **kw))
+        batched.append(gpu_run(P.MODEL_MISFIT, L, M, **kw))
+    b = P.Batch(batched)
+    b.advance(37)
+    for s in singles:
+        s.advance(37)
+    for s, t in zip(singles, batched):
+        a, _ = s.fields_f32()
+        c, _ = t.fields_f32()
+        assert np.array_equal(a.view(np.uint32), c.view(np.uint32))
+
+
+def test_set_fields_roundtrip_and_steps():
+    o = oracle_run(P.MODEL_MISFIT, 64, 64, exact=0)
+    o.step(5)
+    phi, con = o.fields()
+    r = gpu_run(P.MODEL_MISFIT, 64, 64)
+    r.set_fields(phi, con)
+    a, b = r.fields()
+    assert np.abs(a - phi).max() <= 1e-6 and np.abs(b - con).max() <= 1e-6
+    r.advance(50, analysis=True)
+    o.step(50)
+    a, _ = r.fields()
+    assert np.abs(a - o.fields()[0]).max() <= 1e-5
+    assert r.steps == 50
+
+
+def test_invalid_arguments_raise():
+    with pytest.raises(P.PfcError):
+        gpu_run(P.MODEL_MISFIT, 100, 64)
+    with pytest.raises(P.PfcError):
+        gpu_run(P.MODEL_MISFIT, 64, 64, 4)
+    r = gpu_run(P.MODEL_MISFIT, 64, 64)
+    with pytest.raises(P.PfcError):
+        r.energy()  # no analysis step yet

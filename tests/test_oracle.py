@@ -1,0 +1,162 @@
+"""The oracle (CPU restatement) pinned against the reference's own outputs.
+
+The golden fixtures were produced by the unmodified reference program
+(tests/golden/make_golden.py).  In reference-exact mode the restatement must
+reproduce them bit for bit: the VTI Float32 values, energy.txt, and the Phimax,
+strain and q4q6 text files.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import (case_params, energy_line, golden_case, phimax_elastic_lines, phimax_misfit_lines, q4q6_lines,
+                     strain_lines)
+
+MISFIT_CASES = ["misfit_64", "misfit_128_s7", "misfit_256_c1"]
+CVD_CASES = ["cvd_64", "cvd_32x32x8"]
+
+
+def oracle_params(meta, exact=1):
+    model = O.MODEL_MISFIT if meta["model"] == "misfit" else O.MODEL_CVD
+    L, M, N = meta["grid"]
+    p = O.default_params(model, L=L, M=M, N=N, exact=exact)
+    kv = case_params(meta)
+    for k in ("u0", "con0", "sig", "dt", "dx"):
+        if k in kv:
+            setattr(p, k, float(np.float32(kv[k])))
+    if "seed" in kv:
+        p.seed = int(kv["seed"])
+    return p, int(kv["steps"]), int(kv["mod"])
+
+
+def run_oracle_checkpoints(meta, exact=1):
+    """Run the oracle through a golden case; yield (kd, phi, con, energy) at the reference's checkpoints."""
+    p, steps, mod = oracle_params(meta, exact)
+    r = O.Run(p)
+    out = {}
+    energies = []
+    for t in range(steps):
+        r.step()
+        if meta["model"] == "misfit":
+            if (t + 1) % mod == 0 or t + 1 == steps:
+                phi, con = r.fields()
+                out[t + 1] = (phi, con, r.energy())
+                energies.append(energy_line(t + 1, *r.energy()))
+        else:
+            if t % mod == 0:
+                phi, con = r.fields()
+                out[t] = (phi, con, r.energy())
+            energies.append(energy_line(t, *r.energy()))
+    return out, energies
+
+
+@pytest.mark.parametrize("name", MISFIT_CASES + CVD_CASES)
+def test_oracle_reproduces_reference_run(name):
+    d, meta, fields = golden_case(name)
+    got, energies = run_oracle_checkpoints(meta)
+    for kd in meta["kept"]:
+        if kd == 0 and meta["model"] == "misfit":
+            continue  # Misfit writes the initial condition as checkpoint 0; CVD writes the state after step 0
+        phi, con, _ = got[kd]
+        ref_phi, ref_con = fields[f"phi_{kd}"], fields[f"con_{kd}"]
+        assert np.array_equal(phi.astype(np.float32).view(np.uint32), ref_phi.view(np.uint32)), f"phi {kd}"
+        assert np.array_equal(con.astype(np.float32).view(np.uint32), ref_con.view(np.uint32)), f"con {kd}"
+    ref_energy = open(f"{d}/energy.txt").read().splitlines()
+    assert energies == ref_energy
+
+
+@pytest.mark.parametrize("name", MISFIT_CASES)
+def test_oracle_initial_condition(name):
+    d, meta, fields = golden_case(name)
+    if 0 not in meta["kept"]:
+        pytest.skip("initial checkpoint not kept for this case")
+    p, _, _ = oracle_params(meta)
+    r = O.Run(p)
+    phi, con = r.fields()
+    assert np.array_equal(phi.astype(np.float32), fields["phi_0"])
+    assert np.array_equal(con.astype(np.float32), fields["con_0"])
+
+
+@pytest.mark.parametrize("name", MISFIT_CASES)
+def test_oracle_misfit_phimax_text(name):
+    d, meta, fields = golden_case(name)
+    got, _ = run_oracle_checkpoints(meta)
+    for kd in meta["kept"]:
+        if kd == 0:
+            continue
+        phi, con, _ = got[kd]
+        atoms, raw = O.phimax_misfit(phi[:, :, 0], con[:, :, 0], dx=0.125, con0=float(np.float32(case_params(meta).get("con0", 0.2))))
+        assert raw > 0
+        assert phimax_misfit_lines(atoms) == open(f"{d}/Phimax_{kd}.txt").read().splitlines()
+
+
+@pytest.mark.parametrize("name", ["misfit_64", "misfit_128_s7", "misfit_256_c1"])
+def test_oracle_elastic_texts(name):
+    """Elastic peak finder, elastic3D and cryst_order on the reference's own VTI fields."""
+    d, meta, fields = golden_case(name)
+    import glob
+    import json
+    import os
+    for sub in sorted(glob.glob(f"{d}/elastic*")):
+        cj = json.load(open(f"{sub}/case.json"))
+        benchel = 1.7
+        if "--benchel" in cj["args"]:
+            benchel = float(np.float32(cj["args"][cj["args"].index("--benchel") + 1]))
+        L, M, N = meta["grid"]
+        for kd in cj["steps"]:
+            if not os.path.exists(f"{sub}/Phimax_{kd}.txt"):
+                continue
+            phi = fields[f"phi_{kd}"].astype(np.float64)
+            atoms = O.phimax_elastic(phi)
+            assert phimax_elastic_lines(atoms) == open(f"{sub}/Phimax_{kd}.txt").read().splitlines()
+            x, y, z = atoms[:, 0], atoms[:, 1], atoms[:, 2]
+            st, nb = O.elastic3d(x, y, z, L, M, N, benchel=benchel)
+            assert strain_lines(x, y, z, st, nb) == open(f"{sub}/strain_{kd}.txt").read().splitlines()
+            q4, q6 = O.cryst_order(x, y, z, L, M, N)
+            assert q4q6_lines(x, y, z, q4, q6) == open(f"{sub}/q4q6_{kd}.txt").read().splitlines()
+
+
+@pytest.mark.parametrize("shape", [(1, 8, 1), (4, 16, 1), (8, 4, 2), (2, 32, 4), (16, 16, 1), (3, 5, 1)])
+def test_shim_dft_matches_numpy(shape):
+    rng = np.random.default_rng(1)
+    a = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    f = O.dft3d(a, -1)
+    b = O.dft3d(a, +1)
+    ref_f = np.fft.fftn(a)
+    ref_b = np.fft.ifftn(a) * a.size
+    scale = np.abs(ref_f).max()
+    assert np.abs(f - ref_f).max() <= 1e-13 * scale
+    assert np.abs(b - ref_b).max() <= 1e-13 * scale
+
+
+def test_splitmix64_stream():
+    """pfc_common.h:165-181 generator against an independent Python restatement."""
+    import ctypes
+
+    def py_next(state):
+        state = (state + 0x9E3779B97F4A7C15) & (2**64 - 1)
+        z = state
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & (2**64 - 1)
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & (2**64 - 1)
+        return state, z ^ (z >> 31)
+
+    st = ctypes.c_uint64(20200604)
+    pst = 20200604
+    for _ in range(100):
+        v = O.lib().orc_splitmix64_next(ctypes.byref(st))
+        pst, pv = py_next(pst)
+        assert v == pv and st.value == pst
+
+
+def test_pure_fp64_close_to_exact():
+    """The pure-FP64 scheme differs from the reference's mixed precision only at float rounding level."""
+    d, meta, fields = golden_case("misfit_64")
+    pe, _, _ = oracle_params(meta, exact=1)
+    pp, _, _ = oracle_params(meta, exact=0)
+    a, b = O.Run(pe), O.Run(pp)
+    a.step(20)
+    b.step(20)
+    fa, _ = a.fields()
+    fb, _ = b.fields()
+    diff = np.abs(fa - fb).max()
+    assert 0 < diff < 1e-5
