@@ -270,7 +270,8 @@ extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) {
     r->M = p->M;
     r->N = p->N;
     r->P = (long)p->L * p->M * p->N;
-    r->Hp = round_up(p->M / 2 + 1, 16);
+    const int ct = col_tile_width(p->L);
+    r->Hp = round_up(p->M / 2 + 1, ct);
     model_coefs(p->model, &r->k);
     const ModelCoefs &k = r->k;
     r->c2a = c2_params(p->sig, k.gaa1, k.gaa2, k.ka1, k.ka2, k.sigMa1, k.sigMa2);
@@ -328,6 +329,10 @@ extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) {
     d.M = r->M;
     d.N = r->N;
     d.Hp = r->Hp;
+    d.CT = col_tile_width(r->L);
+    d.lct = 0;
+    while ((1 << d.lct) < d.CT) ++d.lct;
+    d.T = r->Hp / d.CT;
     d.model = p->model;
     d.dt = p->dt;
     d.k = r->k;

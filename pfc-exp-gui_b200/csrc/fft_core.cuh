@@ -3,11 +3,16 @@
 // The reference transforms every field with FFTW's complex 3-D DFT
 // (src/experiment/misfit_uniform_time_seed_fftw_early.cpp:438-452, FFTW_ESTIMATE,
 // unnormalised, exp(-2 pi i jk/n) forward).  Here the transforms are written from
-// scratch: a batch of NB interleaved sequences of length N lives in shared memory
-// (element e of sequence b at s[e*NB + b], so consecutive threads touch consecutive
-// words), and each Stockham stage has every thread load a fixed number of complex
-// values into registers, run radix-2/4/8/16 butterflies there, and store them to
-// their autosorted positions.  Natural order in, natural order out; no bit reversal.
+// scratch: a batch of NB interleaved sequences of length N (element e of sequence b
+// at index e*NB + b, so consecutive threads touch consecutive words) is transformed
+// by Stockham stages of radix 16 (plus one radix-2/4/8 stage); each thread holds a
+// fixed set of 16 complex values per stage in registers.  Natural order in and out.
+//
+// A stage reads its inputs from one place and writes its outputs to another:
+// global memory (a contiguous tile with the same e*NB + b layout), shared memory
+// (padded by one element per 16 to spread bank accesses), or registers.  The
+// first stage of a transform can therefore load straight from HBM and the last
+// can store straight to HBM or stay in registers for a pointwise epilogue.
 //
 // Twiddles come from a per-length table tw[j] = exp(-2 pi i j / N) computed on the
 // host in double and rounded once to the working precision.
@@ -21,10 +26,6 @@ namespace pfc {
 // ---------------------------------------------------------------------------
 // complex helpers (float2 / double2)
 // ---------------------------------------------------------------------------
-template <typename T> struct cplx_traits;
-template <> struct cplx_traits<float> { typedef float2 C; };
-template <> struct cplx_traits<double> { typedef double2 C; };
-
 __device__ __forceinline__ float2 mk(float x, float y) { return make_float2(x, y); }
 __device__ __forceinline__ double2 mk(double x, double y) { return make_double2(x, y); }
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
@@ -46,13 +47,17 @@ __device__ __forceinline__ double2 cmulc(double2 a, double2 b) {
 }
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
-__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
-__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
 
 // multiply by -i (forward) or +i (inverse)
 template <bool FWD, typename C> __device__ __forceinline__ C mul_mi(C a) {
     return FWD ? mk(a.y, -a.x) : mk(-a.y, a.x);
 }
+
+// shared-memory padding: one spare element per 16
+__device__ __forceinline__ int spad(int i) { return i + (i >> 4); }
+template <int n> struct padded_len {
+    static constexpr int value = n + (n >> 4) + 1;
+};
 
 // ---------------------------------------------------------------------------
 // Radix butterflies (in registers).  FWD uses exp(-2 pi i / R), inverse exp(+).
@@ -88,22 +93,19 @@ template <typename C> struct real_of;
 template <> struct real_of<float2> { typedef float T; };
 template <> struct real_of<double2> { typedef double T; };
 
-// multiply by w8^k for k = 1, 2, 3 where w8 = exp(-+2 pi i / 8)
+// multiply by w8^k for k = 1, 3 where w8 = exp(-+2 pi i / 8)
 template <bool FWD, typename C> __device__ __forceinline__ C w8_1(C a) {
     typedef typename real_of<C>::T R;
     const R h = kconst<R>::h();
-    // FWD: (h, -h);  INV: (h, +h)
     return FWD ? mk(h * (a.x + a.y), h * (a.y - a.x)) : mk(h * (a.x - a.y), h * (a.x + a.y));
 }
 template <bool FWD, typename C> __device__ __forceinline__ C w8_3(C a) {
     typedef typename real_of<C>::T R;
     const R h = kconst<R>::h();
-    // FWD: (-h, -h); INV: (-h, +h)
     return FWD ? mk(h * (a.y - a.x), -h * (a.x + a.y)) : mk(-h * (a.x + a.y), h * (a.x - a.y));
 }
 
 template <bool FWD, typename C> __device__ __forceinline__ void dft8(C *a) {
-    // radix-2 DIT over two length-4 DFTs
     C e0 = a[0], e1 = a[2], e2 = a[4], e3 = a[6];
     C o0 = a[1], o1 = a[3], o2 = a[5], o3 = a[7];
     dft4<FWD>(e0, e1, e2, e3);
@@ -139,7 +141,6 @@ template <bool FWD, typename C> __device__ __forceinline__ C w16(C a, int j) {
         default: c = -c1; s = -s1; break;  // 9
     }
     if (!FWD) s = -s;
-    // (a.x + i a.y)(c - i s)
     return mk(a.x * c + a.y * s, a.y * c - a.x * s);
 }
 
@@ -147,7 +148,6 @@ template <bool FWD, typename C> __device__ __forceinline__ void dft16(C *a) {
     // 16 = 4 x 4: X[k1 + 4 k2] = sum_n2 w4^(n2 k2) w16^(n2 k1) sum_n1 a[4 n1 + n2] w4^(n1 k1)
 #pragma unroll
     for (int n2 = 0; n2 < 4; ++n2) dft4<FWD>(a[n2], a[n2 + 4], a[n2 + 8], a[n2 + 12]);
-    // now a[n2 + 4*k1] holds the inner DFT output k1 of column n2
 #pragma unroll
     for (int n2 = 1; n2 < 4; ++n2)
 #pragma unroll
@@ -167,10 +167,10 @@ template <bool FWD, typename C> __device__ __forceinline__ void dft16(C *a) {
 }
 
 template <int R, bool FWD, typename C> __device__ __forceinline__ void dftR(C *a) {
-    if (R == 2) dft2<FWD>(a[0], a[1]);
-    else if (R == 4) dft4<FWD>(a[0], a[1], a[2], a[3]);
-    else if (R == 8) dft8<FWD>(a);
-    else if (R == 16) dft16<FWD>(a);
+    if constexpr (R == 2) dft2<FWD>(a[0], a[1]);
+    else if constexpr (R == 4) dft4<FWD>(a[0], a[1], a[2], a[3]);
+    else if constexpr (R == 8) dft8<FWD>(a);
+    else if constexpr (R == 16) dft16<FWD>(a);
 }
 
 // ---------------------------------------------------------------------------
@@ -181,71 +181,141 @@ template <int N> struct radix_plan {
     static constexpr int n16 = log2n / 4;
     static constexpr int tail = 1 << (log2n % 4);  // 1, 2, 4 or 8
     static constexpr int stages = n16 + (tail > 1 ? 1 : 0);
+    static constexpr int last_radix = tail > 1 ? tail : 16;
 };
 template <> struct radix_plan<1> {
     static constexpr int log2n = 0;
     static constexpr int n16 = 0;
     static constexpr int tail = 1;
     static constexpr int stages = 0;
+    static constexpr int last_radix = 1;
 };
 
-// One Stockham stage of radix R on NB interleaved sequences of length N in shared
-// memory, in place.  Each of the NT threads owns PER_T = NB*N/(R*NT) butterflies.
-// tw: table of exp(-2 pi i j / N), j < N.
-template <int N, int NB, int NT, int R, bool FWD, typename C>
-__device__ __forceinline__ void stockham_stage(C *s, const C *__restrict__ tw, int Ns) {
-    constexpr int ITEMS = NB * (N / R);
-    constexpr int PER_T = (ITEMS + NT - 1) / NT;
+template <int N, int NB, int NT, int R> struct StageShape {
+    static constexpr int ITEMS = NB * (N / R);
+    static constexpr int PER_T = (ITEMS + NT - 1) / NT;
+    static constexpr bool EXACT = ITEMS % NT == 0;
+};
+
+// Memory spaces a stage reads from / writes to.
+enum : int { SP_SMEM = 0, SP_GLOBAL = 1, SP_REGS = 2 };
+
+// keeps a parameter out of template argument deduction (it may be passed nullptr)
+template <typename T> struct nodeduce {
+    typedef T type;
+};
+
+// One Stockham stage of radix R on NB interleaved sequences of length N.
+// IN/OUT: SP_SMEM (padded shared array), SP_GLOBAL (plain array).  OUT may also be
+// SP_REGS: the stage's outputs are left in v (element e = j + r*Ns of sequence b,
+// item w = tid + q*NT, b = w % NB, j = w / NB) and nothing is stored.
+// A stage whose input and output are the same shared array synchronises between
+// its loads and its stores.
+template <int N, int NB, int NT, int R, bool FWD, int IN, int OUT, typename C>
+__device__ __forceinline__ void stage(const C *__restrict__ in, typename nodeduce<C>::type *out, const C *__restrict__ tw,
+                                      int Ns,
+                                      C (&v)[StageShape<N, NB, NT, R>::PER_T][R]) {
+    typedef StageShape<N, NB, NT, R> S;
     const int tid = threadIdx.x;
-    C v[PER_T][R];
+    // a stage that only writes shared memory must not overtake earlier readers of it
+    if (IN != SP_SMEM && OUT == SP_SMEM) __syncthreads();
 #pragma unroll
-    for (int q = 0; q < PER_T; ++q) {
+    for (int q = 0; q < S::PER_T; ++q) {
         const int w = tid + q * NT;
-        if (ITEMS % NT == 0 || w < ITEMS) {
+        if (S::EXACT || w < S::ITEMS) {
             const int b = w % NB, j = w / NB;
 #pragma unroll
-            for (int r = 0; r < R; ++r) v[q][r] = s[(j + r * (N / R)) * NB + b];
+            for (int r = 0; r < R; ++r) {
+                const int e = (j + r * (N / R)) * NB + b;
+                v[q][r] = IN == SP_SMEM ? in[spad(e)] : in[e];
+            }
         }
     }
-    __syncthreads();
+    if (IN == SP_SMEM && OUT == SP_SMEM) __syncthreads();
 #pragma unroll
-    for (int q = 0; q < PER_T; ++q) {
+    for (int q = 0; q < S::PER_T; ++q) {
         const int w = tid + q * NT;
-        if (ITEMS % NT == 0 || w < ITEMS) {
+        if (S::EXACT || w < S::ITEMS) {
             const int b = w % NB, j = w / NB;
             const int k = j % Ns;
             if (Ns > 1) {
-                // twiddle w^(r*k) with w = exp(-+2 pi i/(Ns*R)); table step N/(Ns*R)
                 const int step = N / (Ns * R);
 #pragma unroll
                 for (int r = 1; r < R; ++r) {
-                    const C t = tw[(r * k * step) & (N - 1)];
+                    const C t = tw[r * k * step];
                     v[q][r] = FWD ? cmul(v[q][r], t) : cmulc(v[q][r], t);
                 }
             }
             dftR<R, FWD>(v[q]);
-            const int base = (j / Ns) * Ns * R + k;
+            if (OUT != SP_REGS) {
+                const int base = (j / Ns) * Ns * R + k;
 #pragma unroll
-            for (int r = 0; r < R; ++r) s[(base + r * Ns) * NB + b] = v[q][r];
+                for (int r = 0; r < R; ++r) {
+                    const int e = (base + r * Ns) * NB + b;
+                    if (OUT == SP_SMEM)
+                        out[spad(e)] = v[q][r];
+                    else
+                        out[e] = v[q][r];
+                }
+            }
         }
     }
-    __syncthreads();
+    if (OUT == SP_SMEM) __syncthreads();
 }
 
-// Full in-place FFT of NB interleaved length-N sequences in shared memory.
-// Caller must __syncthreads() before (data written) -- the routine syncs after.
-template <int N, int NB, int NT, bool FWD, typename C>
-__device__ __forceinline__ void fft_smem(C *s, const C *__restrict__ tw) {
+// Values a thread holds after a transform that ends in registers.
+template <int N, int NB, int NT> struct RegOut {
     typedef radix_plan<N> P;
+    static constexpr int R = P::last_radix;
+    static constexpr int PER_T = StageShape<N, NB, NT, R>::PER_T;
+    static constexpr int NS = N / R;  // Ns of the last stage
+};
+
+// Full transform of NB interleaved length-N sequences.
+//   IN  = SP_GLOBAL: first stage reads `src` (global); SP_SMEM: reads padded `s`.
+//   OUT = SP_GLOBAL: last stage writes `dst` (global); SP_SMEM: writes `s`;
+//         SP_REGS: last stage output stays in `last` (see RegOut for the layout).
+// Intermediate stages run in place in the padded shared array `s`.  Callers must
+// __syncthreads() before a transform that reads data they wrote to `s`; the
+// routine leaves `s` synchronised when it returns.
+template <int N, int NB, int NT, bool FWD, int IN, int OUT, typename C>
+__device__ __forceinline__ void fft(const typename nodeduce<C>::type *src, C *s, typename nodeduce<C>::type *dst,
+                                    const C *__restrict__ tw,
+                                    C (&last)[RegOut<N, NB, NT>::PER_T][RegOut<N, NB, NT>::R]) {
+    typedef radix_plan<N> P;
+    constexpr int ST = P::stages;
     int Ns = 1;
-    if constexpr (P::n16 > 0) {
+    // stage index i: radix 16 for i < n16, else tail radix
+    if constexpr (ST == 1) {
+        if constexpr (OUT == SP_REGS)
+            stage<N, NB, NT, P::last_radix, FWD, IN, SP_REGS>(IN == SP_GLOBAL ? src : s, nullptr, tw, Ns, last);
+        else
+            stage<N, NB, NT, P::last_radix, FWD, IN, OUT>(IN == SP_GLOBAL ? src : s, OUT == SP_GLOBAL ? dst : s, tw, Ns,
+                                                          last);
+    } else {
+        typedef StageShape<N, NB, NT, 16> S16;
+        C v[S16::PER_T][16];
+        // first stage (radix 16)
+        stage<N, NB, NT, 16, FWD, IN, SP_SMEM>(IN == SP_GLOBAL ? src : s, s, tw, Ns, v);
+        Ns *= 16;
 #pragma unroll
-        for (int st = 0; st < P::n16; ++st) {
-            stockham_stage<N, NB, NT, 16, FWD>(s, tw, Ns);
+        for (int i = 1; i < ST - 1; ++i) {
+            stage<N, NB, NT, 16, FWD, SP_SMEM, SP_SMEM>(s, s, tw, Ns, v);
             Ns *= 16;
         }
+        // last stage
+        if constexpr (OUT == SP_REGS)
+            stage<N, NB, NT, P::last_radix, FWD, SP_SMEM, SP_REGS>(s, nullptr, tw, Ns, last);
+        else
+            stage<N, NB, NT, P::last_radix, FWD, SP_SMEM, OUT>(s, OUT == SP_GLOBAL ? dst : s, tw, Ns, last);
     }
-    if constexpr (P::tail > 1) stockham_stage<N, NB, NT, P::tail, FWD>(s, tw, Ns);
+}
+
+// Convenience: in-place FFT of a padded shared array.
+template <int N, int NB, int NT, bool FWD, typename C>
+__device__ __forceinline__ void fft_smem(C *s, const C *__restrict__ tw) {
+    C last[RegOut<N, NB, NT>::PER_T][RegOut<N, NB, NT>::R];
+    fft<N, NB, NT, FWD, SP_SMEM, SP_SMEM>(nullptr, s, nullptr, tw, last);
 }
 
 }  // namespace pfc

@@ -32,9 +32,10 @@ struct C2Params {
 
 struct RunDesc {
     int L, M, N;      // grid (N = 1 for 2-D)
-    int Hp;           // row stride of row-space arrays, in complex elements
+    int Hp;           // padded number of packed columns (T * CT >= M/2 + 1)
+    int CT, lct, T;   // column-tile width (power of two), its log2, number of tiles
     int model;
-    // row-space arrays, [L][Hp] float2 each
+    // row-space arrays, T tiles of [L][CT] float2 each: (l, km) at ((km/CT)*L + l)*CT + km%CT
     float2 *psi, *con, *ca, *cb, *inn, *inc, *gx, *gy;
     // real-space checkpoint outputs, [L][M] float
     float *psi_real, *con_real;
@@ -69,5 +70,7 @@ enum ColMode : int { COL_STEP = 0, COL_PREPARE = 1, COL_STEP_CHECKPOINT = 2 };
 
 // Number of partial-sum slots the analysis kernel writes per run (2 doubles each).
 int analysis_partials(int L, int M);
+// Column-tile width of the row-space layout for a grid with L rows.
+int col_tile_width(int L);
 
 }  // namespace pfc

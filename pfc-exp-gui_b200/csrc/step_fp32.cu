@@ -9,11 +9,16 @@
 //     pointwise UPDATEINN3 + UPDATEINFMIX + UPDATEINFCMIX tail + UPDATEINC2MIX(C)
 //       (MIS:773-874) -> inn, inc
 //     forward row FFT of inn+i*inc                  (first half of p8/p9)
-//   column kernel (one CTA per C packed columns km):
+//   column kernel (one CTA per tile of CT packed columns km):
 //     forward column FFTs of psi, inn, con, inc     (second half of p1/p8/p6/p9)
 //     semi-implicit update MAINEQUATIONC2_NOI/C2MIX (MIS:983-1014, CVD:865-886) with
 //       the denominators built in FP64 and rounded, k = 0 held out in FP64
 //     C2A/C2B multiply (MIS:807-810) and inverse column FFTs of psi', c2a, c2b, con'
+//
+// Row-space arrays are stored column-tile-major: element (l, km) at
+// ((km / CT) * L + l) * CT + km % CT, so a column kernel tile (L rows x CT columns)
+// is one contiguous block, and RPC consecutive rows of one tile are RPC*CT
+// contiguous elements for the row kernel.
 //
 // Compulsory HBM traffic: row kernel reads 4 and writes 2 row-space arrays, column
 // kernel reads 4 and writes 4; a row-space array is 4 bytes per grid point, so one
@@ -23,19 +28,28 @@
 
 namespace pfc {
 
-constexpr int TILE = 8192;  // complex elements per CTA tile in shared memory (64 KB in FP32)
+constexpr int ROW_TILE = 8192;  // complex elements per row-kernel CTA (64 KB in FP32)
+constexpr int COL_TILE = 4096;  // complex elements per column-kernel tile (32 KB in FP32)
 
 template <int M> struct RowCfg {
-    static constexpr int RPC = (TILE / 2) / M >= 1 ? (TILE / 2) / M : 1;  // rows per CTA
+    static constexpr int RPC = (ROW_TILE / 2) / M >= 1 ? (ROW_TILE / 2) / M : 1;  // rows per CTA
     static constexpr int NB = 2 * RPC;
     static constexpr int NT = (NB * M / 16) < 512 ? (NB * M / 16) : 512;
 };
 
 template <int L> struct ColCfg {
-    static constexpr int C = (TILE / L) > 16 ? 16 : (TILE / L);  // packed columns per CTA
-    static constexpr int NT = (C * L / 16) < 512 ? (C * L / 16) : 512;
-    static constexpr int PER = (C * L) / NT;  // complex values each thread parks
+    static constexpr int C = (COL_TILE / L) > 16 ? 16 : (COL_TILE / L);  // packed columns per tile
+    static constexpr int NT = (C * L / 16) < 32 ? 32 : (C * L / 16);
 };
+
+int col_tile_width(int L) {
+    int c = COL_TILE / L;
+    return c > 16 ? 16 : (c < 1 ? 1 : c);
+}
+
+__device__ __forceinline__ long rs_index(const RunDesc &d, int l, int km) {
+    return ((long)(km >> d.lct) * d.L + l) * d.CT + (km & (d.CT - 1));
+}
 
 __device__ __forceinline__ float c2eval(const C2Params &p, float ks) {
     const float s = sqrtf(ks);
@@ -74,33 +88,48 @@ __device__ __forceinline__ void separate(float2 zk, float2 zm, float2 &X, float2
     Y = make_float2(0.5f * (zk.y + zm.y), 0.5f * (zm.x - zk.x));
 }
 
-// Write Z[k], Z[M-k] of Z = IFFT-input for real pair (x, y) from half spectra X, Y.
+// Write Z[k], Z[M-k] of Z = IFFT-input for the real pair (x, y) from half spectra X, Y.
 __device__ __forceinline__ void build_pair(float2 *s, int NB, int b, int k, int M, float2 X, float2 Y) {
     const int H = M / 2;
     if (k == 0 || k == H) {
-        s[k * NB + b] = make_float2(X.x, Y.x);
+        s[spad(k * NB + b)] = make_float2(X.x, Y.x);
     } else {
-        s[k * NB + b] = make_float2(X.x - Y.y, X.y + Y.x);
-        s[(M - k) * NB + b] = make_float2(X.x + Y.y, Y.x - X.y);
+        s[spad(k * NB + b)] = make_float2(X.x - Y.y, X.y + Y.x);
+        s[spad((M - k) * NB + b)] = make_float2(X.x + Y.y, Y.x - X.y);
     }
 }
+
+// Loop over the row-space elements (l0 + r, km), r < RPC, km <= M/2, in an order
+// that walks each column tile's contiguous RPC*CT block: w -> (tile t, row r, col c).
+#define ROW_TILE_LOOP(RPC, H, NT, ...)                                     \
+    {                                                                       \
+        const int _ct = d.CT, _lct = d.lct;                                 \
+        const int _blk = (RPC) * _ct;                                       \
+        const int _total = d.T * _blk;                                      \
+        for (int w = threadIdx.x; w < _total; w += (NT)) {                  \
+            const int t = w / _blk, rem = w - t * _blk;                     \
+            const int r = rem >> _lct, k = (t << _lct) + (rem & (_ct - 1)); \
+            if (k > (H)) continue;                                          \
+            const int l = l0 + r;                                           \
+            __VA_ARGS__                                                     \
+        }                                                                   \
+    }
 
 // ---------------------------------------------------------------------------
 // Row kernel: 4 row-space arrays in, 2 out.
 // ---------------------------------------------------------------------------
 template <int M>
-__global__ void __launch_bounds__(RowCfg<M>::NT) k_row_step(const RunDesc *__restrict__ runs,
+__global__ void __launch_bounds__(RowCfg<M>::NT, 2) k_row_step(const RunDesc *__restrict__ runs,
                                                              const float2 *__restrict__ tw) {
     constexpr int RPC = RowCfg<M>::RPC, NB = RowCfg<M>::NB, NT = RowCfg<M>::NT, H = M / 2;
     extern __shared__ float2 s[];
     const RunDesc &d = runs[blockIdx.y];
-    const int L = d.L, Hp = d.Hp;
+    const int L = d.L;
     const int l0 = blockIdx.x * RPC;
-    for (int w = threadIdx.x; w < RPC * (H + 1); w += NT) {
-        const int r = w / (H + 1), k = w - r * (H + 1), l = l0 + r;
+    ROW_TILE_LOOP(RPC, H, NT, {
         float2 P = make_float2(0.f, 0.f), Cc = P, A = P, B = P;
         if (l < L) {
-            const size_t o = (size_t)l * Hp + k;
+            const long o = rs_index(d, l, k);
             P = d.psi[o];
             Cc = d.con[o];
             A = d.ca[o];
@@ -108,7 +137,7 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_step(const RunDesc *__res
         }
         build_pair(s, NB, 2 * r, k, M, P, Cc);
         build_pair(s, NB, 2 * r + 1, k, M, A, B);
-    }
+    })
     __syncthreads();
     fft_smem<M, NB, NT, false>(s, tw);
 
@@ -121,7 +150,7 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_step(const RunDesc *__res
         const int w = threadIdx.x + q * NT;
         if (w < RPC * M) {
             const int r = w % RPC, m = w / RPC;
-            const float2 z1 = s[m * NB + 2 * r], z2 = s[m * NB + 2 * r + 1];
+            const float2 z1 = s[spad(m * NB + 2 * r)], z2 = s[spad(m * NB + 2 * r + 1)];
             const float psi = z1.x * invM + d.psi_mean_f, c = z1.y * invM + d.con_mean_f;
             const PointTerms t = point_terms(d.k, inv_c0, inv_1mc0, psi, c, z2.x * invM, z2.y * invM);
             out[q] = make_float2(t.inn, t.inc);
@@ -131,19 +160,19 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_step(const RunDesc *__res
 #pragma unroll
     for (int q = 0; q < PTS; ++q) {
         const int w = threadIdx.x + q * NT;
-        if (w < RPC * M) s[w] = out[q];  // w = m*RPC + r: interleaved layout with NB' = RPC
+        if (w < RPC * M) s[spad(w)] = out[q];  // w = m*RPC + r: interleaved layout with NB' = RPC
     }
     __syncthreads();
     fft_smem<M, RPC, NT, true>(s, tw);
-    for (int w = threadIdx.x; w < RPC * (H + 1); w += NT) {
-        const int r = w / (H + 1), k = w - r * (H + 1), l = l0 + r;
-        if (l >= L) continue;
-        float2 X, Y;
-        separate(s[k * RPC + r], s[((M - k) & (M - 1)) * RPC + r], X, Y);
-        const size_t o = (size_t)l * Hp + k;
-        d.inn[o] = X;
-        d.inc[o] = Y;
-    }
+    ROW_TILE_LOOP(RPC, H, NT, {
+        if (l < L) {
+            float2 X, Y;
+            separate(s[spad(k * RPC + r)], s[spad(((M - k) & (M - 1)) * RPC + r)], X, Y);
+            const long o = rs_index(d, l, k);
+            d.inn[o] = X;
+            d.inc[o] = Y;
+        }
+    })
 }
 
 // ---------------------------------------------------------------------------
@@ -155,7 +184,7 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_forward(const RunDesc *__
     constexpr int RPC = RowCfg<M>::RPC, NT = RowCfg<M>::NT, H = M / 2;
     extern __shared__ float2 s[];
     const RunDesc &d = runs[blockIdx.y];
-    const int L = d.L, Hp = d.Hp;
+    const int L = d.L;
     const int l0 = blockIdx.x * RPC;
     for (int w = threadIdx.x; w < RPC * M; w += NT) {
         const int r = w % RPC, m = w / RPC, l = l0 + r;
@@ -164,155 +193,133 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_forward(const RunDesc *__
             const size_t o = (size_t)l * M + m;
             z = make_float2((float)((double)d.psi_real[o] - d.psi_mean), (float)((double)d.con_real[o] - d.con_mean));
         }
-        s[w] = z;
+        s[spad(w)] = z;
     }
     __syncthreads();
     fft_smem<M, RPC, NT, true>(s, tw);
-    for (int w = threadIdx.x; w < RPC * (H + 1); w += NT) {
-        const int r = w / (H + 1), k = w - r * (H + 1), l = l0 + r;
-        if (l >= L) continue;
-        float2 X, Y;
-        separate(s[k * RPC + r], s[((M - k) & (M - 1)) * RPC + r], X, Y);
-        const size_t o = (size_t)l * Hp + k;
-        d.psi[o] = X;
-        d.con[o] = Y;
-    }
+    ROW_TILE_LOOP(RPC, H, NT, {
+        if (l < L) {
+            float2 X, Y;
+            separate(s[spad(k * RPC + r)], s[spad(((M - k) & (M - 1)) * RPC + r)], X, Y);
+            const long o = rs_index(d, l, k);
+            d.psi[o] = X;
+            d.con[o] = Y;
+        }
+    })
 }
 
 // ---------------------------------------------------------------------------
 // Column kernel.
 // ---------------------------------------------------------------------------
-template <int L, int C, int NT>
-__device__ __forceinline__ void tile_load(float2 *s, const float2 *__restrict__ g, int Hp, int c0) {
-    for (int e = threadIdx.x; e < L * C; e += NT) {
-        const int l = e / C, c = e % C;
-        s[e] = g[(size_t)l * Hp + c0 + c];
-    }
-}
-template <int L, int C, int NT>
-__device__ __forceinline__ void tile_store(const float2 *s, float2 *__restrict__ g, int Hp, int c0, int H) {
-    for (int e = threadIdx.x; e < L * C; e += NT) {
-        const int l = e / C, c = e % C;
-        if (c0 + c <= H) g[(size_t)l * Hp + c0 + c] = s[e];
-    }
-}
-
 template <int L, int MODE>
 __global__ void __launch_bounds__(ColCfg<L>::NT) k_col_step(const RunDesc *__restrict__ runs,
                                                              const float2 *__restrict__ tw) {
-    constexpr int C = ColCfg<L>::C, NT = ColCfg<L>::NT, PER = ColCfg<L>::PER;
+    constexpr int C = ColCfg<L>::C, NT = ColCfg<L>::NT;
+    typedef RegOut<L, C, NT> RO;
     extern __shared__ float2 s[];
     const RunDesc &d = runs[blockIdx.y];
-    const int Hp = d.Hp, H = d.M / 2;
-    const int c0 = blockIdx.x * C;
+    const int H = d.M / 2;
+    const long tile = (long)blockIdx.x * L * C;
+    const int km0 = blockIdx.x * C;
     const float invL = 1.0f / (float)L;
     const float mn_dt = d.k.dynamic_mn * d.dt, mc_dt = d.k.dynamic_mc * d.dt;
     const float mc_dt_alpha = mc_dt * d.k.para_alpha;
-    float2 park[PER];
+    float2 a[RO::PER_T][RO::R], b[RO::PER_T][RO::R];
 
-    // ---- phi: forward column FFT ----
-    tile_load<L, C, NT>(s, d.psi, Hp, c0);
-    __syncthreads();
-    fft_smem<L, C, NT, true>(s, tw);
+    // element held by (q, r) after a transform that ends in registers
+#define COL_ELEM(q, r, l, km)                              \
+    const int _w = threadIdx.x + (q) * NT;                 \
+    const int l = (_w / C) + (r) * RO::NS, km = km0 + _w % C;
+
+    // ---- phi: forward column FFTs of psi and inn, update ----
+    fft<L, C, NT, true, SP_GLOBAL, SP_REGS>(d.psi + tile, s, nullptr, tw, a);
+    if (MODE != COL_PREPARE) fft<L, C, NT, true, SP_GLOBAL, SP_REGS>(d.inn + tile, s, nullptr, tw, b);
 #pragma unroll
-    for (int i = 0; i < PER; ++i) park[i] = s[threadIdx.x + i * NT];
-    __syncthreads();
-    if (MODE != COL_PREPARE) {
-        tile_load<L, C, NT>(s, d.inn, Hp, c0);
-        __syncthreads();
-        fft_smem<L, C, NT, true>(s, tw);
-    }
+    for (int q = 0; q < RO::PER_T; ++q)
 #pragma unroll
-    for (int i = 0; i < PER; ++i) {
-        const int e = threadIdx.x + i * NT, l = e / C, km = c0 + e % C;
-        float2 v = park[i];
-        if (MODE != COL_PREPARE) {
-            const float kl = d.krefl[l], kmv = km <= H ? d.krefm[km] : 0.0f;
-            const float ks = kl * kl + kmv * kmv;
-            const float an = mn_dt * ks;
-            const float den = (float)(1.0 / (1.0 + (double)an));
-            const float2 nh = s[e];
-            v = make_float2((v.x - an * nh.x) * den, (v.y - an * nh.y) * den);
+        for (int r = 0; r < RO::R; ++r) {
+            COL_ELEM(q, r, l, km)
+            float2 v = a[q][r];
+            if (MODE != COL_PREPARE) {
+                const float kl = d.krefl[l], kmv = km <= H ? d.krefm[km] : 0.0f;
+                const float ks = kl * kl + kmv * kmv;
+                const float an = mn_dt * ks;
+                const float den = (float)(1.0 / (1.0 + (double)an));
+                const float2 nh = b[q][r];
+                v = make_float2((v.x - an * nh.x) * den, (v.y - an * nh.y) * den);
+            }
+            if (l == 0 && km == 0) v = make_float2(0.f, 0.f);
+            a[q][r] = cscale(v, invL);
         }
-        if (l == 0 && km == 0) v = make_float2(0.f, 0.f);
-        park[i] = cscale(v, invL);
-    }
-    if (MODE != COL_PREPARE) {
+    // outputs: psi' (not in PREPARE mode), c2a = C2A psi', c2b = C2B psi'
+#pragma unroll
+    for (int pass = (MODE == COL_PREPARE ? 1 : 0); pass < 3; ++pass) {
         __syncthreads();
 #pragma unroll
-        for (int i = 0; i < PER; ++i) s[threadIdx.x + i * NT] = park[i];
-        __syncthreads();
-        fft_smem<L, C, NT, false>(s, tw);
-        tile_store<L, C, NT>(s, d.psi, Hp, c0, H);
-    }
-    // ---- c2a, c2b ----
+        for (int q = 0; q < RO::PER_T; ++q)
 #pragma unroll
-    for (int pass = 0; pass < 2; ++pass) {
+            for (int r = 0; r < RO::R; ++r) {
+                COL_ELEM(q, r, l, km)
+                float g = 1.0f;
+                if (pass > 0) {
+                    const float kl = d.krefl[l], kmv = km <= H ? d.krefm[km] : 0.0f;
+                    g = c2eval(pass == 1 ? d.c2a : d.c2b, kl * kl + kmv * kmv);
+                }
+                s[spad(l * C + (km - km0))] = cscale(a[q][r], g);
+            }
         __syncthreads();
-        const C2Params &cp = pass == 0 ? d.c2a : d.c2b;
-#pragma unroll
-        for (int i = 0; i < PER; ++i) {
-            const int e = threadIdx.x + i * NT, l = e / C, km = c0 + e % C;
-            const float kl = d.krefl[l], kmv = km <= H ? d.krefm[km] : 0.0f;
-            s[e] = cscale(park[i], c2eval(cp, kl * kl + kmv * kmv));
-        }
-        __syncthreads();
-        fft_smem<L, C, NT, false>(s, tw);
-        tile_store<L, C, NT>(s, pass == 0 ? d.ca : d.cb, Hp, c0, H);
+        float2 *dst = pass == 0 ? d.psi : (pass == 1 ? d.ca : d.cb);
+        fft<L, C, NT, false, SP_SMEM, SP_GLOBAL>(nullptr, s, dst + tile, tw, b);
     }
     if (MODE == COL_PREPARE) return;
 
     // ---- con ----
-    __syncthreads();
-    tile_load<L, C, NT>(s, d.con, Hp, c0);
-    __syncthreads();
-    fft_smem<L, C, NT, true>(s, tw);
+    fft<L, C, NT, true, SP_GLOBAL, SP_REGS>(d.con + tile, s, nullptr, tw, a);
+    fft<L, C, NT, true, SP_GLOBAL, SP_REGS>(d.inc + tile, s, nullptr, tw, b);
 #pragma unroll
-    for (int i = 0; i < PER; ++i) park[i] = s[threadIdx.x + i * NT];
-    __syncthreads();
-    tile_load<L, C, NT>(s, d.inc, Hp, c0);
-    __syncthreads();
-    fft_smem<L, C, NT, true>(s, tw);
+    for (int q = 0; q < RO::PER_T; ++q)
 #pragma unroll
-    for (int i = 0; i < PER; ++i) {
-        const int e = threadIdx.x + i * NT, l = e / C, km = c0 + e % C;
-        const float kl = d.krefl[l], kmv = km <= H ? d.krefm[km] : 0.0f;
-        const float ks = kl * kl + kmv * kmv;
-        const float ac = mc_dt * ks;
-        const float dc = mc_dt_alpha * ks * ks;
-        const float den = (float)(1.0 / (1.0 + (double)dc));
-        const float2 ih = s[e];
-        float2 v = make_float2((park[i].x - ac * ih.x) * den, (park[i].y - ac * ih.y) * den);
-        if (l == 0 && km == 0) v = make_float2(0.f, 0.f);
-        park[i] = cscale(v, invL);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < PER; ++i) s[threadIdx.x + i * NT] = park[i];
-    __syncthreads();
-    fft_smem<L, C, NT, false>(s, tw);
-    tile_store<L, C, NT>(s, d.con, Hp, c0, H);
-    if (MODE == COL_STEP_CHECKPOINT) {
-        // gradient of con: -i k con^ along l (gra1) and m (gra2), MIS:884-889
-#pragma unroll
-        for (int pass = 0; pass < 2; ++pass) {
-            __syncthreads();
-#pragma unroll
-            for (int i = 0; i < PER; ++i) {
-                const int e = threadIdx.x + i * NT, l = e / C, km = c0 + e % C;
-                const float kv = pass == 0 ? d.krefl[l] : (km <= H ? d.krefm[km] : 0.0f);
-                s[e] = make_float2(kv * park[i].y, -kv * park[i].x);
-            }
-            __syncthreads();
-            fft_smem<L, C, NT, false>(s, tw);
-            tile_store<L, C, NT>(s, pass == 0 ? d.gx : d.gy, Hp, c0, H);
+        for (int r = 0; r < RO::R; ++r) {
+            COL_ELEM(q, r, l, km)
+            const float kl = d.krefl[l], kmv = km <= H ? d.krefm[km] : 0.0f;
+            const float ks = kl * kl + kmv * kmv;
+            const float ac = mc_dt * ks;
+            const float dc = mc_dt_alpha * ks * ks;
+            const float den = (float)(1.0 / (1.0 + (double)dc));
+            const float2 ih = b[q][r];
+            float2 v = make_float2((a[q][r].x - ac * ih.x) * den, (a[q][r].y - ac * ih.y) * den);
+            if (l == 0 && km == 0) v = make_float2(0.f, 0.f);
+            a[q][r] = cscale(v, invL);
         }
+    constexpr int NOUT = MODE == COL_STEP_CHECKPOINT ? 3 : 1;
+#pragma unroll
+    for (int pass = 0; pass < NOUT; ++pass) {
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < RO::PER_T; ++q)
+#pragma unroll
+            for (int r = 0; r < RO::R; ++r) {
+                COL_ELEM(q, r, l, km)
+                float2 v = a[q][r];
+                if (pass > 0) {
+                    // gradient of con, -i k con^ along l (gra1) and m (gra2), MIS:884-889
+                    const float kv = pass == 1 ? d.krefl[l] : (km <= H ? d.krefm[km] : 0.0f);
+                    v = make_float2(kv * v.y, -kv * v.x);
+                }
+                s[spad(l * C + (km - km0))] = v;
+            }
+        __syncthreads();
+        float2 *dst = pass == 0 ? d.con : (pass == 1 ? d.gx : d.gy);
+        fft<L, C, NT, false, SP_SMEM, SP_GLOBAL>(nullptr, s, dst + tile, tw, b);
     }
+#undef COL_ELEM
 }
 
 // ---------------------------------------------------------------------------
 // Analysis row kernel (checkpoints): real fields, energy density and mass.
-// ENERGYC2 (MIS:1043-1092): float energy terms, double accumulation.
+// ENERGYC2 (MIS:1043-1092): float energy terms, double accumulation.  The mass is
+// accumulated as sum(phi - mean) plus the FP64 mean, so it carries no rounding of
+// the mean itself.
 // ---------------------------------------------------------------------------
 template <int M>
 __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_analysis(const RunDesc *__restrict__ runs,
@@ -322,15 +329,14 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_analysis(const RunDesc *_
     extern __shared__ float2 s[];
     __shared__ double red[2][32];
     const RunDesc &d = runs[blockIdx.y];
-    const int L = d.L, Hp = d.Hp;
+    const int L = d.L;
     const int l0 = blockIdx.x * RPC;
-    for (int w = threadIdx.x; w < RPC * (H + 1); w += NT) {
-        const int r = w / (H + 1), k = w - r * (H + 1), l = l0 + r;
+    ROW_TILE_LOOP(RPC, H, NT, {
         float2 z[6];
 #pragma unroll
         for (int j = 0; j < 6; ++j) z[j] = make_float2(0.f, 0.f);
         if (l < L) {
-            const size_t o = (size_t)l * Hp + k;
+            const long o = rs_index(d, l, k);
             z[0] = d.psi[o];
             z[1] = d.con[o];
             z[2] = d.ca[o];
@@ -341,7 +347,7 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_analysis(const RunDesc *_
         build_pair(s, NB, 3 * r, k, M, z[0], z[1]);
         build_pair(s, NB, 3 * r + 1, k, M, z[2], z[3]);
         build_pair(s, NB, 3 * r + 2, k, M, z[4], z[5]);
-    }
+    })
     __syncthreads();
     fft_smem<M, NB, NT, false>(s, tw);
     const float invM = 1.0f / (float)M;
@@ -351,8 +357,9 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_analysis(const RunDesc *_
     for (int w = threadIdx.x; w < RPC * M; w += NT) {
         const int r = w % RPC, m = w / RPC, l = l0 + r;
         if (l >= L) continue;
-        const float2 z1 = s[m * NB + 3 * r], z2 = s[m * NB + 3 * r + 1], z3 = s[m * NB + 3 * r + 2];
-        const float psi = z1.x * invM + d.psi_mean_f, c = z1.y * invM + d.con_mean_f;
+        const float2 z1 = s[spad(m * NB + 3 * r)], z2 = s[spad(m * NB + 3 * r + 1)], z3 = s[spad(m * NB + 3 * r + 2)];
+        const float dpsi = z1.x * invM;
+        const float psi = dpsi + d.psi_mean_f, c = z1.y * invM + d.con_mean_f;
         const float a = z2.x * invM, b = z2.y * invM, gx = z3.x * invM, gy = z3.y * invM;
         d.psi_real[(size_t)l * M + m] = psi;
         d.con_real[(size_t)l * M + m] = c;
@@ -364,7 +371,7 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_analysis(const RunDesc *_
         const float in3 = -(1.0f - 3.0f * c2 + 2.0f * c2 * c) * a - (1.0f - 3.0f * omc2 + 2.0f * omc2 * omc) * b;
         const float e_ex = 0.5f * psi * in3 + k.para_alpha * (gx * gx + gy * gy + gy * gy);
         acc_e += (double)(e_id + e_mix + e_ex);
-        acc_m += (double)psi;
+        acc_m += (double)dpsi;
     }
     // deterministic block reduction
 #pragma unroll
@@ -384,8 +391,9 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_analysis(const RunDesc *_
             se += red[0][i];
             sm += red[1][i];
         }
+        const int lrows = (L - l0) < RPC ? (L - l0) : RPC;
         d.partials[2 * blockIdx.x] = se;
-        d.partials[2 * blockIdx.x + 1] = sm;
+        d.partials[2 * blockIdx.x + 1] = sm + d.psi_mean * (double)lrows * (double)M;
     }
 }
 
@@ -411,10 +419,12 @@ template <typename K> static cudaError_t set_smem(K kernel, size_t bytes, unsign
     return e;
 }
 
+template <int n> static constexpr size_t smem_bytes() { return sizeof(float2) * padded_len<n>::value; }
+
 template <int M>
 static cudaError_t row_step_impl(const RunDesc *d_runs, int nruns, int L, const TwiddleSet &tw, cudaStream_t st) {
     constexpr int RPC = RowCfg<M>::RPC, NT = RowCfg<M>::NT;
-    const size_t smem = sizeof(float2) * RowCfg<M>::NB * M;
+    constexpr size_t smem = smem_bytes<RowCfg<M>::NB * M>();
     static unsigned mask = 0;
     cudaError_t e = set_smem(k_row_step<M>, smem, mask);
     if (nruns == 0) return e;
@@ -427,7 +437,7 @@ static cudaError_t row_step_impl(const RunDesc *d_runs, int nruns, int L, const 
 template <int M>
 static cudaError_t row_forward_impl(const RunDesc *d_runs, int nruns, int L, const TwiddleSet &tw, cudaStream_t st) {
     constexpr int RPC = RowCfg<M>::RPC, NT = RowCfg<M>::NT;
-    const size_t smem = sizeof(float2) * RPC * M;
+    constexpr size_t smem = smem_bytes<RPC * M>();
     static unsigned mask = 0;
     cudaError_t e = set_smem(k_row_forward<M>, smem, mask);
     if (nruns == 0) return e;
@@ -441,7 +451,7 @@ template <int M>
 static cudaError_t row_analysis_impl(const RunDesc *d_runs, int nruns, int L, const TwiddleSet &tw,
                                      cudaStream_t st) {
     constexpr int RPC = RowCfg<M>::RPC, NT = RowCfg<M>::NT;
-    const size_t smem = sizeof(float2) * 3 * RPC * M;
+    constexpr size_t smem = smem_bytes<3 * RPC * M>();
     static unsigned mask = 0;
     cudaError_t e = set_smem(k_row_analysis<M>, smem, mask);
     if (nruns == 0) return e;
@@ -454,7 +464,7 @@ static cudaError_t row_analysis_impl(const RunDesc *d_runs, int nruns, int L, co
 template <int L, int MODE>
 static cudaError_t col_impl(const RunDesc *d_runs, int nruns, int M, const TwiddleSet &tw, cudaStream_t st) {
     constexpr int C = ColCfg<L>::C, NT = ColCfg<L>::NT;
-    const size_t smem = sizeof(float2) * C * L;
+    constexpr size_t smem = smem_bytes<C * L>();
     static unsigned mask = 0;
     cudaError_t e = set_smem(k_col_step<L, MODE>, smem, mask);
     if (nruns == 0) return e;
@@ -519,7 +529,7 @@ cudaError_t prepare_size(int L, int M) {
 }
 
 int analysis_partials(int L, int M) {
-    int rpc = (TILE / 2) / M;
+    int rpc = (ROW_TILE / 2) / M;
     if (rpc < 1) rpc = 1;
     return (L + rpc - 1) / rpc;
 }

@@ -55,13 +55,13 @@ __global__ void __launch_bounds__(AxisCfg<N>::NT) k_fft_axis(double2 *__restrict
         for (int idx = threadIdx.x; idx < NB * N; idx += NT) {
             const int b = idx / N, e = idx % N;
             const long q = q0 + b;
-            sd[e * NB + b] = q < nseq ? data[q * N + e] : make_double2(0.0, 0.0);
+            sd[spad(e * NB + b)] = q < nseq ? data[q * N + e] : make_double2(0.0, 0.0);
         }
     } else {
         for (int idx = threadIdx.x; idx < NB * N; idx += NT) {
             const int b = idx % NB, e = idx / NB;
             const long q = q0 + b;
-            sd[idx] = q < nseq ? data[(q / stride) * N * stride + (long)e * stride + q % stride] : make_double2(0.0, 0.0);
+            sd[spad(idx)] = q < nseq ? data[(q / stride) * N * stride + (long)e * stride + q % stride] : make_double2(0.0, 0.0);
         }
     }
     __syncthreads();
@@ -70,13 +70,13 @@ __global__ void __launch_bounds__(AxisCfg<N>::NT) k_fft_axis(double2 *__restrict
         for (int idx = threadIdx.x; idx < NB * N; idx += NT) {
             const int b = idx / N, e = idx % N;
             const long q = q0 + b;
-            if (q < nseq) data[q * N + e] = sd[e * NB + b];
+            if (q < nseq) data[q * N + e] = sd[spad(e * NB + b)];
         }
     } else {
         for (int idx = threadIdx.x; idx < NB * N; idx += NT) {
             const int b = idx % NB, e = idx / NB;
             const long q = q0 + b;
-            if (q < nseq) data[(q / stride) * N * stride + (long)e * stride + q % stride] = sd[idx];
+            if (q < nseq) data[(q / stride) * N * stride + (long)e * stride + q % stride] = sd[spad(idx)];
         }
     }
 }
@@ -85,7 +85,7 @@ template <int N>
 static cudaError_t axis_impl(double2 *data, long stride, long nseq, bool fwd, const TwiddleSet &tw, int lg,
                              cudaStream_t st) {
     constexpr int NB = AxisCfg<N>::NB, NT = AxisCfg<N>::NT;
-    const size_t smem = sizeof(double2) * NB * N;
+    const size_t smem = sizeof(double2) * padded_len<NB * N>::value;
     static unsigned mask = 0;
     int dev = 0;
     cudaGetDevice(&dev);

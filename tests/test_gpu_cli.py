@@ -72,7 +72,8 @@ def test_cli_misfit_matches_reference(tmp_path):
                 assert (out / f"{f}_{kd}.pvti").read_text() == open(f"{d}/{f}_{kd}.pvti").read()
                 raw = (out / f"{f}_{kd}_0.vti").read_bytes()
                 rraw = open(f"{d}/{f}_{kd}_0.vti", "rb").read()
-                assert len(raw) == len(rraw) and raw[-40:] == rraw[-40:]
+                trailer = b"\n</AppendedData>\n</VTKFile>\n"
+                assert len(raw) == len(rraw) and raw.endswith(trailer) and rraw.endswith(trailer)
     # energy.txt: same lines (steps) and values within tolerance
     got = [l.split() for l in (out / "energy.txt").read_text().splitlines()]
     ref = [l.split() for l in open(f"{d}/energy.txt").read().splitlines()]
