@@ -135,7 +135,7 @@ def test_fp32_path_matches_fp64_oracle(model, L, M, steps):
     e, d = r.energy()
     oe, od = o.energy()
     assert abs(e - oe) <= 1e-5 * abs(oe) + 1e-7
-    assert abs(d - od) <= 1e-9
+    assert abs(d - od) <= 1e-7 * abs(od)
 
 
 @pytest.mark.parametrize("L,steps", [(128, 200), (256, 200), (1024, 200)])
@@ -183,13 +183,19 @@ def test_fp32_c1_matches_reference_run():
 
 
 def test_mass_is_conserved():
+    """The FP64 k = 0 modes are exact invariants; the FP64 sum over the FP32 real-space
+    field carries a rounding deviation of order 1e-8 that does not accumulate."""
     r = gpu_run(P.MODEL_MISFIT, 256, 256)
     m0 = r.means()
-    r.advance(500, analysis=True)
-    assert r.means() == m0  # the FP64 k = 0 modes are exact invariants of the step
-    _, mass = r.energy()
-    # FP64 reduction of the FP32 field: sum of the deviations from the FP64 mean plus P*mean
-    assert abs(mass - m0[0]) <= 1e-9 * abs(m0[0])
+    devs = []
+    for n in (10, 90, 400, 1500):
+        r.advance(n, analysis=True)
+        assert r.means() == m0
+        _, mass = r.energy()
+        devs.append(abs(mass - m0[0]) / abs(m0[0]))
+    print("relative field-sum deviations:", devs)
+    assert max(devs) <= 1e-7
+    assert devs[-1] <= 10 * max(devs[:2]) + 1e-8  # no drift over 2000 steps
 
 
 def test_batch_results_equal_single_runs():
