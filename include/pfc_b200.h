@@ -116,6 +116,28 @@ int pfc_batch_kernel_times(pfc_batch *b, int reps, double *row_ms, double *col_m
 int pfc_phimax_misfit(const float *phi, const float *con, int L, int M, float dx, float con0, double *out5, int cap,
                       int *count);
 
+/* Allocation-free variant of pfc_phimax_misfit, with no counterpart in the
+ * reference.  It is for callers that cannot allocate device memory: a serving loop
+ * whose admission controller has already committed the whole HBM budget to
+ * resident runs, or a host thread that must not trigger the device-wide
+ * synchronisation that cudaMalloc and cudaFree imply while other streams run.
+ *
+ * The caller passes DEVICE buffers: d_phi and d_con (float[L*M], layout m + M*l)
+ * and d_out5 (cap x 5 doubles, the same records as pfc_phimax_misfit).  The
+ * compaction scratch is a fixed array inside the library (about 32 KB on every GPU
+ * that loads it, held until exit).  L*M must not exceed 4194304 (2048 x 2048);
+ * larger fields are rejected with PFC_E_INVALID.  The function calls no cudaMalloc,
+ * cudaFree or other allocating routine.  It runs on `stream` (a cudaStream_t;
+ * NULL = the default stream) and returns after the atoms are written and *count
+ * is set.
+ *
+ * The first call on a device looks up the scratch array's device address; make
+ * that first call before any stream capture.  All calls on a device share the
+ * array, so calls that overlap on the GPU (from several host threads or streams)
+ * race: serialise them. */
+int pfc_phimax_misfit_noalloc(const float *d_phi, const float *d_con, int L, int M, float dx, float con0,
+                              double *d_out5, int cap, int *count, void *stream);
+
 /* Elastic peak finder (ELA:2802-2921) on a field read from a VTI (layout
  * n + N*(m + M*l)); writes up to cap atoms as 4 doubles (x, y, z, phimax). */
 int pfc_phimax_elastic(const float *phi, int L, int M, int N, float dx, double *out4, int cap, int *count);

@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -722,5 +723,77 @@ extern "C" int pfc_cryst_order(const double *x, const double *y, const double *z
     ATRY(cudaMemcpyAsync(q4, d4, n * sizeof(double), cudaMemcpyDeviceToHost, st));
     ATRY(cudaMemcpyAsync(q6, d6, n * sizeof(double), cudaMemcpyDeviceToHost, st));
     ATRY(cudaStreamSynchronize(st));
+    return PFC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free Misfit peak finder.
+//
+// For callers that cannot allocate device memory: a serving loop whose admission
+// controller has already committed the whole HBM budget to resident runs, or a
+// host thread that must not trigger the device-wide synchronisation that cudaMalloc
+// and cudaFree imply while other streams are busy.  The caller passes device
+// buffers for the fields and the atoms; the compaction's per-block counts and
+// offsets live in the file-scope array below, sized for fields of up to
+// PFC_NOALLOC_MAX_POINTS points (2048 x 2048).  Every GPU that loads the library
+// holds the array (about 32 KB) until the process exits.
+// ---------------------------------------------------------------------------
+namespace pfc {
+static constexpr long NOALLOC_MAX_POINTS = 2048L * 2048L;
+static constexpr int NOALLOC_MAX_BLOCKS = (int)((NOALLOC_MAX_POINTS + CSPAN - 1) / CSPAN);
+// block counts [0, nb), exclusive offsets [nb, 2nb) and the total at [2nb]
+static __device__ __align__(256) int g_noalloc_scratch[2 * NOALLOC_MAX_BLOCKS + 2];
+static std::mutex g_noalloc_mu;
+static int *g_noalloc_addr[64] = {nullptr};  // device address of g_noalloc_scratch, per device ordinal
+}  // namespace pfc
+
+extern "C" int pfc_phimax_misfit_noalloc(const float *d_phi, const float *d_con, int L, int M, float dx, float con0,
+                                         double *d_out5, int cap, int *count, void *stream) {
+    using namespace pfc;
+    if (!d_phi || !d_con || !count || L <= 0 || M <= 0 || cap < 0 || (cap > 0 && !d_out5))
+        return set_error(PFC_E_INVALID, "bad arguments to pfc_phimax_misfit_noalloc");
+    const long n = (long)L * M;
+    if (n > NOALLOC_MAX_POINTS)
+        return set_error(PFC_E_INVALID, "pfc_phimax_misfit_noalloc: L*M = " + std::to_string(n) +
+                                            " exceeds the allocation-free limit of 4194304 points (2048 x 2048)");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_error(e, "cudaGetDevice");
+    if (dev < 0 || dev >= 64) return set_error(PFC_E_INVALID, "device ordinal beyond 63");
+    int *scratch = nullptr;
+    {
+        // first call on this device: look up the array's device address (host code
+        // cannot use the symbol itself as a device pointer)
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            e = cudaGetSymbolAddress((void **)&g_noalloc_addr[dev], g_noalloc_scratch);
+            if (e != cudaSuccess) {
+                g_noalloc_addr[dev] = nullptr;
+                return cuda_error(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+            }
+        }
+        scratch = g_noalloc_addr[dev];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nb = (int)((n + CSPAN - 1) / CSPAN);
+    // k_count writes every count and k_scan every offset and the total before they
+    // are read, so nothing left by an earlier call needs clearing.
+    MisfitPeak f{d_phi, d_con, L, M, dx, con0};
+    k_count<<<nb, CBLK, 0, st>>>(f, n, scratch);
+    k_scan<<<1, 1024, 0, st>>>(scratch, nb, scratch + nb);
+    k_emit<<<nb, CBLK, 0, st>>>(f, n, scratch + nb, d_out5, cap);
+    int total = 0;
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&total, scratch + 2 * nb, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_error(e, "pfc_phimax_misfit_noalloc");
+    if (total == 0) {
+        if (cap > 0) k_misfit_fallback<<<1, 32, 0, st>>>(d_phi, d_con, L, M, dx, con0, d_out5);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return cuda_error(e, "pfc_phimax_misfit_noalloc fallback");
+        total = 1;
+    }
+    *count = total;
     return PFC_OK;
 }

@@ -88,6 +88,8 @@ def lib():
         "pfc_batch_destroy": ([vp], C.c_int),
         "pfc_batch_advance": ([vp, C.c_int], C.c_int),
         "pfc_phimax_misfit": ([fp, fp, C.c_int, C.c_int, C.c_float, C.c_float, dp, C.c_int, P(C.c_int)], C.c_int),
+        "pfc_phimax_misfit_noalloc": ([vp, vp, C.c_int, C.c_int, C.c_float, C.c_float, vp, C.c_int, P(C.c_int), vp],
+                                      C.c_int),
         "pfc_phimax_elastic": ([fp, C.c_int, C.c_int, C.c_int, C.c_float, dp, C.c_int, P(C.c_int)], C.c_int),
         "pfc_elastic3d": ([dp, dp, dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, dp,
                            P(C.c_uint32)], C.c_int),
