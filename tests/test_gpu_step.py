@@ -135,7 +135,8 @@ def test_fp32_path_matches_fp64_oracle(model, L, M, steps):
     e, d = r.energy()
     oe, od = o.energy()
     assert abs(e - oe) <= 1e-5 * abs(oe) + 1e-7
-    assert abs(d - od) <= 1e-7 * abs(od)
+    # FP32 field-sum rounding scales with the field amplitude, not the (possibly small) mean
+    assert abs(d - od) <= 1e-7 * abs(od) + 5e-9
 
 
 @pytest.mark.parametrize("L,steps", [(128, 200), (256, 200), (1024, 200)])
