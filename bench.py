@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--grid", type=int, default=GRID)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-plain", action="store_true")
     return ap.parse_args()
 
 
@@ -317,6 +318,18 @@ def run_ours(args):
         "gpu_launches": 2 * args.steps,
         "clocks": clk,
     }
+    # the plain FP64 GPU path (one run, the reference's step structure) on the same grid
+    if not args.no_fp64_plain:
+        r64 = P.Run(P.default_params(P.MODEL_MISFIT, L=G, M=G, N=1, seed=1000, device=dev, precision=P.FP64))
+        r64.advance(3)
+        n64 = 20
+        ms64 = r64.advance_timed(n64)
+        r64.close()
+        fp64_sps = n64 / (ms64 / 1000.0)
+        line["fp64_plain"] = {"steps_per_s": round(fp64_sps, 2),
+                              "what": "one Misfit run, plain FP64 path (13 complex-double 3-D DFTs + pointwise "
+                                      "kernels per step, reference roundings), CUDA events",
+                              "batched_fp32_over_fp64_plain": round(value / dist.world / fp64_sps, 2)}
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(G)

@@ -72,6 +72,10 @@ int pfc_run_destroy(pfc_run *r);
  * last step also prepares the checkpoint analysis (real fields, energy, mass). */
 int pfc_run_advance(pfc_run *r, int nsteps, int analysis);
 
+/* pfc_run_advance(r, nsteps, 0) bracketed by CUDA events on the run's stream;
+ * *ms receives the device time.  (Measurement hook; no reference counterpart.) */
+int pfc_run_advance_timed(pfc_run *r, int nsteps, float *ms);
+
 /* Steps taken so far. */
 int pfc_run_steps(const pfc_run *r, int *steps);
 

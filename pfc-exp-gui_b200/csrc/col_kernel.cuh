@@ -1,0 +1,133 @@
+// col_kernel.cuh -- the column kernel of the fused FP32 step (included by step_fp32.cu).
+//
+// One CTA per tile of L rows x C packed columns of one run (a contiguous block of
+// the row-space layout).  For phi and then con:
+//   the field's tile is copied HBM -> parked buffer P (float4, coalesced) and
+//     transformed forward in place (scratch s for the intermediate stages),
+//   its nonlinear term's tile is copied HBM -> s and transformed forward in place,
+//   the semi-implicit update runs in place in P (MAINEQUATIONC2_NOI / C2MIX,
+//     MIS:983-1014, CVD:865-886) with the FP64-built factors of the shared
+//     coefficient table,
+//   each output is an inverse transform whose first stage reads P through a
+//     multiplier (1, C2A, C2B for phi, MIS:807-810; 1 and the -i k gradients for
+//     con at checkpoints, MIS:884-889) into s, copied s -> HBM (float4).
+// Staging the tiles through shared memory keeps every transform shared-memory to
+// shared-memory, which fits 128 registers per thread without spills: two CTAs of
+// 256 threads (2 x 69 KB of shared memory) per SM.
+
+// multiplier applied by an inverse transform's first stage: P * g(l, km)
+struct ScaleByTable {
+    const float2 *tab;  // kc2 tile (c2a, c2b)
+    int C, which;       // which: 0 = .x, 1 = .y
+    __device__ __forceinline__ float2 operator()(int e, int b, float2 v) const {
+        const float2 t = tab[e * C + b];
+        const float g = which == 0 ? t.x : t.y;
+        return make_float2(v.x * g, v.y * g);
+    }
+};
+// -i k P along l (which = 0, krefl) or m (which = 1, krefm)
+struct GradientOf {
+    const float *krefl, *krefm;
+    int km0, H, which;
+    __device__ __forceinline__ float2 operator()(int e, int b, float2 v) const {
+        const int km = km0 + b;
+        const float kv = which == 0 ? krefl[e] : krefm[km <= H ? km : 0];
+        return make_float2(kv * v.y, -kv * v.x);
+    }
+};
+
+template <int L, int C, int NT> __device__ __forceinline__ void tile_in(const float2 *__restrict__ g, float2 *sm) {
+    __syncthreads();
+    const float4 *g4 = reinterpret_cast<const float4 *>(g);
+    for (int i = threadIdx.x; i < L * C / 2; i += NT) {
+        const float4 v = g4[i];
+        sm[spad(2 * i)] = make_float2(v.x, v.y);
+        sm[spad(2 * i + 1)] = make_float2(v.z, v.w);
+    }
+    __syncthreads();
+}
+template <int L, int C, int NT> __device__ __forceinline__ void tile_out(const float2 *sm, float2 *__restrict__ g) {
+    float4 *g4 = reinterpret_cast<float4 *>(g);
+    for (int i = threadIdx.x; i < L * C / 2; i += NT) {
+        const float2 a = sm[spad(2 * i)], b = sm[spad(2 * i + 1)];
+        g4[i] = make_float4(a.x, a.y, b.x, b.y);
+    }
+}
+
+template <int L, int MODE>
+__global__ void __launch_bounds__(ColCfg<L>::NT, 2) k_col_step(const RunDesc *__restrict__ runs,
+                                                                const float2 *__restrict__ tw) {
+    constexpr int C = ColCfg<L>::C, NT = ColCfg<L>::NT;
+    constexpr int SPAD = padded_len<C * L>::value;
+    typedef RegOut<L, C, NT> RO;  // register scratch the transforms need for their last stage
+    extern __shared__ float2 smem[];
+    float2 *s = smem;          // FFT scratch
+    float2 *Pk = smem + SPAD;  // parked spectrum
+    const RunDesc &d = runs[blockIdx.y];
+    const int H = d.M / 2;
+    const long tile = (long)blockIdx.x * L * C;
+    const int km0 = blockIdx.x * C;
+    const float invL = 1.0f / (float)L;
+    const float mn_dt = d.k.dynamic_mn * d.dt, mc_dt = d.k.dynamic_mc * d.dt;
+    float2 b[RO::PER_T][RO::R];
+
+    // ---- phi ----
+    tile_in<L, C, NT>(d.psi + tile, Pk);
+    fft<L, C, NT, true, SP_SMEM, SP_SMEM>(Pk, s, Pk, tw, b);
+    if (MODE != COL_PREPARE) {
+        tile_in<L, C, NT>(d.inn + tile, s);
+        fft<L, C, NT, true, SP_SMEM, SP_SMEM>(s, s, s, tw, b);
+    }
+    for (int e = threadIdx.x; e < L * C; e += NT) {
+        const int l = e / C, c = e % C, km = km0 + c;
+        const int pi = spad(e);
+        float2 v = Pk[pi];
+        if (MODE != COL_PREPARE) {
+            // (psi^ - Mn dt k^2 N^) / (1 + Mn dt k^2) / L; the FP64-built factor is 0 at k = 0
+            const float kl = d.krefl[l], kmv = d.krefm[km <= H ? km : 0];
+            const float an = mn_dt * (kl * kl + kmv * kmv);
+            const float2 nh = s[pi];
+            const float f = d.kden[tile + e].x;
+            v = make_float2((v.x - an * nh.x) * f, (v.y - an * nh.y) * f);
+        } else {
+            v = (l == 0 && km == 0) ? make_float2(0.f, 0.f) : cscale(v, invL);
+        }
+        Pk[pi] = v;
+    }
+    __syncthreads();
+    if (MODE != COL_PREPARE) {
+        fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b);
+        tile_out<L, C, NT>(s, d.psi + tile);
+    }
+    fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, ScaleByTable{d.kc2 + tile, C, 0});
+    tile_out<L, C, NT>(s, d.ca + tile);
+    fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, ScaleByTable{d.kc2 + tile, C, 1});
+    tile_out<L, C, NT>(s, d.cb + tile);
+    if (MODE == COL_PREPARE) return;
+
+    // ---- con ----
+    tile_in<L, C, NT>(d.con + tile, Pk);
+    fft<L, C, NT, true, SP_SMEM, SP_SMEM>(Pk, s, Pk, tw, b);
+    tile_in<L, C, NT>(d.inc + tile, s);
+    fft<L, C, NT, true, SP_SMEM, SP_SMEM>(s, s, s, tw, b);
+    for (int e = threadIdx.x; e < L * C; e += NT) {
+        const int l = e / C, c = e % C, km = km0 + c;
+        const int pi = spad(e);
+        // (c^ - Mc dt k^2 I^) / (1 + Mc dt alpha k^4) / L; the FP64-built factor is 0 at k = 0
+        const float kl = d.krefl[l], kmv = d.krefm[km <= H ? km : 0];
+        const float ac = mc_dt * (kl * kl + kmv * kmv);
+        const float f = d.kden[tile + e].y;
+        const float2 ih = s[pi];
+        const float2 v = Pk[pi];
+        Pk[pi] = make_float2((v.x - ac * ih.x) * f, (v.y - ac * ih.y) * f);
+    }
+    __syncthreads();
+    fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b);
+    tile_out<L, C, NT>(s, d.con + tile);
+    if (MODE == COL_STEP_CHECKPOINT) {
+        fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, GradientOf{d.krefl, d.krefm, km0, H, 0});
+        tile_out<L, C, NT>(s, d.gx + tile);
+        fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, GradientOf{d.krefl, d.krefm, km0, H, 1});
+        tile_out<L, C, NT>(s, d.gy + tile);
+    }
+}

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -161,7 +162,77 @@ static C2Params c2_params(float sig, float g1, float g2, float k1, float k2, flo
     p.k2 = k2;
     p.i1 = (float)(1.0 / (double)(2 * g1 * g1));
     p.i2 = (float)(1.0 / (double)(2 * g2 * g2));
+    p.q1 = sig / s1;
+    p.q2 = sig / s2;
+    p.gg1 = 2 * g1 * g1;
+    p.gg2 = 2 * g2 * g2;
     return p;
+}
+
+// ---------------------------------------------------------------------------
+// Shared per k-point coefficient tables: runs with the same model, grid, sig, dt
+// and dx use one table, so a batch of such runs reads it from L2.
+// ---------------------------------------------------------------------------
+struct KcoefKey {
+    int device, model, L, M;
+    uint32_t sig, dt, dx;
+    bool operator<(const KcoefKey &o) const {
+        return std::tie(device, model, L, M, sig, dt, dx) < std::tie(o.device, o.model, o.L, o.M, o.sig, o.dt, o.dx);
+    }
+};
+struct KcoefEntry {
+    float2 *ptr = nullptr;
+    int refs = 0;
+};
+static std::mutex g_kcoef_mu;
+static std::map<KcoefKey, KcoefEntry> g_kcoef;
+
+static uint32_t fbits(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, sizeof(u));
+    return u;
+}
+
+static KcoefKey kcoef_key(const pfc_run *r) {
+    return KcoefKey{r->p.device, r->p.model, r->L, r->M, fbits(r->p.sig), fbits(r->p.dt), fbits(r->p.dx)};
+}
+
+// Table for run r (its descriptor must already be on the device); built on first use.
+static int acquire_kcoef(pfc_run *r) {
+    std::lock_guard<std::mutex> lk(g_kcoef_mu);
+    KcoefEntry &e = g_kcoef[kcoef_key(r)];
+    if (!e.ptr) {
+        const size_t bytes = 2 * (size_t)r->desc.T * r->L * r->desc.CT * sizeof(float2);
+        cudaError_t ce = cudaMalloc(&e.ptr, bytes);
+        if (ce != cudaSuccess) {
+            e.ptr = nullptr;
+            return set_error(PFC_E_NOMEM, std::string("cudaMalloc coefficient table: ") + cudaGetErrorString(ce));
+        }
+        ce = launch_build_kcoef(r->d_desc, e.ptr, e.ptr + (size_t)r->desc.T * r->L * r->desc.CT, r->stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(r->stream);
+        if (ce != cudaSuccess) {
+            cudaFree(e.ptr);
+            e.ptr = nullptr;
+            return cuda_error(ce, "building the coefficient table");
+        }
+    }
+    e.refs++;
+    r->desc.kden = e.ptr;
+    r->desc.kc2 = e.ptr + (size_t)r->desc.T * r->L * r->desc.CT;
+    return PFC_OK;
+}
+
+static void release_kcoef(pfc_run *r) {
+    if (!r->desc.kden) return;
+    std::lock_guard<std::mutex> lk(g_kcoef_mu);
+    auto it = g_kcoef.find(kcoef_key(r));
+    if (it == g_kcoef.end()) return;
+    if (--it->second.refs <= 0) {
+        cudaFree(it->second.ptr);
+        g_kcoef.erase(it);
+    }
+    r->desc.kden = nullptr;
+    r->desc.kc2 = nullptr;
 }
 
 // k-vectors exactly as MIS:455-462 (float storage, double arithmetic).
@@ -236,6 +307,7 @@ extern "C" int pfc_default_params(int model, pfc_run_params *p) {
 
 static void free_run(pfc_run *r) {
     if (!r) return;
+    release_kcoef(r);
     if (r->dev_mem) cudaFree(r->dev_mem);
     if (r->f64) fp64_destroy(r->f64);
     delete r;
@@ -338,6 +410,18 @@ extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) {
     d.k = r->k;
     d.c2a = r->c2a;
     d.c2b = r->c2b;
+    if (fp32) {
+        cudaError_t ce = cudaMemcpyAsync(r->d_desc, &d, sizeof(RunDesc), cudaMemcpyHostToDevice, r->stream);
+        if (ce != cudaSuccess) {
+            free_run(r);
+            return cuda_error(ce, "descriptor upload");
+        }
+        rc = acquire_kcoef(r);
+        if (rc != PFC_OK) {
+            free_run(r);
+            return rc;
+        }
+    }
 
     if (!fp32) {
         rc = fp64_create(r);
@@ -500,6 +584,26 @@ extern "C" int pfc_run_advance(pfc_run *r, int nsteps, int analysis) {
     PFC_CUDA_TRY(cudaSetDevice(r->p.device));
     if (r->p.precision != PFC_PRECISION_FP32) return fp64_advance(r, nsteps);
     return fp32_advance(r, nsteps, analysis);
+}
+
+extern "C" int pfc_run_advance_timed(pfc_run *r, int nsteps, float *ms) {
+    if (!r || !ms || nsteps < 0) return set_error(PFC_E_INVALID, "bad argument");
+    PFC_CUDA_TRY(cudaSetDevice(r->p.device));
+    cudaEvent_t e0, e1;
+    PFC_CUDA_TRY(cudaEventCreate(&e0));
+    PFC_CUDA_TRY(cudaEventCreate(&e1));
+    int rc = PFC_OK;
+    cudaError_t e = cudaStreamSynchronize(r->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, r->stream);
+    if (e == cudaSuccess) rc = pfc_run_advance(r, nsteps, 0);
+    if (e == cudaSuccess && rc == PFC_OK) e = cudaEventRecord(e1, r->stream);
+    if (e == cudaSuccess && rc == PFC_OK) e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess && rc == PFC_OK) e = cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != PFC_OK) return rc;
+    if (e != cudaSuccess) return cuda_error(e, "pfc_run_advance_timed");
+    return PFC_OK;
 }
 
 extern "C" int pfc_run_steps(const pfc_run *r, int *steps) {

@@ -205,16 +205,21 @@ template <typename T> struct nodeduce {
     typedef T type;
 };
 
+// Transform applied to each value a transform's first stage loads: v -> f(e, b, v)
+// with e the element index along the sequence and b the sequence.
+struct Identity {
+    template <typename C> __device__ __forceinline__ C operator()(int, int, C v) const { return v; }
+};
+
 // One Stockham stage of radix R on NB interleaved sequences of length N.
 // IN/OUT: SP_SMEM (padded shared array), SP_GLOBAL (plain array).  OUT may also be
 // SP_REGS: the stage's outputs are left in v (element e = j + r*Ns of sequence b,
 // item w = tid + q*NT, b = w % NB, j = w / NB) and nothing is stored.
 // A stage whose input and output are the same shared array synchronises between
 // its loads and its stores.
-template <int N, int NB, int NT, int R, bool FWD, int IN, int OUT, typename C>
+template <int N, int NB, int NT, int R, bool FWD, int IN, int OUT, typename C, typename XF = Identity>
 __device__ __forceinline__ void stage(const C *__restrict__ in, typename nodeduce<C>::type *out, const C *__restrict__ tw,
-                                      int Ns,
-                                      C (&v)[StageShape<N, NB, NT, R>::PER_T][R]) {
+                                      int Ns, C (&v)[StageShape<N, NB, NT, R>::PER_T][R], XF xf = XF()) {
     typedef StageShape<N, NB, NT, R> S;
     const int tid = threadIdx.x;
     // a stage that only writes shared memory must not overtake earlier readers of it
@@ -226,8 +231,9 @@ __device__ __forceinline__ void stage(const C *__restrict__ in, typename nodeduc
             const int b = w % NB, j = w / NB;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                const int e = (j + r * (N / R)) * NB + b;
-                v[q][r] = IN == SP_SMEM ? in[spad(e)] : in[e];
+                const int ei = j + r * (N / R);
+                const int e = ei * NB + b;
+                v[q][r] = xf(ei, b, IN == SP_SMEM ? in[spad(e)] : in[e]);
             }
         }
     }
@@ -272,42 +278,36 @@ template <int N, int NB, int NT> struct RegOut {
 };
 
 // Full transform of NB interleaved length-N sequences.
-//   IN  = SP_GLOBAL: first stage reads `src` (global); SP_SMEM: reads padded `s`.
-//   OUT = SP_GLOBAL: last stage writes `dst` (global); SP_SMEM: writes `s`;
-//         SP_REGS: last stage output stays in `last` (see RegOut for the layout).
-// Intermediate stages run in place in the padded shared array `s`.  Callers must
-// __syncthreads() before a transform that reads data they wrote to `s`; the
-// routine leaves `s` synchronised when it returns.
-template <int N, int NB, int NT, bool FWD, int IN, int OUT, typename C>
+//   IN  = SP_GLOBAL: the first stage reads global `src`; SP_SMEM: reads the padded
+//         shared array `src` (which may be `s` itself or another buffer).  Every
+//         value it loads passes through xf(e, b, v).
+//   OUT = SP_GLOBAL: the last stage writes global `dst`; SP_SMEM: writes the padded
+//         shared array `dst`; SP_REGS: the output stays in `last` (RegOut layout).
+// Intermediate stages run in place in the padded shared scratch `s`.  Callers must
+// __syncthreads() before a transform that reads shared data they wrote; a
+// transform whose last stage writes shared memory synchronises before returning.
+template <int N, int NB, int NT, bool FWD, int IN, int OUT, typename C, typename XF = Identity>
 __device__ __forceinline__ void fft(const typename nodeduce<C>::type *src, C *s, typename nodeduce<C>::type *dst,
                                     const C *__restrict__ tw,
-                                    C (&last)[RegOut<N, NB, NT>::PER_T][RegOut<N, NB, NT>::R]) {
+                                    C (&last)[RegOut<N, NB, NT>::PER_T][RegOut<N, NB, NT>::R], XF xf = XF()) {
     typedef radix_plan<N> P;
     constexpr int ST = P::stages;
     int Ns = 1;
-    // stage index i: radix 16 for i < n16, else tail radix
     if constexpr (ST == 1) {
-        if constexpr (OUT == SP_REGS)
-            stage<N, NB, NT, P::last_radix, FWD, IN, SP_REGS>(IN == SP_GLOBAL ? src : s, nullptr, tw, Ns, last);
-        else
-            stage<N, NB, NT, P::last_radix, FWD, IN, OUT>(IN == SP_GLOBAL ? src : s, OUT == SP_GLOBAL ? dst : s, tw, Ns,
-                                                          last);
+        stage<N, NB, NT, P::last_radix, FWD, IN, OUT>(src, dst, tw, Ns, last, xf);
     } else {
         typedef StageShape<N, NB, NT, 16> S16;
         C v[S16::PER_T][16];
-        // first stage (radix 16)
-        stage<N, NB, NT, 16, FWD, IN, SP_SMEM>(IN == SP_GLOBAL ? src : s, s, tw, Ns, v);
+        // first stage (radix 16): src -> scratch
+        stage<N, NB, NT, 16, FWD, IN, SP_SMEM>(src, s, tw, Ns, v, xf);
         Ns *= 16;
 #pragma unroll
         for (int i = 1; i < ST - 1; ++i) {
             stage<N, NB, NT, 16, FWD, SP_SMEM, SP_SMEM>(s, s, tw, Ns, v);
             Ns *= 16;
         }
-        // last stage
-        if constexpr (OUT == SP_REGS)
-            stage<N, NB, NT, P::last_radix, FWD, SP_SMEM, SP_REGS>(s, nullptr, tw, Ns, last);
-        else
-            stage<N, NB, NT, P::last_radix, FWD, SP_SMEM, OUT>(s, OUT == SP_GLOBAL ? dst : s, tw, Ns, last);
+        // last stage: scratch -> dst / registers
+        stage<N, NB, NT, P::last_radix, FWD, SP_SMEM, OUT>(s, dst, tw, Ns, last);
     }
 }
 
@@ -315,7 +315,7 @@ __device__ __forceinline__ void fft(const typename nodeduce<C>::type *src, C *s,
 template <int N, int NB, int NT, bool FWD, typename C>
 __device__ __forceinline__ void fft_smem(C *s, const C *__restrict__ tw) {
     C last[RegOut<N, NB, NT>::PER_T][RegOut<N, NB, NT>::R];
-    fft<N, NB, NT, FWD, SP_SMEM, SP_SMEM>(nullptr, s, nullptr, tw, last);
+    fft<N, NB, NT, FWD, SP_SMEM, SP_SMEM>(s, s, s, tw, last);
 }
 
 }  // namespace pfc

@@ -28,6 +28,8 @@ struct ModelCoefs {
 // C2(k) = e1 * exp(-(|k| - k1)^2 * i1) for |k| <= kc, else e2 * exp(-(|k| - k2)^2 * i2).
 struct C2Params {
     float kc, e1, e2, k1, k2, i1, i2;
+    float q1, q2;    // sig / sigM1, sig / sigM2 (float quotients, as the reference forms them)
+    float gg1, gg2;  // 2 * g1 * g1, 2 * g2 * g2 (float products)
 };
 
 struct RunDesc {
@@ -41,6 +43,10 @@ struct RunDesc {
     float *psi_real, *con_real;
     // reference k-vectors (float), lengths L and M
     const float *krefl, *krefm;
+    // per k-point coefficients in the row-space tile layout (0 at k = 0, the FP64-held mode):
+    //   kden = ((float)(1/(1 + Mn dt k^2) / L), (float)(1/(1 + Mc dt alpha k^4) / L))
+    //   kc2  = (C2A(k), C2B(k)) as the reference's float tables
+    const float2 *kden, *kc2;
     // FP64 means of phi and con (the k = 0 modes / P), and their float roundings
     double psi_mean, con_mean;
     float psi_mean_f, con_mean_f;
@@ -64,6 +70,9 @@ cudaError_t launch_col_step(const RunDesc *d_runs, int nruns, int L, int M, int 
 cudaError_t launch_row_forward(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw, cudaStream_t s);
 cudaError_t launch_row_analysis(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw,
                                 cudaStream_t s);
+
+// Build the per k-point coefficient table of one run (layout and values as RunDesc::kcoef).
+cudaError_t launch_build_kcoef(const RunDesc *d_run, float2 *kden, float2 *kc2, cudaStream_t s);
 
 // column-kernel modes
 enum ColMode : int { COL_STEP = 0, COL_PREPARE = 1, COL_STEP_CHECKPOINT = 2 };

@@ -51,14 +51,49 @@ __device__ __forceinline__ long rs_index(const RunDesc &d, int l, int km) {
     return ((long)(km >> d.lct) * d.L + l) * d.CT + (km & (d.CT - 1));
 }
 
-__device__ __forceinline__ float c2eval(const C2Params &p, float ks) {
-    const float s = sqrtf(ks);
+// C2 correlation kernel at |k| = sqrtf(ks), as the reference builds its float table
+// (misfit_uniform_time_seed_fftw_early.cpp:700-750): exp in double of float arguments.
+__device__ __forceinline__ float c2_ref(const C2Params &p, float ks) {
+    const float s = __fsqrt_rn(ks);
     if (s <= p.kc) {
-        const float d = s - p.k1;
-        return p.e1 * expf(-d * d * p.i1);
+        const double d = (double)__fsub_rn(s, p.k1);
+        return (float)(exp(-(double)p.q1 * (double)p.q1) * exp(-(d * d) / (double)p.gg1));
     }
-    const float d = s - p.k2;
-    return p.e2 * expf(-d * d * p.i2);
+    const double d = (double)__fsub_rn(s, p.k2);
+    return (float)(exp(-(double)p.q2 * (double)p.q2) * exp(-(d * d) / (double)p.gg2));
+}
+
+// Per k-point coefficients of one run (RunDesc::kcoef), built once in FP64 and rounded.
+// ks and the k^4 product use the reference's float operation order (ks, MAINEQUATIONC2_NOI,
+// MIS:1002-1010); the intrinsics keep them from being contracted into FMAs.
+__global__ void k_build_kcoef(const RunDesc *__restrict__ run, float2 *__restrict__ den, float2 *__restrict__ c2) {
+    const RunDesc &d = *run;
+    const int H = d.M / 2;
+    const long tile = (long)d.L * d.CT, total = (long)d.T * tile;
+    const float mn_dt = __fmul_rn(d.k.dynamic_mn, d.dt), mc_dt = __fmul_rn(d.k.dynamic_mc, d.dt);
+    const float mc_dt_alpha = __fmul_rn(mc_dt, d.k.para_alpha);
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int t = (int)(i / tile), rem = (int)(i % tile);
+        const int l = rem / d.CT, km = t * d.CT + rem % d.CT;
+        if (km > H || (l == 0 && km == 0)) {
+            den[i] = make_float2(0.f, 0.f);
+            c2[i] = make_float2(0.f, 0.f);
+            continue;
+        }
+        const float kl = d.krefl[l], kmv = d.krefm[km];
+        const float ks = __fadd_rn(__fmul_rn(kl, kl), __fmul_rn(kmv, kmv));
+        const float an = __fmul_rn(mn_dt, ks);
+        const float dc = __fmul_rn(__fmul_rn(mc_dt_alpha, ks), ks);
+        const float fn = (float)((1.0 / (1.0 + (double)an)) / (double)d.L);
+        const float fc = (float)((1.0 / (1.0 + (double)dc)) / (double)d.L);
+        den[i] = make_float2(fn, fc);
+        c2[i] = make_float2(c2_ref(d.c2a, ks), c2_ref(d.c2b, ks));
+    }
+}
+
+cudaError_t launch_build_kcoef(const RunDesc *d_run, float2 *kden, float2 *kc2, cudaStream_t s) {
+    k_build_kcoef<<<148 * 4, 256, 0, s>>>(d_run, kden, kc2);
+    return cudaGetLastError();
 }
 
 // Nonlinear chemical-potential terms at one grid point (MIS:773-874), FP32.
@@ -211,109 +246,7 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_forward(const RunDesc *__
 // ---------------------------------------------------------------------------
 // Column kernel.
 // ---------------------------------------------------------------------------
-template <int L, int MODE>
-__global__ void __launch_bounds__(ColCfg<L>::NT) k_col_step(const RunDesc *__restrict__ runs,
-                                                             const float2 *__restrict__ tw) {
-    constexpr int C = ColCfg<L>::C, NT = ColCfg<L>::NT;
-    typedef RegOut<L, C, NT> RO;
-    extern __shared__ float2 s[];
-    const RunDesc &d = runs[blockIdx.y];
-    const int H = d.M / 2;
-    const long tile = (long)blockIdx.x * L * C;
-    const int km0 = blockIdx.x * C;
-    const float invL = 1.0f / (float)L;
-    const float mn_dt = d.k.dynamic_mn * d.dt, mc_dt = d.k.dynamic_mc * d.dt;
-    const float mc_dt_alpha = mc_dt * d.k.para_alpha;
-    float2 a[RO::PER_T][RO::R], b[RO::PER_T][RO::R];
-
-    // element held by (q, r) after a transform that ends in registers
-#define COL_ELEM(q, r, l, km)                              \
-    const int _w = threadIdx.x + (q) * NT;                 \
-    const int l = (_w / C) + (r) * RO::NS, km = km0 + _w % C;
-
-    // ---- phi: forward column FFTs of psi and inn, update ----
-    fft<L, C, NT, true, SP_GLOBAL, SP_REGS>(d.psi + tile, s, nullptr, tw, a);
-    if (MODE != COL_PREPARE) fft<L, C, NT, true, SP_GLOBAL, SP_REGS>(d.inn + tile, s, nullptr, tw, b);
-#pragma unroll
-    for (int q = 0; q < RO::PER_T; ++q)
-#pragma unroll
-        for (int r = 0; r < RO::R; ++r) {
-            COL_ELEM(q, r, l, km)
-            float2 v = a[q][r];
-            if (MODE != COL_PREPARE) {
-                const float kl = d.krefl[l], kmv = km <= H ? d.krefm[km] : 0.0f;
-                const float ks = kl * kl + kmv * kmv;
-                const float an = mn_dt * ks;
-                const float den = (float)(1.0 / (1.0 + (double)an));
-                const float2 nh = b[q][r];
-                v = make_float2((v.x - an * nh.x) * den, (v.y - an * nh.y) * den);
-            }
-            if (l == 0 && km == 0) v = make_float2(0.f, 0.f);
-            a[q][r] = cscale(v, invL);
-        }
-    // outputs: psi' (not in PREPARE mode), c2a = C2A psi', c2b = C2B psi'
-#pragma unroll
-    for (int pass = (MODE == COL_PREPARE ? 1 : 0); pass < 3; ++pass) {
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < RO::PER_T; ++q)
-#pragma unroll
-            for (int r = 0; r < RO::R; ++r) {
-                COL_ELEM(q, r, l, km)
-                float g = 1.0f;
-                if (pass > 0) {
-                    const float kl = d.krefl[l], kmv = km <= H ? d.krefm[km] : 0.0f;
-                    g = c2eval(pass == 1 ? d.c2a : d.c2b, kl * kl + kmv * kmv);
-                }
-                s[spad(l * C + (km - km0))] = cscale(a[q][r], g);
-            }
-        __syncthreads();
-        float2 *dst = pass == 0 ? d.psi : (pass == 1 ? d.ca : d.cb);
-        fft<L, C, NT, false, SP_SMEM, SP_GLOBAL>(nullptr, s, dst + tile, tw, b);
-    }
-    if (MODE == COL_PREPARE) return;
-
-    // ---- con ----
-    fft<L, C, NT, true, SP_GLOBAL, SP_REGS>(d.con + tile, s, nullptr, tw, a);
-    fft<L, C, NT, true, SP_GLOBAL, SP_REGS>(d.inc + tile, s, nullptr, tw, b);
-#pragma unroll
-    for (int q = 0; q < RO::PER_T; ++q)
-#pragma unroll
-        for (int r = 0; r < RO::R; ++r) {
-            COL_ELEM(q, r, l, km)
-            const float kl = d.krefl[l], kmv = km <= H ? d.krefm[km] : 0.0f;
-            const float ks = kl * kl + kmv * kmv;
-            const float ac = mc_dt * ks;
-            const float dc = mc_dt_alpha * ks * ks;
-            const float den = (float)(1.0 / (1.0 + (double)dc));
-            const float2 ih = b[q][r];
-            float2 v = make_float2((a[q][r].x - ac * ih.x) * den, (a[q][r].y - ac * ih.y) * den);
-            if (l == 0 && km == 0) v = make_float2(0.f, 0.f);
-            a[q][r] = cscale(v, invL);
-        }
-    constexpr int NOUT = MODE == COL_STEP_CHECKPOINT ? 3 : 1;
-#pragma unroll
-    for (int pass = 0; pass < NOUT; ++pass) {
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < RO::PER_T; ++q)
-#pragma unroll
-            for (int r = 0; r < RO::R; ++r) {
-                COL_ELEM(q, r, l, km)
-                float2 v = a[q][r];
-                if (pass > 0) {
-                    // gradient of con, -i k con^ along l (gra1) and m (gra2), MIS:884-889
-                    const float kv = pass == 1 ? d.krefl[l] : (km <= H ? d.krefm[km] : 0.0f);
-                    v = make_float2(kv * v.y, -kv * v.x);
-                }
-                s[spad(l * C + (km - km0))] = v;
-            }
-        __syncthreads();
-        float2 *dst = pass == 0 ? d.con : (pass == 1 ? d.gx : d.gy);
-        fft<L, C, NT, false, SP_SMEM, SP_GLOBAL>(nullptr, s, dst + tile, tw, b);
-    }
-#undef COL_ELEM
-}
+#include "col_kernel.cuh"
 
 // ---------------------------------------------------------------------------
 // Analysis row kernel (checkpoints): real fields, energy density and mass.
@@ -464,7 +397,7 @@ static cudaError_t row_analysis_impl(const RunDesc *d_runs, int nruns, int L, co
 template <int L, int MODE>
 static cudaError_t col_impl(const RunDesc *d_runs, int nruns, int M, const TwiddleSet &tw, cudaStream_t st) {
     constexpr int C = ColCfg<L>::C, NT = ColCfg<L>::NT;
-    constexpr size_t smem = smem_bytes<C * L>();
+    constexpr size_t smem = 2 * smem_bytes<C * L>();
     static unsigned mask = 0;
     cudaError_t e = set_smem(k_col_step<L, MODE>, smem, mask);
     if (nruns == 0) return e;

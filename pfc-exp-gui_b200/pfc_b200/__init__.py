@@ -79,6 +79,7 @@ def lib():
         "pfc_run_destroy": ([vp], C.c_int),
         "pfc_run_advance": ([vp, C.c_int, C.c_int], C.c_int),
         "pfc_run_steps": ([vp, P(C.c_int)], C.c_int),
+        "pfc_run_advance_timed": ([vp, C.c_int, P(C.c_float)], C.c_int),
         "pfc_run_get_fields": ([vp, dp, dp], C.c_int),
         "pfc_run_get_fields_f32": ([vp, fp, fp], C.c_int),
         "pfc_run_set_fields": ([vp, dp, dp], C.c_int),
@@ -152,6 +153,12 @@ class Run:
 
     def advance(self, nsteps: int = 1, analysis: bool = False):
         _check(lib().pfc_run_advance(self.h, nsteps, 1 if analysis else 0), "pfc_run_advance")
+
+    def advance_timed(self, nsteps: int) -> float:
+        """Advance and return the device time in ms (CUDA events on the run's stream)."""
+        ms = C.c_float()
+        _check(lib().pfc_run_advance_timed(self.h, nsteps, C.byref(ms)), "pfc_run_advance_timed")
+        return ms.value
 
     @property
     def steps(self) -> int:
