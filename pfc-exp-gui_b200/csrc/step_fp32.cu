@@ -134,6 +134,57 @@ __device__ __forceinline__ void build_pair(float2 *s, int NB, int b, int k, int 
     }
 }
 
+// build_pair in two passes, for a Y whose scale is known only after all of the
+// block's values are seen: park_pair leaves X at Z[k] and Y at Z[M-k] (at k = 0 and
+// M/2 the only parts build_pair uses, (X.x, Y.x), at Z[k]); unpark_pair, run later
+// by the same thread for the same (b, k), writes build_pair(X, g * Y) over them.
+__device__ __forceinline__ void park_pair(float2 *s, int NB, int b, int k, int M, float2 X, float2 Y) {
+    if (k == 0 || k == M / 2) {
+        s[spad(k * NB + b)] = make_float2(X.x, Y.x);
+    } else {
+        s[spad(k * NB + b)] = X;
+        s[spad((M - k) * NB + b)] = Y;
+    }
+}
+__device__ __forceinline__ void unpark_pair(float2 *s, int NB, int b, int k, int M, float g) {
+    if (k == 0 || k == M / 2) {
+        s[spad(k * NB + b)].y *= g;
+    } else {
+        const float2 X = s[spad(k * NB + b)], Y = s[spad((M - k) * NB + b)];
+        build_pair(s, NB, b, k, M, X, make_float2(Y.x * g, Y.y * g));
+    }
+}
+
+// Balancing the two members of a packed transform.  The rounding error a transform
+// adds to either member of x + i y is set by the larger of the two, so a member that
+// is much smaller than its partner (con beside phi in Misfit runs: deviations about
+// 60 times smaller) loses that many bits.  The smaller member therefore rides as
+// 2^e * y, e = exponent(max|x|) - exponent(max|y|); multiplying by 2^e and 2^-e is
+// exact, so the balancing adds no rounding of its own.
+// The exponent is chosen in the same kernel from the values being packed: the
+// fields change by orders of magnitude within a few steps early in a run, so an
+// exponent carried over from the previous step can push y far past x.
+__device__ __forceinline__ float pow2f(int e) { return __int_as_float((127 + e) << 23); }  // |e| <= 30
+__device__ __forceinline__ int balance_exp(unsigned ax, unsigned ay) {  // bit patterns of max|x|, max|y|
+    if (ax == 0u || ay == 0u) return 0;
+    const int e = (int)(ax >> 23) - (int)(ay >> 23);
+    return e < -30 ? -30 : (e > 30 ? 30 : e);
+}
+// Block-wide maximum of non-negative floats: every thread calls block_max_put, each
+// warp leaves its maximum (float bits) in wm[warp], and after the next
+// __syncthreads block_max_get<NT / 32> combines the warps' slots.
+__device__ __forceinline__ void block_max_put(unsigned *wm, float v) {
+    const unsigned u = __reduce_max_sync(0xffffffffu, __float_as_uint(v));
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = u;
+}
+template <int NW> __device__ __forceinline__ unsigned block_max_get(const unsigned *wm) {
+    unsigned u = 0u;
+#pragma unroll
+    for (int i = 0; i < NW; ++i) u = u > wm[i] ? u : wm[i];
+    return u;
+}
+__device__ __forceinline__ float absmax2(float2 v) { return fmaxf(fabsf(v.x), fabsf(v.y)); }
+
 // Loop over the row-space elements (l0 + r, km), r < RPC, km <= M/2, in an order
 // that walks each column tile's contiguous RPC*CT block: w -> (tile t, row r, col c).
 #define ROW_TILE_LOOP(RPC, H, NT, ...)                                     \
@@ -157,10 +208,13 @@ template <int M>
 __global__ void __launch_bounds__(RowCfg<M>::NT, 2) k_row_step(const RunDesc *__restrict__ runs,
                                                              const float2 *__restrict__ tw) {
     constexpr int RPC = RowCfg<M>::RPC, NB = RowCfg<M>::NB, NT = RowCfg<M>::NT, H = M / 2;
+    constexpr int NW = NT / 32;
     extern __shared__ float2 s[];
+    __shared__ unsigned wmax[4][NW];  // per-warp maxima of |phi^|, |con^|, |inn|, |inc| (float bits)
     const RunDesc &d = runs[blockIdx.y];
     const int L = d.L;
     const int l0 = blockIdx.x * RPC;
+    float mp = 0.f, mc = 0.f;
     ROW_TILE_LOOP(RPC, H, NT, {
         float2 P = make_float2(0.f, 0.f), Cc = P, A = P, B = P;
         if (l < L) {
@@ -170,42 +224,60 @@ __global__ void __launch_bounds__(RowCfg<M>::NT, 2) k_row_step(const RunDesc *__
             A = d.ca[o];
             B = d.cb[o];
         }
-        build_pair(s, NB, 2 * r, k, M, P, Cc);
+        park_pair(s, NB, 2 * r, k, M, P, Cc);
         build_pair(s, NB, 2 * r + 1, k, M, A, B);
+        mp = fmaxf(mp, absmax2(P));
+        mc = fmaxf(mc, absmax2(Cc));
     })
+    block_max_put(wmax[0], mp);
+    block_max_put(wmax[1], mc);
+    __syncthreads();
+    // con rides as 2^e1 * con beside phi (balance_exp)
+    const int e1 = balance_exp(block_max_get<NW>(wmax[0]), block_max_get<NW>(wmax[1]));
+    ROW_TILE_LOOP(RPC, H, NT, { unpark_pair(s, NB, 2 * r, k, M, pow2f(e1)); })
     __syncthreads();
     fft_smem<M, NB, NT, false>(s, tw);
 
     constexpr int PTS = (RPC * M + NT - 1) / NT;
     const float invM = 1.0f / (float)M;
+    const float cs = invM * pow2f(-e1);
     const float inv_c0 = 1.0f / d.k.para_c0, inv_1mc0 = 1.0f / (1.0f - d.k.para_c0);
     float2 out[PTS];
+    float mi = 0.f, mj = 0.f;
 #pragma unroll
     for (int q = 0; q < PTS; ++q) {
         const int w = threadIdx.x + q * NT;
         if (w < RPC * M) {
             const int r = w % RPC, m = w / RPC;
             const float2 z1 = s[spad(m * NB + 2 * r)], z2 = s[spad(m * NB + 2 * r + 1)];
-            const float psi = z1.x * invM + d.psi_mean_f, c = z1.y * invM + d.con_mean_f;
+            const float psi = z1.x * invM + d.psi_mean_f, c = z1.y * cs + d.con_mean_f;
             const PointTerms t = point_terms(d.k, inv_c0, inv_1mc0, psi, c, z2.x * invM, z2.y * invM);
             out[q] = make_float2(t.inn, t.inc);
+            mi = fmaxf(mi, fabsf(t.inn));
+            mj = fmaxf(mj, fabsf(t.inc));
         }
     }
+    block_max_put(wmax[2], mi);
+    block_max_put(wmax[3], mj);
     __syncthreads();
+    // inc rides as 2^e2 * inc beside inn
+    const int e2 = balance_exp(block_max_get<NW>(wmax[2]), block_max_get<NW>(wmax[3]));
+    const float s2 = pow2f(e2);
 #pragma unroll
     for (int q = 0; q < PTS; ++q) {
         const int w = threadIdx.x + q * NT;
-        if (w < RPC * M) s[spad(w)] = out[q];  // w = m*RPC + r: interleaved layout with NB' = RPC
+        if (w < RPC * M) s[spad(w)] = make_float2(out[q].x, out[q].y * s2);  // w = m*RPC + r: NB' = RPC
     }
     __syncthreads();
     fft_smem<M, RPC, NT, true>(s, tw);
+    const float is2 = pow2f(-e2);
     ROW_TILE_LOOP(RPC, H, NT, {
         if (l < L) {
             float2 X, Y;
             separate(s[spad(k * RPC + r)], s[spad(((M - k) & (M - 1)) * RPC + r)], X, Y);
             const long o = rs_index(d, l, k);
             d.inn[o] = X;
-            d.inc[o] = Y;
+            d.inc[o] = make_float2(Y.x * is2, Y.y * is2);
         }
     })
 }
@@ -217,10 +289,14 @@ template <int M>
 __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_forward(const RunDesc *__restrict__ runs,
                                                                 const float2 *__restrict__ tw) {
     constexpr int RPC = RowCfg<M>::RPC, NT = RowCfg<M>::NT, H = M / 2;
+    constexpr int NW = NT / 32;
     extern __shared__ float2 s[];
+    __shared__ unsigned wmax[2][NW];
     const RunDesc &d = runs[blockIdx.y];
     const int L = d.L;
     const int l0 = blockIdx.x * RPC;
+    // deviations from the FP64 means; con rides as 2^e * con beside phi (balance_exp)
+    float mp = 0.f, mc = 0.f;
     for (int w = threadIdx.x; w < RPC * M; w += NT) {
         const int r = w % RPC, m = w / RPC, l = l0 + r;
         float2 z = make_float2(0.f, 0.f);
@@ -229,16 +305,25 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_forward(const RunDesc *__
             z = make_float2((float)((double)d.psi_real[o] - d.psi_mean), (float)((double)d.con_real[o] - d.con_mean));
         }
         s[spad(w)] = z;
+        mp = fmaxf(mp, fabsf(z.x));
+        mc = fmaxf(mc, fabsf(z.y));
     }
+    block_max_put(wmax[0], mp);
+    block_max_put(wmax[1], mc);
+    __syncthreads();
+    const int e = balance_exp(block_max_get<NW>(wmax[0]), block_max_get<NW>(wmax[1]));
+    const float sc = pow2f(e);
+    for (int w = threadIdx.x; w < RPC * M; w += NT) s[spad(w)].y *= sc;
     __syncthreads();
     fft_smem<M, RPC, NT, true>(s, tw);
+    const float isc = pow2f(-e);
     ROW_TILE_LOOP(RPC, H, NT, {
         if (l < L) {
             float2 X, Y;
             separate(s[spad(k * RPC + r)], s[spad(((M - k) & (M - 1)) * RPC + r)], X, Y);
             const long o = rs_index(d, l, k);
             d.psi[o] = X;
-            d.con[o] = Y;
+            d.con[o] = make_float2(Y.x * isc, Y.y * isc);
         }
     })
 }
@@ -259,11 +344,14 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_analysis(const RunDesc *_
                                                                  const float2 *__restrict__ tw) {
     constexpr int RPC = RowCfg<M>::RPC, NT = RowCfg<M>::NT, H = M / 2;
     constexpr int NB = 3 * RPC;
+    constexpr int NW = NT / 32;
     extern __shared__ float2 s[];
     __shared__ double red[2][32];
+    __shared__ unsigned wmax[2][NW];
     const RunDesc &d = runs[blockIdx.y];
     const int L = d.L;
     const int l0 = blockIdx.x * RPC;
+    float mp = 0.f, mc = 0.f;
     ROW_TILE_LOOP(RPC, H, NT, {
         float2 z[6];
 #pragma unroll
@@ -277,10 +365,18 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_analysis(const RunDesc *_
             z[4] = d.gx[o];
             z[5] = d.gy[o];
         }
-        build_pair(s, NB, 3 * r, k, M, z[0], z[1]);
+        park_pair(s, NB, 3 * r, k, M, z[0], z[1]);
         build_pair(s, NB, 3 * r + 1, k, M, z[2], z[3]);
         build_pair(s, NB, 3 * r + 2, k, M, z[4], z[5]);
+        mp = fmaxf(mp, absmax2(z[0]));
+        mc = fmaxf(mc, absmax2(z[1]));
     })
+    block_max_put(wmax[0], mp);
+    block_max_put(wmax[1], mc);
+    __syncthreads();
+    // con rides as 2^e1 * con beside phi (balance_exp)
+    const int e1 = balance_exp(block_max_get<NW>(wmax[0]), block_max_get<NW>(wmax[1]));
+    ROW_TILE_LOOP(RPC, H, NT, { unpark_pair(s, NB, 3 * r, k, M, pow2f(e1)); })
     __syncthreads();
     fft_smem<M, NB, NT, false>(s, tw);
     const float invM = 1.0f / (float)M;
@@ -292,7 +388,7 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_analysis(const RunDesc *_
         if (l >= L) continue;
         const float2 z1 = s[spad(m * NB + 3 * r)], z2 = s[spad(m * NB + 3 * r + 1)], z3 = s[spad(m * NB + 3 * r + 2)];
         const float dpsi = z1.x * invM;
-        const float psi = dpsi + d.psi_mean_f, c = z1.y * invM + d.con_mean_f;
+        const float psi = dpsi + d.psi_mean_f, c = z1.y * (invM * pow2f(-e1)) + d.con_mean_f;
         const float a = z2.x * invM, b = z2.y * invM, gx = z3.x * invM, gy = z3.y * invM;
         d.psi_real[(size_t)l * M + m] = psi;
         d.con_real[(size_t)l * M + m] = c;
