@@ -12,8 +12,8 @@
 //     multiplier (1, C2A, C2B for phi, MIS:807-810; 1 and the -i k gradients for
 //     con at checkpoints, MIS:884-889) into s, copied s -> HBM (float4).
 // Staging the tiles through shared memory keeps every transform shared-memory to
-// shared-memory, which fits 128 registers per thread without spills: two CTAs of
-// 256 threads (2 x 69 KB of shared memory) per SM.
+// shared-memory, which fits 80 registers per thread without spills: three CTAs of
+// 256 threads (3 x 69 KB of shared memory) per SM.
 
 // multiplier applied by an inverse transform's first stage: P * g(l, km)
 struct ScaleByTable {
@@ -55,7 +55,7 @@ template <int L, int C, int NT> __device__ __forceinline__ void tile_out(const f
 }
 
 template <int L, int MODE>
-__global__ void __launch_bounds__(ColCfg<L>::NT, 2) k_col_step(const RunDesc *__restrict__ runs,
+__global__ void __launch_bounds__(ColCfg<L>::NT, 3) k_col_step(const RunDesc *__restrict__ runs,
                                                                 const float2 *__restrict__ tw) {
     constexpr int C = ColCfg<L>::C, NT = ColCfg<L>::NT;
     constexpr int SPAD = padded_len<C * L>::value;

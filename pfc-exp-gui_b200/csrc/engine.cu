@@ -72,20 +72,36 @@ int get_context(int device, Context **out) {
     Context *c = new Context();
     c->device = device;
     PFC_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-    // twiddles: for n = 2^1 .. 2^11, exp(-2 pi i j / n), j < n, in double, rounded once for FP32
+    // twiddles for n = 2^1 .. 2^11 in the stage layout of the transforms (twiddle_offset,
+    // fft_core.cuh): stage (Ns, R) entry k*R + r = exp(-2 pi i j / n), j = r*k*n/(Ns*R),
+    // in double, rounded once for FP32.  Each length gets 2n entries (enough for every
+    // stage table up to n = 2048; 16-byte aligned starts).
     size_t total = 0;
-    for (int lg = 1; lg <= 11; ++lg) total += (size_t)1 << lg;
-    std::vector<double2> h64(total);
-    std::vector<float2> h32(total);
+    for (int lg = 1; lg <= 11; ++lg) total += (size_t)2 << lg;
+    std::vector<double2> h64(total, make_double2(0.0, 0.0));
+    std::vector<float2> h32(total, make_float2(0.f, 0.f));
     size_t off = 0;
     for (int lg = 1; lg <= 11; ++lg) {
         const int n = 1 << lg;
-        for (int j = 0; j < n; ++j) {
-            const double a = 2.0 * M_PI * (double)j / (double)n;
-            h64[off + j] = make_double2(std::cos(a), -std::sin(a));
-            h32[off + j] = make_float2((float)std::cos(a), (float)-std::sin(a));
+        int ns = 1, rem = n;
+        size_t at = off;
+        while (rem > 1) {
+            const int R = rem >= 16 ? 16 : rem;  // radix-16 stages first, the small radix last
+            if (ns > 1) {
+                for (int k = 0; k < ns; ++k)
+                    for (int r = 0; r < R; ++r) {
+                        const long j = (long)r * k * (n / (ns * R));
+                        const double a = 2.0 * M_PI * (double)j / (double)n;
+                        h64[at + (size_t)k * R + r] = make_double2(std::cos(a), -std::sin(a));
+                        h32[at + (size_t)k * R + r] = make_float2((float)std::cos(a), (float)-std::sin(a));
+                    }
+                at += (size_t)ns * R;
+            }
+            ns *= R;
+            rem /= R;
         }
-        off += n;
+        if (at - off > (size_t)2 * n) return set_error(PFC_E_INVALID, "twiddle table overflow");
+        off += (size_t)2 * n;
     }
     char *mem = nullptr;
     PFC_CUDA_TRY(cudaMalloc(&mem, total * (sizeof(double2) + sizeof(float2))));
@@ -96,7 +112,7 @@ int get_context(int device, Context **out) {
     for (int lg = 1; lg <= 11; ++lg) {
         c->tw.f64[lg] = reinterpret_cast<const double2 *>(mem) + off;
         c->tw.f32[lg] = reinterpret_cast<const float2 *>(mem + total * sizeof(double2)) + off;
-        off += (size_t)1 << lg;
+        off += (size_t)2 << lg;
     }
     c->tw.f64[0] = c->tw.f64[1];
     c->tw.f32[0] = c->tw.f32[1];

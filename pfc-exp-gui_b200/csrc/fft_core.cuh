@@ -14,8 +14,10 @@
 // first stage of a transform can therefore load straight from HBM and the last
 // can store straight to HBM or stay in registers for a pointwise epilogue.
 //
-// Twiddles come from a per-length table tw[j] = exp(-2 pi i j / N) computed on the
-// host in double and rounded once to the working precision.
+// Twiddles come from a per-length table computed on the host in double and rounded
+// once to the working precision, laid out by stage (twiddle_offset): the R factors
+// exp(-2 pi i r k / (Ns R)), r < R, that one butterfly of a stage needs are
+// contiguous, so a thread fetches them with R/2 (FP32) or R (FP64) 16-byte loads.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -197,6 +199,38 @@ template <int N, int NB, int NT, int R> struct StageShape {
     static constexpr bool EXACT = ITEMS % NT == 0;
 };
 
+// Twiddle table of one length: every stage but the first (which has Ns = 1 and no
+// twiddles) owns Ns*R entries, entry k*R + r = exp(-2 pi i r k / (Ns R)).  All stages
+// before the last have radix 16, so the stage with Ns = 16^m starts at
+// 16 * (16 + 256 + ... + 16^(m-1)) = 16 (Ns - 16) / 15.
+__host__ __device__ constexpr int twiddle_offset(int Ns) { return Ns < 16 ? 0 : 16 * ((Ns - 16) / 15); }
+// entries of the whole table of length N (at most 2N for N <= 2048)
+__host__ __device__ constexpr int twiddle_entries(int N) {
+    int total = 0, ns = 1, rem = N;
+    while (rem > 1) {
+        const int r = rem >= 16 ? 16 : rem;
+        if (ns > 1) total += ns * r;
+        ns *= r;
+        rem /= r;
+    }
+    return total;
+}
+
+// the R twiddles of one butterfly (t[0] = 1 is loaded but not used)
+template <int R> __device__ __forceinline__ void load_twiddles(const float2 *__restrict__ p, float2 (&t)[R]) {
+    const float4 *p4 = reinterpret_cast<const float4 *>(p);
+#pragma unroll
+    for (int i = 0; i < R / 2; ++i) {
+        const float4 q = __ldg(p4 + i);
+        t[2 * i] = make_float2(q.x, q.y);
+        t[2 * i + 1] = make_float2(q.z, q.w);
+    }
+}
+template <int R> __device__ __forceinline__ void load_twiddles(const double2 *__restrict__ p, double2 (&t)[R]) {
+#pragma unroll
+    for (int i = 0; i < R; ++i) t[i] = __ldg(p + i);
+}
+
 // Memory spaces a stage reads from / writes to.
 enum : int { SP_SMEM = 0, SP_GLOBAL = 1, SP_REGS = 2 };
 
@@ -211,29 +245,38 @@ struct Identity {
     template <typename C> __device__ __forceinline__ C operator()(int, int, C v) const { return v; }
 };
 
-// One Stockham stage of radix R on NB interleaved sequences of length N.
+// One Stockham stage of radix R on NB interleaved sequences of length N; NS is the
+// product of the radices of the earlier stages.
 // IN/OUT: SP_SMEM (padded shared array), SP_GLOBAL (plain array).  OUT may also be
-// SP_REGS: the stage's outputs are left in v (element e = j + r*Ns of sequence b,
+// SP_REGS: the stage's outputs are left in v (element e = j + r*NS of sequence b,
 // item w = tid + q*NT, b = w % NB, j = w / NB) and nothing is stored.
 // A stage whose input and output are the same shared array synchronises between
 // its loads and its stores.
-template <int N, int NB, int NT, int R, bool FWD, int IN, int OUT, typename C, typename XF = Identity>
+template <int N, int NB, int NT, int R, int NS, bool FWD, int IN, int OUT, typename C, typename XF = Identity>
 __device__ __forceinline__ void stage(const C *__restrict__ in, typename nodeduce<C>::type *out, const C *__restrict__ tw,
-                                      int Ns, C (&v)[StageShape<N, NB, NT, R>::PER_T][R], XF xf = XF()) {
+                                      C (&v)[StageShape<N, NB, NT, R>::PER_T][R], XF xf = XF()) {
     typedef StageShape<N, NB, NT, R> S;
+    constexpr int DIN = (N / R) * NB;  // element offset between a butterfly's inputs
+    constexpr int DOUT = NS * NB;      // ... and between its outputs
     const int tid = threadIdx.x;
     // a stage that only writes shared memory must not overtake earlier readers of it
     if (IN != SP_SMEM && OUT == SP_SMEM) __syncthreads();
 #pragma unroll
     for (int q = 0; q < S::PER_T; ++q) {
-        const int w = tid + q * NT;
+        const int w = tid + q * NT;  // = j * NB + b
         if (S::EXACT || w < S::ITEMS) {
             const int b = w % NB, j = w / NB;
+            const int pw = spad(w);
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                const int ei = j + r * (N / R);
-                const int e = ei * NB + b;
-                v[q][r] = xf(ei, b, IN == SP_SMEM ? in[spad(e)] : in[e]);
+                C x;
+                if constexpr (IN != SP_SMEM)
+                    x = in[w + r * DIN];
+                else if constexpr (DIN % 16 == 0)  // spad(w + r*DIN) = spad(w) + r*DIN*17/16
+                    x = in[pw + r * (DIN + DIN / 16)];
+                else
+                    x = in[spad(w + r * DIN)];
+                v[q][r] = xf(j + r * (N / R), b, x);
             }
         }
     }
@@ -243,25 +286,25 @@ __device__ __forceinline__ void stage(const C *__restrict__ in, typename nodeduc
         const int w = tid + q * NT;
         if (S::EXACT || w < S::ITEMS) {
             const int b = w % NB, j = w / NB;
-            const int k = j % Ns;
-            if (Ns > 1) {
-                const int step = N / (Ns * R);
+            const int k = j % NS;
+            if constexpr (NS > 1) {
+                C t[R];
+                load_twiddles<R>(tw + twiddle_offset(NS) + k * R, t);
 #pragma unroll
-                for (int r = 1; r < R; ++r) {
-                    const C t = tw[r * k * step];
-                    v[q][r] = FWD ? cmul(v[q][r], t) : cmulc(v[q][r], t);
-                }
+                for (int r = 1; r < R; ++r) v[q][r] = FWD ? cmul(v[q][r], t[r]) : cmulc(v[q][r], t[r]);
             }
             dftR<R, FWD>(v[q]);
-            if (OUT != SP_REGS) {
-                const int base = (j / Ns) * Ns * R + k;
+            if constexpr (OUT != SP_REGS) {
+                const int e0 = ((j / NS) * NS * R + k) * NB + b;
+                const int pe = spad(e0);
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    const int e = (base + r * Ns) * NB + b;
-                    if (OUT == SP_SMEM)
-                        out[spad(e)] = v[q][r];
+                    if constexpr (OUT != SP_SMEM)
+                        out[e0 + r * DOUT] = v[q][r];
+                    else if constexpr (DOUT % 16 == 0)  // as for the loads
+                        out[pe + r * (DOUT + DOUT / 16)] = v[q][r];
                     else
-                        out[e] = v[q][r];
+                        out[spad(e0 + r * DOUT)] = v[q][r];
                 }
             }
         }
@@ -277,6 +320,16 @@ template <int N, int NB, int NT> struct RegOut {
     static constexpr int NS = N / R;  // Ns of the last stage
 };
 
+// The radix-16 stages between the first and the last, in place in shared memory.
+template <int N, int NB, int NT, int NS, int LAST_NS, bool FWD, typename C>
+__device__ __forceinline__ void middle_stages(C *s, const C *__restrict__ tw,
+                                              C (&v)[StageShape<N, NB, NT, 16>::PER_T][16]) {
+    if constexpr (NS < LAST_NS) {
+        stage<N, NB, NT, 16, NS, FWD, SP_SMEM, SP_SMEM>(s, s, tw, v);
+        middle_stages<N, NB, NT, NS * 16, LAST_NS, FWD>(s, tw, v);
+    }
+}
+
 // Full transform of NB interleaved length-N sequences.
 //   IN  = SP_GLOBAL: the first stage reads global `src`; SP_SMEM: reads the padded
 //         shared array `src` (which may be `s` itself or another buffer).  Every
@@ -291,23 +344,16 @@ __device__ __forceinline__ void fft(const typename nodeduce<C>::type *src, C *s,
                                     const C *__restrict__ tw,
                                     C (&last)[RegOut<N, NB, NT>::PER_T][RegOut<N, NB, NT>::R], XF xf = XF()) {
     typedef radix_plan<N> P;
-    constexpr int ST = P::stages;
-    int Ns = 1;
-    if constexpr (ST == 1) {
-        stage<N, NB, NT, P::last_radix, FWD, IN, OUT>(src, dst, tw, Ns, last, xf);
+    if constexpr (P::stages == 1) {
+        stage<N, NB, NT, P::last_radix, 1, FWD, IN, OUT>(src, dst, tw, last, xf);
     } else {
         typedef StageShape<N, NB, NT, 16> S16;
         C v[S16::PER_T][16];
         // first stage (radix 16): src -> scratch
-        stage<N, NB, NT, 16, FWD, IN, SP_SMEM>(src, s, tw, Ns, v, xf);
-        Ns *= 16;
-#pragma unroll
-        for (int i = 1; i < ST - 1; ++i) {
-            stage<N, NB, NT, 16, FWD, SP_SMEM, SP_SMEM>(s, s, tw, Ns, v);
-            Ns *= 16;
-        }
+        stage<N, NB, NT, 16, 1, FWD, IN, SP_SMEM>(src, s, tw, v, xf);
+        middle_stages<N, NB, NT, 16, RegOut<N, NB, NT>::NS, FWD>(s, tw, v);
         // last stage: scratch -> dst / registers
-        stage<N, NB, NT, P::last_radix, FWD, SP_SMEM, OUT>(s, dst, tw, Ns, last);
+        stage<N, NB, NT, P::last_radix, RegOut<N, NB, NT>::NS, FWD, SP_SMEM, OUT>(s, dst, tw, last);
     }
 }
 

@@ -187,16 +187,24 @@ __device__ __forceinline__ float absmax2(float2 v) { return fmaxf(fabsf(v.x), fa
 
 // Loop over the row-space elements (l0 + r, km), r < RPC, km <= M/2, in an order
 // that walks each column tile's contiguous RPC*CT block: w -> (tile t, row r, col c).
+// RPC and CT are powers of two, so the block split is a shift and a mask.
+template <int n> struct ilog2 {
+    static constexpr int value = n <= 1 ? 0 : 1 + ilog2<n / 2>::value;
+};
+template <> struct ilog2<1> {
+    static constexpr int value = 0;
+};
 #define ROW_TILE_LOOP(RPC, H, NT, ...)                                     \
     {                                                                       \
         const int _ct = d.CT, _lct = d.lct;                                 \
-        const int _blk = (RPC) * _ct;                                       \
-        const int _total = d.T * _blk;                                      \
+        const int _lblk = ilog2<(RPC)>::value + _lct;                       \
+        const int _total = d.T << _lblk;                                    \
         for (int w = threadIdx.x; w < _total; w += (NT)) {                  \
-            const int t = w / _blk, rem = w - t * _blk;                     \
+            const int t = w >> _lblk, rem = w & ((1 << _lblk) - 1);         \
             const int r = rem >> _lct, k = (t << _lct) + (rem & (_ct - 1)); \
             if (k > (H)) continue;                                          \
             const int l = l0 + r;                                           \
+            (void)l;                                                        \
             __VA_ARGS__                                                     \
         }                                                                   \
     }
