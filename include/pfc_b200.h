@@ -166,6 +166,87 @@ int pfc_dft3d(const double *in, double *out, int n0, int n1, int n2, int sign);
  * --precision fp32|fp64 options.  Returns the process exit code. */
 int pfc_run_cli(int argc, char **argv);
 
+/* ------------------------------------------------------------------------------
+ * Engine: many Misfit / CVD runs and Elastic analyses on one GPU, submitted and
+ * polled from any thread.  It replaces the GUI's one-process-per-run queue
+ * (src/gui/mainwindow.cpp:3453-3522 starts pfc-exp-cli once per parameter set) and
+ * has no direct counterpart in the reference.  Runs whose memory fits the HBM
+ * budget are admitted in submission order and advanced together (continuous
+ * batching: runs join and leave between scheduling quanta); each run's kernels
+ * and results are the same as when it runs alone.  Checkpoint files (the same
+ * files and formats as pfc-exp-cli) are written by an engine-owned writer thread.
+ * ------------------------------------------------------------------------------ */
+typedef struct pfc_engine pfc_engine;
+
+#define PFC_JOB_MISFIT 0  /* same values as PFC_MODEL_* */
+#define PFC_JOB_CVD 1
+#define PFC_JOB_ELASTIC 2
+
+#define PFC_EV_ADMITTED 1   /* job's memory reserved, run created */
+#define PFC_EV_CHECKPOINT 2 /* a checkpoint's results are available (its files are written) */
+#define PFC_EV_DONE 3       /* job finished; its files are written */
+#define PFC_EV_FAILED 4     /* job failed; status holds the PFC_E_* code */
+#define PFC_EV_CANCELLED 5
+
+typedef struct pfc_engine_opts {
+    int device;               /* CUDA device ordinal */
+    double hbm_budget_bytes;  /* device memory the engine may commit to runs; <= 0: 150e9,
+                                 capped by the memory free when the engine starts */
+    int max_active;           /* most runs resident at once; <= 0: no limit */
+    int quantum_steps;        /* most steps between scheduling decisions; <= 0: 64 */
+} pfc_engine_opts;
+
+typedef struct pfc_job {
+    int kind;                 /* PFC_JOB_MISFIT, PFC_JOB_CVD or PFC_JOB_ELASTIC */
+    pfc_run_params params;    /* Misfit / CVD: the run (precision must be FP32, N = 1);
+                                 Elastic: dx is the lattice spacing, L/M/N unused */
+    int steps;                /* Misfit / CVD: time steps (> 0) */
+    int mod;                  /* checkpoint interval as in --mod (> 0) */
+    const char *outdir;       /* NULL: no files; else the directory pfc-exp-cli --outdir
+                                 would write (created if missing) */
+    /* Elastic only: the fields to analyse are either the final state of an earlier
+     * job (source_job != 0; the analysis waits until that job is done) or every
+     * phi/con checkpoint pair found in input_dir (as pfc-exp-cli --model elastic). */
+    uint64_t source_job;
+    const char *input_dir;
+    float benchel;            /* Elastic neighbour cutoff (--benchel; <= 0: 1.7) */
+} pfc_job;
+
+typedef struct pfc_event {
+    uint64_t job;             /* id returned by pfc_submit */
+    int type;                 /* PFC_EV_* */
+    int status;               /* PFC_OK or a PFC_E_* code */
+    int step;                 /* checkpoint step (kd), or the job's steps when done */
+    int atoms;                /* Misfit / Elastic: atoms found at this checkpoint */
+    double energy, mass;      /* energy.txt values of this checkpoint (e/P, sum(phi)/P) */
+    double t_submit, t_admit, t_event; /* seconds on the engine's clock */
+    double t_finish;          /* DONE / FAILED / CANCELLED: when the job left the GPU and
+                                 its memory was returned (its files are written after
+                                 that, before the event is posted) */
+} pfc_event;
+
+/* Start an engine (its scheduler and writer threads) on opts->device (NULL: defaults). */
+int pfc_engine_create(const pfc_engine_opts *opts, pfc_engine **out);
+/* Cancel queued and running jobs, finish writing files, join the threads and free
+ * all device memory. */
+int pfc_engine_destroy(pfc_engine *e);
+/* Queue a job; *id receives its id (never 0).  The job's strings are copied. */
+int pfc_submit(pfc_engine *e, const pfc_job *job, uint64_t *id);
+/* Copy up to max pending events into ev (oldest first) without waiting; *n
+ * receives the number copied. */
+int pfc_poll(pfc_engine *e, pfc_event *ev, int max, int *n);
+/* Same, waiting up to timeout_ms (< 0: forever) for at least one event. */
+int pfc_wait(pfc_engine *e, pfc_event *ev, int max, int *n, int timeout_ms);
+/* Cancel a queued or running job (a PFC_EV_CANCELLED event follows). */
+int pfc_cancel(pfc_engine *e, uint64_t id);
+/* Final real fields of a finished Misfit / CVD job (P floats each, layout
+ * m + M*l); either pointer may be NULL.  Kept until pfc_release. */
+int pfc_job_fields(pfc_engine *e, uint64_t id, float *phi, float *con);
+/* Forget a finished job's kept fields. */
+int pfc_release(pfc_engine *e, uint64_t id);
+/* Device bytes a Misfit / CVD run with these parameters reserves. */
+int pfc_run_bytes(const pfc_run_params *p, double *bytes);
+
 #ifdef __cplusplus
 }
 #endif

@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "pfc_b200.h"
+#include "checkpoint.h"
 #include "pfc_engine.h"
 
 namespace pfc {
@@ -46,6 +47,7 @@ int cryst_order_dev(const double *x, const double *y, const double *z, int n, in
 }  // namespace pfc
 
 using namespace pfc;
+using namespace pfc::ckpt;
 using std::cerr;
 using std::cout;
 using std::endl;
@@ -124,144 +126,6 @@ bool setup_outdir(const std::string &dir) {
     }
     return true;
 }
-std::string opath(const std::string &dir, const std::string &name) {
-    return dir.empty() ? name : (std::filesystem::path(dir) / name).string();
-}
-
-long long now_ms() {
-    return std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::system_clock::now().time_since_epoch())
-        .count();
-}
-
-// ---------------------------------------------------------------------------
-// VTI / PVTI writers (MIS:1588-1810).  data: field in layout n + N*(m + M*l);
-// written as Float32 with l fastest.
-// ---------------------------------------------------------------------------
-bool write_vti(const std::string &path, const char *name, const float *data, int L, int M, int N) {
-    FILE *f = fopen(path.c_str(), "wb");
-    if (!f) return false;
-    const int startn = 0, endn = L - 1;
-    const int bytes = (int)((long)N * M * L * (long)sizeof(float) + (long)sizeof(int));
-    fprintf(f, "<?xml version=\"1.0\"?>\n");
-    fprintf(f, "<VTKFile type=\"ImageData\" version=\"0.1\"  byte_order=\"LittleEndian\">\n");
-    fprintf(f, "<ImageData WholeExtent=\"%d %d %d %d %d %d\"   Origin=\"%d %d %d\" Spacing=\"%d %d %d\">\n", startn, endn,
-            0, M - 1, 0, N - 1, 0, 0, 0, 1, 1, 1);
-    fprintf(f, "<Piece Extent=\"%d %d %d %d %d %d\">\n", startn, endn, 0, M - 1, 0, N - 1);
-    fprintf(f, "<PointData Scalars=\"%s\">\n", name);
-    fprintf(f, "<DataArray type=\"Float32\" Name=\"%s\"   format=\"appended\" offset=\"%d\" />\n", name, 0);
-    fprintf(f, "</PointData>\n");
-    fprintf(f, "<CellData>\n");
-    fprintf(f, "</CellData>\n");
-    fprintf(f, "</Piece>\n");
-    fprintf(f, "</ImageData>\n");
-    fprintf(f, "<AppendedData encoding=\"raw\">\n");
-    fprintf(f, "_");
-    fwrite(&bytes, sizeof(int), 1, f);
-    std::vector<float> out((size_t)L * M * N);
-    size_t o = 0;
-    for (int n = 0; n < N; n++)
-        for (int m = 0; m < M; m++)
-            for (int l = 0; l < L; l++) out[o++] = data[n + (long)N * (m + (long)M * l)];
-    fwrite(out.data(), sizeof(float), out.size(), f);
-    fprintf(f, "\n");
-    fprintf(f, "</AppendedData>\n");
-    fprintf(f, "</VTKFile>\n");
-    return fclose(f) == 0;
-}
-
-void write_pvti(const std::string &path, const char *name, const std::string &prefix, int kd, int L, int M, int N) {
-    std::ofstream o(path, std::ios_base::out);
-    o.setf(std::ios_base::fixed, std::ios_base::floatfield);
-    o.precision(4);
-    o << "<?xml version=\"1.0\"?>" << endl;
-    o << "<VTKFile type=\"PImageData\" version=\"0.1\" byte_order=\"LittleEndian\">" << endl;
-    o << "  <PImageData WholeExtent=\"0 " << L - 1 << " 0 " << M - 1 << " " << 0 << " " << N - 1
-      << "\" GhostLevel=\"#\" Origin=\"0  0  0\"  Spacing=\"1  1  1\">" << endl;
-    o << "    <PPointData>" << endl;
-    o << "      <PDataArray type=\"Float32\" Name=\"" << name << "\"/>" << endl;
-    o << "    </PPointData>" << endl;
-    o << "    <Piece Extent=\"0 " << L - 1 << " 0 " << M - 1 << " " << 0 << " " << N - 1 << "\" Source=\"" << prefix
-      << kd << "_0.vti\"/>" << endl;
-    o << "  </PImageData>" << endl;
-    o << "</VTKFile>" << endl;
-}
-
-bool write_checkpoint_fields(const std::string &outdir, int kd, const float *phi, const float *con, int L, int M, int N) {
-    char fn[64];
-    snprintf(fn, sizeof(fn), "phi_%d_%d.vti", kd, 0);
-    if (!write_vti(opath(outdir, fn), "phi", phi, L, M, N)) return false;
-    snprintf(fn, sizeof(fn), "phi_%d.pvti", kd);
-    write_pvti(opath(outdir, fn), "phi", "phi_", kd, L, M, N);
-    snprintf(fn, sizeof(fn), "con_%d_%d.vti", kd, 0);
-    if (!write_vti(opath(outdir, fn), "con", con, L, M, N)) return false;
-    snprintf(fn, sizeof(fn), "con_%d.pvti", kd);
-    write_pvti(opath(outdir, fn), "con", "con_", kd, L, M, N);
-    return true;
-}
-
-// VTI reader (ELA:2562-2645): 12 header lines, '_', int32 byte count, then Float32
-// values with l fastest.  The grid comes from WholeExtent unless given.
-bool read_vti(const std::string &path, int &L, int &M, int &N, std::vector<float> &field) {
-    FILE *f = fopen(path.c_str(), "rb");
-    if (!f) return false;
-    char buf[100];
-    int gl = -1, gm = -1, gn = -1;
-    for (int i = 1; i < 13; ++i) {
-        if (!fgets(buf, sizeof(buf), f)) break;
-        int a, b, c, d, e, g;
-        const char *w = strstr(buf, "WholeExtent=\"");
-        if (w && sscanf(w + 13, "%d %d %d %d %d %d", &a, &b, &c, &d, &e, &g) == 6 && gl < 0) {
-            gl = b - a + 1;
-            gm = d - c + 1;
-            gn = g - e + 1;
-        }
-    }
-    (void)fgetc(f);
-    int bytes = 0;
-    if (fread(&bytes, sizeof(int), 1, f) != 1) {
-        fclose(f);
-        return false;
-    }
-    if (L <= 0) {
-        L = gl;
-        M = gm;
-        N = gn;
-    }
-    if (L <= 0 || M <= 0 || N <= 0) {
-        fclose(f);
-        return false;
-    }
-    const long P = (long)L * M * N;
-    std::vector<float> raw(P, 0.0f);
-    const size_t got = fread(raw.data(), sizeof(float), P, f);
-    fclose(f);
-    (void)got;  // a short file leaves the remaining values 0, as the reference's unchecked reads do
-    field.assign(P, 0.0f);
-    long o = 0;
-    for (int n = 0; n < N; n++)
-        for (int m = 0; m < M; m++)
-            for (int l = 0; l < L; l++) field[n + (long)N * (m + (long)M * l)] = raw[o++];
-    return true;
-}
-
-// Device scratch owned by a CLI run.
-struct DevScratch {
-    void *p = nullptr;
-    size_t bytes = 0;
-    ~DevScratch() {
-        if (p) cudaFree(p);
-    }
-    bool ensure(size_t b) {
-        if (b <= bytes) return true;
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-        if (cudaMalloc(&p, b) != cudaSuccess) return false;
-        bytes = b;
-        return true;
-    }
-};
-
 struct RunGuard {
     pfc_run *r = nullptr;
     ~RunGuard() {
@@ -327,7 +191,6 @@ int misfit_phimax(pfc_run *r, const SimOpts &o, const std::vector<float> &phi, c
     // debug statistics of the reference (MIS:3310-3330) from the host copy
     double gmin = std::numeric_limits<double>::infinity(), gmax = -std::numeric_limits<double>::infinity();
     int finite_phi = 0, above_cut = 0;
-    bool any_max = false;
     for (long i = 0; i < (long)L * M; ++i) {
         const double v = phi[i];
         if (!std::isfinite(v)) continue;
@@ -336,40 +199,16 @@ int misfit_phimax(pfc_run *r, const SimOpts &o, const std::vector<float> &phi, c
         gmax = std::max(gmax, v);
         if (v > -0.07) above_cut++;
     }
-    (void)any_max;
     if (raw == 0) cout << "WARNING: no local maxima found; writing global max fallback point" << endl;
     cout << count << " " << 0 << endl;
     cout << "second" << "myid=" << 0 << endl;
     cout << "third" << "myid=" << 0 << endl;
-    int total = 0;
-    for (int i = 0; i < count; ++i) {
-        const double *a = &atoms[(size_t)i * 5];
-        if (!std::isfinite(a[0]) || !std::isfinite(a[1]) || !std::isfinite(a[2]) || !std::isfinite(a[3]) ||
-            !std::isfinite(a[4]))
-            continue;
-        if (a[0] < 0) continue;
-        total++;
-    }
+    const int total = count_misfit_atoms(atoms, count);
     cout << "num_atoms_total=" << total << endl;
     if (total <= 2)
         cout << "phimax_atmposi debug: finite_phi=" << finite_phi << " above_cut=" << above_cut << " phi_min=" << gmin
              << " phi_max=" << gmax << endl;
-    char fn[64];
-    snprintf(fn, sizeof(fn), "Phimax_%d.txt", kd);
-    std::ofstream f(opath(o.outdir, fn), std::ios_base::out);
-    f.setf(std::ios_base::fixed, std::ios_base::floatfield);
-    f.precision(4);
-    f << 2 * total << endl;
-    f << "Kommentar" << endl;
-    for (int i = 0; i < count; ++i) {
-        const double *a = &atoms[(size_t)i * 5];
-        if (!std::isfinite(a[0]) || !std::isfinite(a[1]) || !std::isfinite(a[2]) || !std::isfinite(a[3]) ||
-            !std::isfinite(a[4]))
-            continue;
-        if (a[0] < 0) continue;
-        f << a[0] << " " << a[1] << " " << a[2] << " " << a[3] << " " << a[4] << endl;
-        f << a[0] << " " << a[1] << " " << a[2] + 20 << " " << a[3] << " " << a[4] << endl;
-    }
+    write_phimax_misfit(o.outdir, kd, atoms, count);
     (void)con;
     return 0;
 }
@@ -377,8 +216,7 @@ int misfit_phimax(pfc_run *r, const SimOpts &o, const std::vector<float> &phi, c
 int append_energy(pfc_run *r, const SimOpts &o, int kd) {
     double e = 0.0, d = 0.0;
     if (pfc_run_energy(r, &e, &d) != PFC_OK) return gpu_fail("energy");
-    std::ofstream f(opath(o.outdir, "energy.txt"), std::ios_base::out | std::ios_base::app);
-    f << kd << " " << e << " " << d << endl;
+    append_energy_line(o.outdir, kd, e, d);
     return 0;
 }
 
@@ -747,42 +585,6 @@ void elastic_usage(const char *argv0) {
          << "  -h, --help          Show this help\n";
 }
 
-std::string input_file(const std::string &input_dir, const char *prefix, int step) {
-    char fn[64];
-    snprintf(fn, sizeof(fn), "%s%d%s%d%s", prefix, step, "_", 0, ".vti");
-    if (input_dir.empty()) return std::string(fn);
-    return (std::filesystem::path(input_dir) / fn).string();
-}
-
-// CollectAvailableCheckpointSteps (ELA:37-74)
-std::vector<int> collect_steps(const std::string &input_dir) {
-    std::vector<int> out;
-    const std::filesystem::path dir = input_dir.empty() ? std::filesystem::current_path() : std::filesystem::path(input_dir);
-    std::error_code ec;
-    if (!std::filesystem::exists(dir, ec) || ec) return out;
-    std::set<int> ps, cs;
-    for (const auto &e : std::filesystem::directory_iterator(dir, ec)) {
-        if (ec) break;
-        if (!e.is_regular_file()) continue;
-        const std::string name = e.path().filename().string();
-        int step = 0, rank = 0;
-        if (sscanf(name.c_str(), "phi_%d_%d.vti", &step, &rank) == 2) {
-            ps.insert(step);
-            continue;
-        }
-        if (sscanf(name.c_str(), "con_%d_%d.vti", &step, &rank) == 2) cs.insert(step);
-    }
-    bool has_positive = false;
-    for (int s : ps) {
-        if (!cs.count(s)) continue;
-        if (s > 0) has_positive = true;
-        out.push_back(s);
-    }
-    std::sort(out.begin(), out.end());
-    if (has_positive) out.erase(std::remove(out.begin(), out.end(), 0), out.end());
-    return out;
-}
-
 // One checkpoint of the Elastic analysis; returns the process exit code (0 = go on).
 int elastic_checkpoint(int kd, const std::string &input_dir, const std::string &outdir, int gL, int gM, int gN, float dx,
                        float benchel, cudaStream_t st, DevScratch &scratch) {
@@ -799,78 +601,9 @@ int elastic_checkpoint(int kd, const std::string &input_dir, const std::string &
         cerr << "can't open input file: " << fcon << endl;
         return 2;
     }
-    const long P = (long)L * M * N;
-    const long cap = P + 1;
-    if (!scratch.ensure(P * sizeof(float) + cap * 4 * sizeof(double))) return gpu_fail("device allocation");
-    float *dphi = (float *)scratch.p;
-    double *datoms = (double *)((char *)scratch.p + ((P * sizeof(float) + 255) / 256) * 256);
-    if (cudaMemcpyAsync(dphi, phi.data(), P * sizeof(float), cudaMemcpyHostToDevice, st) != cudaSuccess)
-        return gpu_fail("field upload");
-    int n = 0;
-    if (phimax_elastic_dev(dphi, L, M, N, dx, datoms, (int)cap, &n, st) != PFC_OK) return gpu_fail("Phimax");
-    std::vector<double> atoms((size_t)n * 4);
-    if (n > 0 && cudaMemcpyAsync(atoms.data(), datoms, atoms.size() * sizeof(double), cudaMemcpyDeviceToHost, st) !=
-                     cudaSuccess)
-        return gpu_fail("Phimax copy");
-    std::vector<double> x(n), y(n), z(n);
-    if (cudaStreamSynchronize(st) != cudaSuccess) return gpu_fail("Phimax");
-    for (int i = 0; i < n; ++i) {
-        x[i] = atoms[4 * i];
-        y[i] = atoms[4 * i + 1];
-        z[i] = atoms[4 * i + 2];
-    }
-    char fn[64];
-    {
-        snprintf(fn, sizeof(fn), "Phimax_%d.txt", kd);
-        std::ofstream f(opath(outdir, fn), std::ios_base::out);
-        f.setf(std::ios_base::fixed, std::ios_base::floatfield);
-        f.precision(4);
-        f << n << endl;
-        f << "Kommentar" << endl;
-        for (int i = 0; i < n; ++i)
-            if (x[i] >= 0) f << x[i] << " " << y[i] << " " << z[i] << " " << atoms[4 * i + 3] << endl;
-    }
-    std::vector<double> strain(n), q4(n), q6(n);
-    std::vector<uint32_t> nb(n);
-    if (n > 0) {
-        if (pfc_elastic3d(x.data(), y.data(), z.data(), n, L, M, N, dx, benchel, strain.data(), nb.data()) != PFC_OK)
-            return gpu_fail("elastic3D");
-        if (pfc_cryst_order(x.data(), y.data(), z.data(), n, L, M, N, dx, q4.data(), q6.data()) != PFC_OK)
-            return gpu_fail("cryst_order");
-    }
-    {
-        snprintf(fn, sizeof(fn), "strain_%d.txt", kd);
-        std::ofstream f(opath(outdir, fn), std::ios_base::out);
-        f.setf(std::ios_base::fixed, std::ios_base::floatfield);
-        f.precision(4);
-        f << n << endl;
-        f << "Kommentar" << endl;
-        for (int i = 0; i < n; ++i)
-            if (x[i] >= 0) f << "st" << " " << x[i] << " " << y[i] << " " << z[i] << " " << strain[i] << " " << nb[i] << endl;
-    }
-    {
-        int total = 0;
-        for (int i = 0; i < n; ++i)
-            if (x[i] >= 0) total++;
-        snprintf(fn, sizeof(fn), "q4q6_%d.txt", kd);
-        std::ofstream f(opath(outdir, fn), std::ios_base::out);
-        f.setf(std::ios_base::fixed, std::ios_base::floatfield);
-        f.precision(4);
-        f << total << endl;
-        f << "Kommentar" << endl;
-        double qMinX = 1e30, qMaxX = -1e30, qMinY = 1e30, qMaxY = -1e30;
-        for (int i = 0; i < n; ++i) {
-            if (x[i] >= 0) {
-                f << "qc" << " " << x[i] << " " << y[i] << " " << z[i] << " " << q4[i] << " " << q6[i] << endl;
-                if (x[i] < qMinX) qMinX = x[i];
-                if (x[i] > qMaxX) qMaxX = x[i];
-                if (y[i] < qMinY) qMinY = y[i];
-                if (y[i] > qMaxY) qMaxY = y[i];
-            }
-        }
-        cerr << "q4q6_" << kd << ".txt: atoms=" << total << " x=[" << qMinX << "," << qMaxX << "] y=[" << qMinY << ","
-             << qMaxY << "]" << endl;
-    }
+    ElasticResult res;
+    if (elastic_analyze(phi.data(), L, M, N, dx, benchel, st, scratch, res) != PFC_OK) return gpu_fail("Elastic analysis");
+    write_elastic_files(outdir, kd, res, cerr);
     return 0;
 }
 

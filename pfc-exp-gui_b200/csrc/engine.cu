@@ -42,12 +42,6 @@ int cuda_error(cudaError_t e, const char *what) {
     return set_error(PFC_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-#define PFC_CUDA_TRY(expr)                                   \
-    do {                                                     \
-        cudaError_t _e = (expr);                             \
-        if (_e != cudaSuccess) return cuda_error(_e, #expr); \
-    } while (0)
-
 static constexpr double PI_REF = 3.1415926;  // pfc_common.h:152
 
 // ---------------------------------------------------------------------------
@@ -273,7 +267,35 @@ bool is_supported_len(int n) { return n >= 32 && n <= 2048 && (n & (n - 1)) == 0
 
 static int round_up(int x, int a) { return (x + a - 1) / a * a; }
 
+// Bytes of a run's own device allocation: 8 row-space arrays (FP32 path) + 2 real
+// fields + k tables + partials + result slots + descriptor.
+static size_t run_state_bytes(int L, int M, int N, bool fp32) {
+    const int Hp = round_up(M / 2 + 1, col_tile_width(L));
+    const size_t rs = (size_t)L * Hp * sizeof(float2);
+    const size_t real = (size_t)L * M * N * sizeof(float);
+    const size_t ktab = (size_t)(L + M + N) * sizeof(float);
+    const size_t parts = (size_t)(2 * analysis_partials(L, M) + 4096) * sizeof(double);
+    return (fp32 ? 8 * rs : 0) + 2 * real + round_up((int)ktab, 256) + parts + sizeof(RunDesc) + 1024;
+}
+
 }  // namespace pfc
+
+// Device bytes a run reserves: its own allocation, plus for the FP32 path the shared
+// coefficient table (counted in full, as if not shared), plus for the FP64 paths the
+// 22 complex-double and 6 real working arrays.
+extern "C" int pfc_run_bytes(const pfc_run_params *p, double *bytes) {
+    using namespace pfc;
+    if (!p || !bytes) return set_error(PFC_E_INVALID, "null argument");
+    if (!is_supported_len(p->L) || !is_supported_len(p->M) || p->N < 1)
+        return set_error(PFC_E_INVALID, "unsupported grid");
+    const bool fp32 = p->precision == PFC_PRECISION_FP32;
+    double b = (double)run_state_bytes(p->L, p->M, p->N, fp32);
+    const double P = (double)p->L * p->M * p->N;
+    if (fp32) b += 2.0 * (double)p->L * round_up(p->M / 2 + 1, col_tile_width(p->L)) * sizeof(float2);
+    else b += P * (22.0 * 16.0 + 6.0 * 8.0);
+    *bytes = b;
+    return PFC_OK;
+}
 
 using namespace pfc;
 
@@ -377,10 +399,8 @@ extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) {
     r->nparts = nparts;
     const size_t ktab = (size_t)(r->L + r->M + r->N) * sizeof(float);
     const size_t parts = (size_t)(2 * nparts + 4096) * sizeof(double);
-    size_t bytes = 0;
     const bool fp32 = p->precision == PFC_PRECISION_FP32;
-    if (fp32) bytes += 8 * rs;
-    bytes += 2 * real + round_up((int)ktab, 256) + parts + sizeof(RunDesc) + 1024;
+    const size_t bytes = run_state_bytes(r->L, r->M, r->N, fp32);
     cudaError_t e = cudaMalloc(&r->dev_mem, bytes);
     if (e != cudaSuccess) {
         free_run(r);

@@ -135,4 +135,20 @@ cudaError_t launch_reduce_fixed(const double *partials, int count, int stride, i
     return cudaGetLastError();
 }
 
+// k_reduce_fixed(partials, count, 2, 2, ...) for run blockIdx.x of a batch.
+__global__ void k_reduce_runs(const RunDesc *__restrict__ runs, int count, int slot) {
+    const RunDesc &d = runs[blockIdx.x];
+    const int j = threadIdx.x;
+    if (j >= 2) return;
+    double s = 0.0;
+    for (int i = 0; i < count; ++i) s += d.partials[(long)i * 2 + j];
+    d.ehist[2 * slot + j] = s;
+}
+
+cudaError_t launch_reduce_runs(const RunDesc *d_runs, int nruns, int nparts, int slot, cudaStream_t s) {
+    if (nruns <= 0) return cudaSuccess;
+    k_reduce_runs<<<nruns, 32, 0, s>>>(d_runs, nparts, slot);
+    return cudaGetLastError();
+}
+
 }  // namespace pfc

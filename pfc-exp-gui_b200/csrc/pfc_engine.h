@@ -22,6 +22,13 @@ struct Context {
 
 int set_error(int code, const std::string &msg);
 int cuda_error(cudaError_t e, const char *what);
+
+// return the PFC_E_CUDA status of a failed CUDA call from the enclosing function
+#define PFC_CUDA_TRY(expr)                                          \
+    do {                                                            \
+        cudaError_t _e = (expr);                                    \
+        if (_e != cudaSuccess) return pfc::cuda_error(_e, #expr);   \
+    } while (0)
 int get_context(int device, Context **out);
 void model_coefs(int model, ModelCoefs *k);
 void kref_table(int n, float dx, std::vector<float> &k);

@@ -55,6 +55,8 @@ struct RunDesc {
     C2Params c2a, c2b;
     // per-CTA partial sums written by the analysis row kernel: [2 * L] doubles
     double *partials;
+    // batched runs only: slots of (energy sum, mass sum) that launch_reduce_runs fills
+    double *ehist;
 };
 
 // Twiddle tables exp(-2 pi i j / n) for n = 2^1 .. 2^11, FP32 and FP64.
@@ -70,6 +72,11 @@ cudaError_t launch_col_step(const RunDesc *d_runs, int nruns, int L, int M, int 
 cudaError_t launch_row_forward(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw, cudaStream_t s);
 cudaError_t launch_row_analysis(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw,
                                 cudaStream_t s);
+
+// For each of nruns runs: (sum, in CTA order, of the analysis row kernel's nparts
+// partial pairs) -> runs[i].ehist[2*slot], [2*slot+1]; the same additions in the same
+// order as the single-run reduction (launch_reduce_fixed), so the sums are identical.
+cudaError_t launch_reduce_runs(const RunDesc *d_runs, int nruns, int nparts, int slot, cudaStream_t s);
 
 // Build the per k-point coefficient table of one run (layout and values as RunDesc::kcoef).
 cudaError_t launch_build_kcoef(const RunDesc *d_run, float2 *kden, float2 *kc2, cudaStream_t s);

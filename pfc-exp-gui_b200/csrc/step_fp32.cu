@@ -361,9 +361,7 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_analysis(const RunDesc *_
     const int l0 = blockIdx.x * RPC;
     float mp = 0.f, mc = 0.f;
     ROW_TILE_LOOP(RPC, H, NT, {
-        float2 z[6];
-#pragma unroll
-        for (int j = 0; j < 6; ++j) z[j] = make_float2(0.f, 0.f);
+        float2 z[6] = {};
         if (l < L) {
             const long o = rs_index(d, l, k);
             z[0] = d.psi[o];

@@ -53,6 +53,47 @@ class RunParams(C.Structure):
     ]
 
 
+class EngineOpts(C.Structure):
+    _fields_ = [
+        ("device", C.c_int),
+        ("hbm_budget_bytes", C.c_double),
+        ("max_active", C.c_int),
+        ("quantum_steps", C.c_int),
+    ]
+
+
+class JobSpec(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int),
+        ("params", RunParams),
+        ("steps", C.c_int),
+        ("mod", C.c_int),
+        ("outdir", C.c_char_p),
+        ("source_job", C.c_uint64),
+        ("input_dir", C.c_char_p),
+        ("benchel", C.c_float),
+    ]
+
+
+class Event(C.Structure):
+    _fields_ = [
+        ("job", C.c_uint64),
+        ("type", C.c_int),
+        ("status", C.c_int),
+        ("step", C.c_int),
+        ("atoms", C.c_int),
+        ("energy", C.c_double),
+        ("mass", C.c_double),
+        ("t_submit", C.c_double),
+        ("t_admit", C.c_double),
+        ("t_event", C.c_double),
+        ("t_finish", C.c_double),
+    ]
+
+
+JOB_MISFIT, JOB_CVD, JOB_ELASTIC = 0, 1, 2
+EV_ADMITTED, EV_CHECKPOINT, EV_DONE, EV_FAILED, EV_CANCELLED = 1, 2, 3, 4, 5
+
 _lib = None
 
 
@@ -99,6 +140,15 @@ def lib():
         "pfc_batch_advance_timed": ([vp, C.c_int, P(C.c_float)], C.c_int),
         "pfc_batch_kernel_times": ([vp, C.c_int, dp, dp], C.c_int),
         "pfc_run_cli": ([C.c_int, P(C.c_char_p)], C.c_int),
+        "pfc_engine_create": ([P(EngineOpts), P(vp)], C.c_int),
+        "pfc_engine_destroy": ([vp], C.c_int),
+        "pfc_submit": ([vp, P(JobSpec), P(C.c_uint64)], C.c_int),
+        "pfc_poll": ([vp, P(Event), C.c_int, P(C.c_int)], C.c_int),
+        "pfc_wait": ([vp, P(Event), C.c_int, P(C.c_int), C.c_int], C.c_int),
+        "pfc_cancel": ([vp, C.c_uint64], C.c_int),
+        "pfc_job_fields": ([vp, C.c_uint64, fp, fp], C.c_int),
+        "pfc_release": ([vp, C.c_uint64], C.c_int),
+        "pfc_run_bytes": ([P(RunParams), dp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -230,6 +280,69 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class Engine:
+    """Many runs on one GPU: submit jobs, then poll or wait for their events."""
+
+    def __init__(self, device=0, hbm_budget_bytes=0.0, max_active=0, quantum_steps=0):
+        o = EngineOpts(device, hbm_budget_bytes, max_active, quantum_steps)
+        self.h = C.c_void_p()
+        _check(lib().pfc_engine_create(C.byref(o), C.byref(self.h)), "pfc_engine_create")
+        self.grids = {}
+
+    def submit(self, kind, params=None, steps=0, mod=0, outdir=None, source_job=0, input_dir=None, benchel=0.0):
+        if params is None:
+            params = default_params(MODEL_CVD if kind == JOB_CVD else MODEL_MISFIT)
+        j = JobSpec(kind, params, steps, mod, outdir.encode() if outdir else None, source_job,
+                    input_dir.encode() if input_dir else None, benchel)
+        jid = C.c_uint64()
+        _check(lib().pfc_submit(self.h, C.byref(j), C.byref(jid)), "pfc_submit")
+        self.grids[jid.value] = (params.L, params.M, params.N)
+        return jid.value
+
+    def poll(self, max_events=256):
+        ev = (Event * max_events)()
+        n = C.c_int()
+        _check(lib().pfc_poll(self.h, ev, max_events, C.byref(n)), "pfc_poll")
+        return [ev[i] for i in range(n.value)]
+
+    def wait(self, timeout_ms=-1, max_events=256):
+        ev = (Event * max_events)()
+        n = C.c_int()
+        _check(lib().pfc_wait(self.h, ev, max_events, C.byref(n), timeout_ms), "pfc_wait")
+        return [ev[i] for i in range(n.value)]
+
+    def cancel(self, jid):
+        _check(lib().pfc_cancel(self.h, jid), "pfc_cancel")
+
+    def fields(self, jid):
+        L, M, N = self.grids[jid]
+        phi = np.empty((L, M, N) if N > 1 else (L, M), np.float32)
+        con = np.empty_like(phi)
+        _check(lib().pfc_job_fields(self.h, jid, _fp(phi), _fp(con)), "pfc_job_fields")
+        return phi, con
+
+    def release(self, jid):
+        _check(lib().pfc_release(self.h, jid), "pfc_release")
+
+    def close(self):
+        if self.h:
+            lib().pfc_engine_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def run_bytes(params) -> float:
+    """Device bytes a run with these parameters reserves (pfc_run_bytes)."""
+    b = C.c_double()
+    _check(lib().pfc_run_bytes(C.byref(params), C.byref(b)), "pfc_run_bytes")
+    return b.value
 
 
 def phimax_misfit(phi, con, dx=0.125, con0=0.2):
