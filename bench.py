@@ -43,6 +43,9 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-plain", action="store_true")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the 64-run mixed-size sweep measurement")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving (Poisson arrivals) measurement")
+    ap.add_argument("--serve-requests", type=int, default=48)
     return ap.parse_args()
 
 
@@ -247,6 +250,136 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+# ---------------------------------------------------------------------------
+# Sweep and serving workloads through the engine (pfc_engine_* in the C ABI)
+# ---------------------------------------------------------------------------
+MASK64 = (1 << 64) - 1
+
+
+class SplitMix64:
+    """splitmix64 (Steele, Lea, Flood 2014), the generator the reference seeds with."""
+
+    def __init__(self, seed):
+        self.x = seed & MASK64
+
+    def next(self):
+        self.x = (self.x + 0x9E3779B97F4A7C15) & MASK64
+        z = self.x
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & MASK64
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & MASK64
+        return z ^ (z >> 31)
+
+
+def drain_engine(P, eng, n, timeout_s=900.0):
+    """Wait for n jobs to finish; returns {job: final event}."""
+    done = {}
+    t_end = time.time() + timeout_s
+    while len(done) < n and time.time() < t_end:
+        for ev in eng.wait(timeout_ms=500):
+            if ev.type in (P.EV_DONE, P.EV_FAILED, P.EV_CANCELLED):
+                done[ev.job] = ev
+    return done
+
+
+def sweep_bench(P, dev, nruns=64, steps=2000, master_seed=4242):
+    """64 Misfit runs of mixed grids {128, 256, 512}^2, u0 and con0 from the GUI's value
+    lists, drawn with splitmix64 from a master seed; 2000 steps, one checkpoint (mod 2000).
+    Timed as one engine sweep (all submitted at once) and as sequential GPU runs (the
+    same engine with one run resident at a time, as the GUI's one-process queue)."""
+    rng = SplitMix64(master_seed)
+    jobs = []
+    for i in range(nruns):
+        g = (128, 256, 512)[rng.next() % 3]
+        u0 = (0.02, 0.05, 0.08, 0.11)[rng.next() % 4]
+        con0 = (0.1, 0.2, 0.3, 0.4)[rng.next() % 4]
+        jobs.append(P.default_params(P.MODEL_MISFIT, L=g, M=g, seed=1000 + i, u0=u0, con0=con0, device=dev))
+
+    def run(max_active):
+        eng = P.Engine(device=dev, max_active=max_active)
+        warm = eng.submit(P.JOB_MISFIT, P.default_params(P.MODEL_MISFIT, L=128, M=128, device=dev), steps=40, mod=40)
+        drain_engine(P, eng, 1)
+        eng.release(warm)
+        t0 = time.perf_counter()
+        ids = [eng.submit(P.JOB_MISFIT, p, steps=steps, mod=steps) for p in jobs]
+        done = drain_engine(P, eng, len(ids))
+        wall = time.perf_counter() - t0
+        ok = sum(1 for j in ids if j in done and done[j].type == P.EV_DONE)
+        eng.close()
+        return wall, ok
+
+    wall_b, ok_b = run(0)
+    wall_s, ok_s = run(1)
+    grids = {}
+    for p in jobs:
+        grids[p.L] = grids.get(p.L, 0) + 1
+    return {"runs": nruns, "steps": steps, "grids": {f"{g}^2": n for g, n in sorted(grids.items())},
+            "master_seed": master_seed,
+            "batched_s": round(wall_b, 3), "sequential_gpu_s": round(wall_s, 3),
+            "runs_per_hour_batched": round(ok_b / wall_b * 3600.0, 1),
+            "runs_per_hour_sequential_gpu": round(ok_s / wall_s * 3600.0, 1),
+            "batched_over_sequential": round(wall_s / wall_b, 2), "completed": [ok_b, ok_s],
+            "what": "wall clock from the first submit to the last DONE event (run set-up, 2000 steps, "
+                    "final Phimax/energy checkpoint); sequential = engine with max_active=1"}
+
+
+def serve_bench(P, dev, n_req=48, lam=4.0, seed=777, budget=150e9):
+    """Poisson arrivals (rate lam/s): 70 % Misfit, 20 % CVD (2-D), 10 % Elastic on a
+    finished run's fields; grid 2^U(7,11) rounded to a power of two, steps U[500, 20000],
+    u0 U[0.02, 0.12], con0 U[0.1, 0.4], random seeds; HBM admission budget 150 GB.
+    Latency = DONE event - submission (files and results ready)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / lam, n_req))
+    kinds = rng.choice([P.JOB_MISFIT, P.JOB_CVD, P.JOB_ELASTIC], size=n_req, p=[0.7, 0.2, 0.1])
+    eng = P.Engine(device=dev, hbm_budget_bytes=budget)
+    warm = eng.submit(P.JOB_MISFIT, P.default_params(P.MODEL_MISFIT, L=128, M=128, device=dev), steps=20, mod=20)
+    drain_engine(P, eng, 1)
+    eng.release(warm)
+    misfit_ids, submitted, done, kind_of = [], [], {}, {}
+    t0 = time.perf_counter()
+    i = 0
+    while len(done) < n_req:
+        now = time.perf_counter() - t0
+        while i < n_req and arrivals[i] <= now:
+            k = int(kinds[i])
+            if k == P.JOB_ELASTIC and not misfit_ids:
+                k = P.JOB_MISFIT
+            if k == P.JOB_ELASTIC:
+                src = misfit_ids[int(rng.integers(len(misfit_ids)))]
+                jid = eng.submit(P.JOB_ELASTIC, P.default_params(P.MODEL_MISFIT, device=dev), source_job=src)
+            else:
+                g = 2 ** int(round(rng.uniform(7.0, 11.0)))
+                model = P.MODEL_CVD if k == P.JOB_CVD else P.MODEL_MISFIT
+                p = P.default_params(model, L=g, M=g, seed=int(rng.integers(1, 2**31)), u0=float(rng.uniform(0.02, 0.12)),
+                                     con0=float(rng.uniform(0.1, 0.4)), device=dev)
+                steps = int(rng.integers(500, 20001))
+                jid = eng.submit(k, p, steps=steps, mod=steps)
+                if k == P.JOB_MISFIT:
+                    misfit_ids.append(jid)
+            kind_of[jid] = k
+            submitted.append(jid)
+            i += 1
+        wait_ms = 200 if i >= n_req else max(1, int((arrivals[i] - (time.perf_counter() - t0)) * 1000))
+        for ev in eng.wait(timeout_ms=min(wait_ms, 200)):
+            if ev.type in (P.EV_DONE, P.EV_FAILED, P.EV_CANCELLED):
+                done[ev.job] = ev
+        if time.perf_counter() - t0 > 1200:
+            break
+    makespan = time.perf_counter() - t0
+    eng.close()
+    lat = np.array([done[j].t_event - done[j].t_submit for j in submitted if j in done and done[j].type == P.EV_DONE])
+    ok = len(lat)
+    return {"requests": n_req, "arrival_rate_per_s": lam, "seed": seed, "completed": ok,
+            "mix": {"misfit": int(sum(1 for k in kind_of.values() if k == P.JOB_MISFIT)),
+                    "cvd": int(sum(1 for k in kind_of.values() if k == P.JOB_CVD)),
+                    "elastic": int(sum(1 for k in kind_of.values() if k == P.JOB_ELASTIC))},
+            "p50_s": round(float(np.percentile(lat, 50)), 3) if ok else None,
+            "p99_s": round(float(np.percentile(lat, 99)), 3) if ok else None,
+            "makespan_s": round(makespan, 2), "runs_per_hour": round(ok / makespan * 3600.0, 1),
+            "hbm_budget_gb": budget / 1e9,
+            "what": "engine with continuous batching; latency = submission to DONE (results and events ready)"}
+
+
 def run_ours(args):
     dist = Dist(args.gpus)
     import numpy as np
@@ -338,6 +471,11 @@ def run_ours(args):
     batch.close()
     for r in runs:
         r.close()
+    # sweep and serving workloads, each rank on its own GPU (rank 0 reports its own)
+    if not args.no_sweep:
+        line["sweep"] = sweep_bench(P, dev)
+    if not args.no_serve:
+        line["serving"] = serve_bench(P, dev, n_req=args.serve_requests, seed=777 + dist.rank)
     if dist.rank == 0:
         print(json.dumps(line), flush=True)
     dist.close()
