@@ -84,6 +84,13 @@ def lib():
                                         dp, P(C.c_uint32)]
             L.orc_cryst_order.argtypes = [dp, dp, dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, dp, dp]
             L.orc_dft3d.argtypes = [C.c_int, C.c_int, C.c_int, dp, dp, C.c_int]
+            L.orc_cvd_atoms.argtypes = [fp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, fp, fp, fp, C.c_int]
+            L.orc_cvd_atoms.restype = C.c_int
+            L.orc_cvd_gr_hist.argtypes = [fp, fp, fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float,
+                                          P(C.c_uint32), C.c_int]
+            L.orc_cvd_gr_hist.restype = C.c_int
+            L.orc_cvd_q6.argtypes = [fp, fp, fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, P(C.c_uint32),
+                                     fp, fp, P(C.c_uint32)]
             L.orc_splitmix64_next.argtypes = [P(C.c_uint64)]
             L.orc_splitmix64_next.restype = C.c_uint64
             L.orc_rng_u01.argtypes = [P(C.c_uint64)]
@@ -204,6 +211,40 @@ def cryst_order(x, y, z, L, M, N, dx=0.125):
     q6 = np.zeros(n, np.float64)
     lib().orc_cryst_order(_dp(x), _dp(y), _dp(z), n, L, M, N, dx, _dp(q4), _dp(q6))
     return q4, q6
+
+
+def cvd_atoms(phi, u0, dx=0.125):
+    """atompositionCFGC2 peak finder (CVD:1076-1165) on a float32 field shaped (L, M, N).
+    Returns (phic, phimax, records[n, 4] = (x, y, z, phi) fractional float32)."""
+    phi = np.ascontiguousarray(phi, np.float32)
+    L, M, N = phi.shape
+    cap = L * M * N + 1
+    out = np.zeros((cap, 4), np.float32)
+    phic, pmax = C.c_float(), C.c_float()
+    n = lib().orc_cvd_atoms(_fp(phi), L, M, N, dx, u0, C.byref(phic), C.byref(pmax), _fp(out), cap)
+    return np.float32(phic.value), np.float32(pmax.value), out[:n].copy()
+
+
+def cvd_gr_hist(rec, L, M, N, dx=0.125):
+    """GR's pair-distance histogram (CVD:1277-1312) of the records."""
+    x, y, z = (np.ascontiguousarray(rec[:, k], np.float32) for k in range(3))
+    hist = np.zeros(L * 8 + 16, np.uint32)
+    mb = lib().orc_cvd_gr_hist(_fp(x), _fp(y), _fp(z), len(x), L, M, N, dx,
+                               hist.ctypes.data_as(C.POINTER(C.c_uint32)), len(hist))
+    return hist[:mb].copy()
+
+
+def cvd_q6(rec, L, M, N, dx=0.125):
+    """Q6_GLO (CVD:1349-1520): (neighbour counts, local Q6, global Q6, 30-bin histogram)."""
+    x, y, z = (np.ascontiguousarray(rec[:, k], np.float32) for k in range(3))
+    n = len(x)
+    nb = np.zeros(n, np.uint32)
+    ql = np.zeros(n, np.float32)
+    qg = C.c_float()
+    histq = np.zeros(30, np.uint32)
+    lib().orc_cvd_q6(_fp(x), _fp(y), _fp(z), n, L, M, N, dx, nb.ctypes.data_as(C.POINTER(C.c_uint32)), _fp(ql),
+                     C.byref(qg), histq.ctypes.data_as(C.POINTER(C.c_uint32)))
+    return nb, ql, np.float32(qg.value), histq
 
 
 def dft3d(a, sign=-1):

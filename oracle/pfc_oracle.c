@@ -1066,3 +1066,194 @@ void orc_cryst_order(const double *x, const double *y, const double *z, int n, i
     free(fai);
     free(nb_index);
 }
+
+/* ------------------------------------------------------------------------- */
+/* CVD checkpoint analysis: atompositionCFGC2 (CVD:1067-1275), GR (CVD:1277-1347), */
+/* Q6_GLO (CVD:1349-1520).  Single rank: the x halo planes are copies of the     */
+/* first and last plane (the MPI_Sendrecv stub copies a rank's own plane,        */
+/* COM:101-110); neighbours are taken at flat offsets +-1 (n), +-N (m) and       */
+/* +-N*M (l) of the haloed buffer, without wrap, as the reference indexes them.  */
+/* ------------------------------------------------------------------------- */
+int orc_cvd_atoms(const float *phi, int L, int M, int N, float dx, float u0, float *phic_out, float *phimax_out,
+                  float *out4, int cap) {
+    const float phi_rat = 0.618f;
+    const long P = (long)L * M * N, NM = (long)N * M;
+    float phimax = -1.0f; /* phimm */
+    for (long i = 0; i < P; i++)
+        if (phi[i] > phimax) phimax = phi[i];
+    const float t = (phimax - u0) * phi_rat;
+    const float phic = u0 + t;
+    *phic_out = phic;
+    *phimax_out = phimax;
+    float *buf = (float *)malloc(sizeof(float) * (size_t)(NM * (L + 2)));
+    for (int lp = 0; lp < L + 2; lp++) {
+        const int src = lp == 0 ? 0 : (lp == L + 1 ? L - 1 : lp - 1);
+        memcpy(buf + lp * NM, phi + src * NM, sizeof(float) * (size_t)NM);
+    }
+    const float frame_x = (float)L * dx, frame_y = (float)M * dx, frame_z = (float)N * dx;
+    int num = 0;
+    for (int l = 1; l < L + 1; l++)
+        for (int m = 0; m < M; m++)
+            for (int n = 0; n < N; n++) {
+                const long idx = n + (long)N * (m + (long)M * l);
+                const float v = buf[idx];
+                if (!(v >= phic)) continue;
+                if (!(v >= buf[idx - NM] && v >= buf[idx + NM])) continue;
+                if (!(v >= buf[idx - N] && v >= buf[idx + N])) continue;
+                if (!(v >= buf[idx - 1] && v >= buf[idx + 1])) continue;
+                if (num < cap) {
+                    const float yd = (float)(m + 1) * dx, zd = (float)(n + 1) * dx, xd = (float)l * dx;
+                    out4[4 * num] = yd / frame_y;
+                    out4[4 * num + 1] = zd / frame_z;
+                    out4[4 * num + 2] = xd / frame_x;
+                    out4[4 * num + 3] = v;
+                }
+                num++;
+            }
+    free(buf);
+    if (num == 0) {
+        if (cap > 0) {
+            out4[0] = -1.0f;
+            out4[1] = -1.0f;
+            out4[2] = -1.0f;
+            out4[3] = 0.0f;
+        }
+        num = 1;
+    }
+    return num;
+}
+
+/* Pair geometry shared by GR and Q6_GLO (CVD:1297-1310): the minimum-image
+ * components (each scaled by the reference's frame of that slot) and the distance
+ * rr = sqrt(...) + 1e-6, the sum taken in double and stored to float. */
+static float cvd_pair(const float *x, const float *y, const float *z, int i, int j, float fx, float fy, float fz,
+                      float *r3, float *drx, float *dry, float *drz) {
+    r3[0] = (x[i] - x[j]) * fx;
+    r3[1] = (y[i] - y[j]) * fy;
+    r3[2] = (z[i] - z[j]) * fz;
+    r3[3] = r3[0] + fx;
+    r3[4] = r3[1] + fy;
+    r3[5] = r3[2] + fz;
+    r3[6] = r3[0] - fx;
+    r3[7] = r3[1] - fy;
+    r3[8] = r3[2] - fz;
+    *drx = min3f(r3[0], r3[3], r3[6]);
+    *dry = min3f(r3[1], r3[4], r3[7]);
+    *drz = min3f(r3[2], r3[5], r3[8]);
+    const float s = *drx * *drx + *dry * *dry + *drz * *drz;
+    return (float)((double)sqrtf(s) + 1e-6);
+}
+
+int orc_cvd_gr_hist(const float *x, const float *y, const float *z, int n, int L, int M, int N, float dx,
+                    unsigned *hist, int cap) {
+    const float a_lattice = 1.0f;
+    const float delr = (float)(a_lattice / 25.);
+    const int maxbin = (int)(((float)L * dx) / delr);
+    /* the reference scales x by L*dx, y by M*dx, z by N*dx although the records hold
+     * (y, z, x) fractions (CVD:1297-1299); reproduced */
+    const float fx = (float)L * dx, fy = (float)M * dx, fz = (float)N * dx;
+    for (int b = 0; b < maxbin && b < cap; b++) hist[b] = 0;
+    for (int i = 0; i < n - 1; i++)
+        for (int j = i + 1; j < n; j++) {
+            float r3[9], drx, dry, drz;
+            const float rr = cvd_pair(x, y, z, i, j, fx, fy, fz, r3, &drx, &dry, &drz);
+            const unsigned bin = (unsigned)(int)(rr / delr);
+            if ((double)rr > (double)a_lattice / sqrt(2.) * 0.5 && bin < (unsigned)maxbin && (int)bin < cap)
+                hist[bin] = hist[bin] + 2;
+        }
+    return maxbin;
+}
+
+void orc_cvd_q6(const float *x, const float *y, const float *z, int n, int L, int M, int N, float dx, unsigned *Nb,
+                float *ql_out, float *ql_global, unsigned *histq) {
+    const int CNmax = 24, l = 6;
+    const float a_lattice = 1.0f;
+    const float fx = (float)L * dx, fy = (float)M * dx, fz = (float)N * dx;
+    float *rij = (float *)calloc((size_t)n * CNmax + 1, sizeof(float));
+    float *CoX = (float *)calloc((size_t)n * CNmax + 1, sizeof(float));
+    float *CoY = (float *)calloc((size_t)n * CNmax + 1, sizeof(float));
+    float *CoZ = (float *)calloc((size_t)n * CNmax + 1, sizeof(float));
+    float *theta = (float *)calloc((size_t)n * CNmax + 1, sizeof(float));
+    float *fai = (float *)calloc((size_t)n * CNmax + 1, sizeof(float));
+    const double rhi = (double)a_lattice * sqrt(3.) / 2. * 1.2 + 1e-3;
+    const double rlo = (double)a_lattice * sqrt(3.) / 2. * 0.9 - 1e-3;
+    float rjx = 0, rjy = 0, rjz = 0;
+    for (int i = 0; i < n; i++) {
+        Nb[i] = 0;
+        for (int j = 0; j < n; j++) {
+            if (i == j) continue;
+            float r3[9], drx, dry, drz;
+            const float rr = cvd_pair(x, y, z, i, j, fx, fy, fz, r3, &drx, &dry, &drz);
+            if (!((double)rr <= rhi && (double)rr >= rlo)) continue;
+            Nb[i] = Nb[i] + 1;
+            if (Nb[i] > (unsigned)CNmax) continue;
+            rij[Nb[i] - 1 + CNmax * i] = rr;
+            for (int ii = 0; ii < 7; ii += 3)
+                if ((double)(fabsf(r3[ii]) - drx) < 1e-5) rjx = x[i] * fx - r3[ii];
+            for (int ii = 1; ii < 8; ii += 3)
+                if ((double)(fabsf(r3[ii]) - dry) < 1e-5) rjy = y[i] * fy - r3[ii];
+            for (int ii = 2; ii < 9; ii += 3)
+                if ((double)(fabsf(r3[ii]) - drz) < 1e-5) rjz = z[i] * fz - r3[ii];
+            CoX[Nb[i] - 1 + CNmax * i] = rjx;
+            CoY[Nb[i] - 1 + CNmax * i] = rjy;
+            CoZ[Nb[i] - 1 + CNmax * i] = rjz;
+        }
+    }
+    for (int i = 0; i < n; i++) {
+        if (!(Nb[i] > 0 && Nb[i] <= (unsigned)CNmax)) continue;
+        for (int j = 0; j < (int)Nb[i]; j++) {
+            const int k = j + CNmax * i;
+            theta[k] = acosf((CoZ[k] - z[i] * fz) / rij[k]);
+            const float dyv = CoY[k] - y[i] * fy;
+            if (dyv == 0.) fai[k] = 0.f;
+            else fai[k] = atanf(dyv / (CoX[k] - x[i] * fx));
+        }
+    }
+    float *qlmb_m = (float *)calloc((size_t)n + 1, sizeof(float));
+    double *qre = (double *)calloc((size_t)n + 1, sizeof(double)), *qim = (double *)calloc((size_t)n + 1, sizeof(double));
+    float Qlm_m = 0.f;
+    for (int m = -l; m <= l; m++) {
+        for (int i = 0; i < n; i++) {
+            double ar = 0.0, ai = 0.0;
+            qre[i] = 0.0;
+            qim[i] = 0.0;
+            if (Nb[i] > 0 && Nb[i] <= (unsigned)CNmax)
+                for (int j = 0; j < (int)Nb[i]; j++) {
+                    ar += (double)ylm_r(l, m, theta[j + CNmax * i], fai[j + CNmax * i]);
+                    ai += (double)ylm_c(l, m, theta[j + CNmax * i], fai[j + CNmax * i]);
+                    if (j == (int)Nb[i] - 1) {
+                        qre[i] = ar / (double)(float)Nb[i];
+                        qim[i] = ai / (double)(float)Nb[i];
+                    }
+                }
+        }
+        float SumNb = 0.f, Qlm_r = 0.f, Qlm_c = 0.f;
+        for (int i = 0; i < n; i++) {
+            qlmb_m[i] = (float)((double)qlmb_m[i] + (qre[i] * qre[i] + qim[i] * qim[i]));
+            Qlm_r = (float)((double)Qlm_r + (double)Nb[i] * qre[i]);
+            Qlm_c = (float)((double)Qlm_c + (double)Nb[i] * qim[i]);
+            SumNb = SumNb + (float)Nb[i];
+        }
+        Qlm_r /= SumNb;
+        Qlm_c /= SumNb;
+        Qlm_m += (Qlm_r * Qlm_r + Qlm_c * Qlm_c);
+    }
+    const float delq = 0.05f;
+    const float xishu = (float)(4 * PI_REF / (double)(float)(2 * l + 1));
+    *ql_global = sqrtf(xishu * Qlm_m);
+    for (int b = 0; b < 30; b++) histq[b] = 0;
+    for (int i = 0; i < n; i++) {
+        ql_out[i] = sqrtf(xishu * qlmb_m[i]);
+        const unsigned bin = (unsigned)(int)(ql_out[i] / delq);
+        if (bin < 30) histq[bin] = histq[bin] + 1;
+    }
+    free(rij);
+    free(CoX);
+    free(CoY);
+    free(CoZ);
+    free(theta);
+    free(fai);
+    free(qlmb_m);
+    free(qre);
+    free(qim);
+}

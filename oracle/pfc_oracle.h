@@ -88,6 +88,23 @@ void orc_elastic3d(const double *x, const double *y, const double *z, int n, int
 void orc_cryst_order(const double *x, const double *y, const double *z, int n, int L, int M, int N, float dx,
                      double *q4, double *q6);
 
+/* CVD checkpoint analysis (CVD:1067-1520).
+ * orc_cvd_atoms: atompositionCFGC2's peak finder on phi (float[L*M*N], layout
+ * n + N*(m + M*l)).  *phic / *phimax receive the threshold and the field maximum (the
+ * first line of phimax.txt); out4 receives up to cap records (x, y, z, phi) as the
+ * reference's pc_x / pc_y / pc_z / pc_phi (fractional y, z, x coordinates); returns
+ * the record count (>= 1: a (-1, -1, -1, 0) record stands for "no atoms"). */
+int orc_cvd_atoms(const float *phi, int L, int M, int N, float dx, float u0, float *phic, float *phimax,
+                  float *out4, int cap);
+/* GR (CVD:1277-1312): pair-distance histogram of the records; returns maxbin and
+ * fills hist[0..maxbin) (cap entries at most). */
+int orc_cvd_gr_hist(const float *x, const float *y, const float *z, int n, int L, int M, int N, float dx,
+                    unsigned *hist, int cap);
+/* Q6_GLO (CVD:1349-1520): per-record neighbour count nb, local Q6 ql, the global
+ * Q6 *ql_global and the 30-bin histogram of the local values. */
+void orc_cvd_q6(const float *x, const float *y, const float *z, int n, int L, int M, int N, float dx, unsigned *nb,
+                float *ql, float *ql_global, unsigned *histq);
+
 /* Splitmix64 helpers (COM:165-181), exposed for tests. */
 uint64_t orc_splitmix64_next(uint64_t *state);
 double orc_rng_u01(uint64_t *state);

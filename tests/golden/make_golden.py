@@ -8,7 +8,9 @@ the cases below and stores, per case, in tests/golden/<case>/:
   fields.npz        phi_<kd>, con_<kd>: the Float32 values of every kept VTI checkpoint,
                     shaped (L, M, N) in the reference layout n + N*(m + M*l)
   *.txt             the reference's text outputs, verbatim (energy.txt, Phimax_<kd>.txt,
-                    run_config.txt, and for the Elastic runs strain_/q4q6_/Phimax_)
+                    run_config.txt; for CVD runs the checkpoint analysis files phimax.txt,
+                    phiball_<kd>.cfg, hist_<kd>.txt, Grq6_<kd>.txt, Ql_<kd>.txt, HistQ_<kd>.txt;
+                    for the Elastic runs strain_/q4q6_/Phimax_)
   *.vti / *.pvti    a few raw checkpoint files, for byte-level writer tests
   stdout.txt        the reference's stdout (progress and peak-finder lines)
   case.json         the command line and grid
@@ -50,7 +52,13 @@ CASES = [
          keep=None, raw=[], elastic=[]),
     dict(name="cvd_32x32x8", model="cvd", grid=(32, 32, 8), args=["--steps", "11", "--mod", "5"],
          keep=None, raw=[], elastic=[]),
+    # CVD with more atoms: checkpoints 0, 20, 40 (Q6_GLO runs at kd % 20 == 0)
+    dict(name="cvd_128", model="cvd", grid=(128, 128, 1), args=["--steps", "41", "--mod", "20", "--u0", "0.05"],
+         keep=None, raw=[], elastic=[]),
 ]
+
+# CVD checkpoint analysis outputs (CVD:1067-1520), kept verbatim
+CVD_ANALYSIS = ("phimax.txt", "phiball_", "hist_", "Grq6_", "Ql_", "HistQ_")
 
 
 def read_vti(path, shape):
@@ -89,6 +97,8 @@ def run_case(c):
         np.savez_compressed(os.path.join(out, "fields.npz"), **arrays)
         for f in sorted(os.listdir(run_dir)):
             if f == "energy.txt" or f == "run_config.txt" or (f.startswith("Phimax_") and int(f[7:-4]) in keep):
+                shutil.copy(os.path.join(run_dir, f), out)
+            elif c["model"] == "cvd" and f.startswith(CVD_ANALYSIS):
                 shutil.copy(os.path.join(run_dir, f), out)
         for s in c["raw"]:
             for f in (f"phi_{s}_0.vti", f"con_{s}_0.vti", f"phi_{s}.pvti", f"con_{s}.pvti"):

@@ -9,11 +9,12 @@ import numpy as np
 import pytest
 
 import oracle as O
-from helpers import (case_params, energy_line, golden_case, phimax_elastic_lines, phimax_misfit_lines, q4q6_lines,
-                     strain_lines)
+from helpers import (case_params, cvd_phimax_lines, cvd_phimax_txt_lines, energy_line, golden_case, grq6_lines,
+                     hist_lines, histq_lines, phimax_elastic_lines, phimax_misfit_lines, phiball_lines, q4q6_lines,
+                     ql_lines, strain_lines)
 
 MISFIT_CASES = ["misfit_64", "misfit_128_s7", "misfit_256_c1"]
-CVD_CASES = ["cvd_64", "cvd_32x32x8"]
+CVD_CASES = ["cvd_64", "cvd_32x32x8", "cvd_128"]
 
 
 def oracle_params(meta, exact=1):
@@ -160,3 +161,34 @@ def test_pure_fp64_close_to_exact():
     fb, _ = b.fields()
     diff = np.abs(fa - fb).max()
     assert 0 < diff < 1e-5
+
+
+def text(path):
+    return open(path).read().split("\n")[:-1]
+
+
+@pytest.mark.parametrize("name", CVD_CASES)
+def test_oracle_cvd_checkpoint_analysis(name):
+    """atompositionCFGC2, GR and Q6_GLO (CVD:1067-1520) restated: every analysis file of
+    every checkpoint of the reference run, byte for byte."""
+    import os
+    d, meta, fields = golden_case(name)
+    L, M, N = meta["grid"]
+    u0 = float(np.float32(case_params(meta).get("u0", 0.01)))
+    phimax_txt = []
+    for kd in meta["checkpoints"]:
+        phic, pmax, rec = O.cvd_atoms(fields[f"phi_{kd}"], u0)
+        phimax_txt += cvd_phimax_txt_lines(kd, phic, pmax)
+        assert phiball_lines(rec, L, M, N, 0.125) == text(os.path.join(d, f"phiball_{kd}.cfg"))
+        assert cvd_phimax_lines(rec, L, M, N, 0.125) == text(os.path.join(d, f"Phimax_{kd}.txt"))
+        hist = O.cvd_gr_hist(rec, L, M, N)
+        assert hist_lines(hist) == text(os.path.join(d, f"hist_{kd}.txt"))
+        num_t = int((rec[:, 0] >= 0).sum())
+        assert grq6_lines(hist, num_t, L, M, N, 0.125) == text(os.path.join(d, f"Grq6_{kd}.txt"))
+        if kd % 20 == 0:
+            nb, ql, qg, histq = O.cvd_q6(rec, L, M, N)
+            assert ql_lines(nb, ql, qg) == text(os.path.join(d, f"Ql_{kd}.txt"))
+            assert histq_lines(histq) == text(os.path.join(d, f"HistQ_{kd}.txt"))
+        else:
+            assert not os.path.exists(os.path.join(d, f"Ql_{kd}.txt"))
+    assert phimax_txt == text(os.path.join(d, "phimax.txt"))
