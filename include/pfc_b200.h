@@ -155,6 +155,21 @@ int pfc_elastic3d(const double *x, const double *y, const double *z, int n, int 
 int pfc_cryst_order(const double *x, const double *y, const double *z, int n, int L, int M, int N, float dx,
                     double *q4, double *q6);
 
+/* CVD checkpoint analysis, atompositionCFGC2 (CVD:1067-1275): the peak finder on phi
+ * (float[L*M*N], layout n + N*(m + M*l)).  Writes up to cap records (x, y, z, phi) as
+ * the reference's pc_x / pc_y / pc_z / pc_phi (fractional y, z and x positions); a
+ * field without atoms gives the one record (-1, -1, -1, 0) as in the reference.
+ * *phic and *phimax receive the threshold u0 + (max - u0) * 0.618 and the maximum. */
+int pfc_cvd_atoms(const float *phi, int L, int M, int N, float dx, float u0, float *out4, int cap, int *count,
+                  float *phic, float *phimax);
+/* GR (CVD:1277-1347): pair-distance histogram of n records (the x, y, z columns of
+ * pfc_cvd_atoms); *maxbin receives its length, hist must hold cap >= maxbin entries. */
+int pfc_cvd_gr_hist(const float *x, const float *y, const float *z, int n, int L, int M, int N, float dx,
+                    uint32_t *hist, int cap, int *maxbin);
+/* Q6_GLO (CVD:1349-1520): per-record neighbour counts and local Q6, and the global Q6. */
+int pfc_cvd_q6(const float *x, const float *y, const float *z, int n, int L, int M, int N, float dx, uint32_t *nb,
+               float *ql, float *ql_global);
+
 /* 3-D complex-double DFT with FFTW's conventions (row-major, n2 fastest,
  * sign -1 = forward exp(-2 pi i jk/n), +1 = backward, unnormalised): the transform
  * the reference obtains from fftw_plan_dft_3d + fftw_execute (MIS:438-452).

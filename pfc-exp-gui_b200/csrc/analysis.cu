@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -611,6 +612,309 @@ int cryst_order_dev(const double *x, const double *y, const double *z, int n, in
     return e == cudaSuccess ? PFC_OK : cuda_error(e, "cryst_order kernels");
 }
 
+// ---------------------------------------------------------------------------
+// CVD checkpoint analysis (CVD:1067-1520): the atompositionCFGC2 peak finder, the GR
+// pair-distance histogram and Q6_GLO.  All float arithmetic is the reference's (this
+// file is compiled without FMA contraction).
+// ---------------------------------------------------------------------------
+
+// Peak finder of CVD:1112-1165 on a single rank: buffer planes 0 and L+1 are copies
+// of the first and last plane (the MPI_Sendrecv stub, pfc_common.h:101-110); a point
+// >= phic is an atom when it is >= its neighbours at flat buffer offsets +-N*M, +-N
+// and +-1 (no wrap: at the ends of a row the neighbour is in the adjacent row).
+// Emission index o = natural index n + N*(m + M*p), buffer plane p + 1.
+struct CvdPeak {
+    const float *phi;
+    const float *stats;  // device [phic, phimax]
+    int L, M, N;
+    float dx;
+    __device__ __forceinline__ float buf(long idx) const {
+        const long slab = (long)M * N;
+        long row = idx / slab - 1;
+        row = row < 0 ? 0 : (row > L - 1 ? L - 1 : row);
+        return phi[row * slab + idx % slab];
+    }
+    __device__ bool test(long o) const {
+        const long slab = (long)M * N, idx = o + slab;
+        const float v = phi[o];
+        if (!(v >= stats[0])) return false;
+        if (!(v >= buf(idx - slab) && v >= buf(idx + slab))) return false;
+        if (!(v >= buf(idx - N) && v >= buf(idx + N))) return false;
+        return v >= buf(idx - 1) && v >= buf(idx + 1);
+    }
+    // (pc_x, pc_y, pc_z, pc_phi) of CVD:1152-1155: fractional y, z and x positions
+    __device__ void record(long o, double *out) const {
+        const int n = (int)(o % N), m = (int)((o / N) % M), p = (int)(o / ((long)N * M));
+        const float fx = __fmul_rn((float)L, dx), fy = __fmul_rn((float)M, dx), fz = __fmul_rn((float)N, dx);
+        out[0] = (double)__fdiv_rn(__fmul_rn((float)(m + 1), dx), fy);
+        out[1] = (double)__fdiv_rn(__fmul_rn((float)(n + 1), dx), fz);
+        out[2] = (double)__fdiv_rn(__fmul_rn((float)(p + 1), dx), fx);
+        out[3] = (double)phi[o];
+    }
+    static constexpr int REC = 4;
+};
+
+// phimax starts at phimm = -1 (CVD:58, 1077); phic = u0 + (phimax - u0) * phi_rat.
+__global__ void k_cvd_stats(const float *phi, long n, float u0, float *stats) {
+    __shared__ float red[32];
+    float m = -1.0f;
+    for (long i = threadIdx.x; i < n; i += blockDim.x) {
+        const float v = phi[i];
+        if (v > m) m = v;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        const float o = __shfl_down_sync(0xffffffffu, m, off);
+        if (o > m) m = o;
+    }
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float s = -1.0f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+            if (red[w] > s) s = red[w];
+        stats[0] = __fadd_rn(u0, __fmul_rn(__fsub_rn(s, u0), 0.618f));
+        stats[1] = s;
+    }
+}
+
+// Pair geometry of GR and Q6_GLO (CVD:1297-1310): float differences of the records
+// scaled by the frame of each slot, minimum image, rr = sqrt(...) + 1e-6 added in
+// double and stored to float.
+struct CvdPair {
+    float r3[9];
+    float drx, dry, drz, rr;
+};
+__device__ __forceinline__ void cvd_pair(float xi, float yi, float zi, float xj, float yj, float zj, float fx, float fy,
+                                         float fz, CvdPair &g) {
+    g.r3[0] = __fmul_rn(__fsub_rn(xi, xj), fx);
+    g.r3[1] = __fmul_rn(__fsub_rn(yi, yj), fy);
+    g.r3[2] = __fmul_rn(__fsub_rn(zi, zj), fz);
+    g.r3[3] = __fadd_rn(g.r3[0], fx);
+    g.r3[4] = __fadd_rn(g.r3[1], fy);
+    g.r3[5] = __fadd_rn(g.r3[2], fz);
+    g.r3[6] = __fsub_rn(g.r3[0], fx);
+    g.r3[7] = __fsub_rn(g.r3[1], fy);
+    g.r3[8] = __fsub_rn(g.r3[2], fz);
+    g.drx = min3f(g.r3[0], g.r3[3], g.r3[6]);
+    g.dry = min3f(g.r3[1], g.r3[4], g.r3[7]);
+    g.drz = min3f(g.r3[2], g.r3[5], g.r3[8]);
+    const float s = __fadd_rn(__fadd_rn(__fmul_rn(g.drx, g.drx), __fmul_rn(g.dry, g.dry)), __fmul_rn(g.drz, g.drz));
+    g.rr = __double2float_rn(__dadd_rn((double)__fsqrt_rn(s), 1e-6));
+}
+
+// GR histogram (CVD:1293-1311): pairs i < j over upper-triangle tiles of 256 x 256
+// records; counts go to a shared-memory histogram, then to the global one (integer
+// additions, so the result does not depend on the order).
+constexpr int GR_TILE = 256;
+__global__ void k_cvd_gr(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z, int n,
+                         int tiles, float fx, float fy, float fz, float delr, int maxbin, double rmin,
+                         unsigned *__restrict__ hist) {
+    extern __shared__ unsigned sh[];
+    float *jx = reinterpret_cast<float *>(sh + maxbin), *jy = jx + GR_TILE, *jz = jy + GR_TILE;
+    int bi = 0, rem = blockIdx.x;
+    while (rem >= tiles - bi) {
+        rem -= tiles - bi;
+        ++bi;
+    }
+    const int bj = bi + rem;
+    for (int b = threadIdx.x; b < maxbin; b += blockDim.x) sh[b] = 0u;
+    const int j0 = bj * GR_TILE;
+    for (int t = threadIdx.x; t < GR_TILE; t += blockDim.x) {
+        const int j = j0 + t;
+        jx[t] = j < n ? x[j] : 0.f;
+        jy[t] = j < n ? y[j] : 0.f;
+        jz[t] = j < n ? z[j] : 0.f;
+    }
+    __syncthreads();
+    const int i = bi * GR_TILE + threadIdx.x;
+    if (i < n) {
+        const float xi = x[i], yi = y[i], zi = z[i];
+        const int jend = min(GR_TILE, n - j0);
+        for (int t = 0; t < jend; ++t) {
+            if (j0 + t <= i) continue;
+            CvdPair g;
+            cvd_pair(xi, yi, zi, jx[t], jy[t], jz[t], fx, fy, fz, g);
+            const unsigned bin = (unsigned)(int)__fdiv_rn(g.rr, delr);
+            if ((double)g.rr > rmin && bin < (unsigned)maxbin) atomicAdd(&sh[bin], 2u);
+        }
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < maxbin; b += blockDim.x)
+        if (sh[b]) atomicAdd(&hist[b], sh[b]);
+}
+
+// Q6_GLO neighbour lists (CVD:1376-1419): one warp per record i scans j in ascending
+// chunks of 32; every j != i with rr in [rlo, rhi] counts, the first 24 are kept.
+constexpr int Q6_CN = 24;
+__global__ void k_cvd_q6_neighbours(const float *__restrict__ x, const float *__restrict__ y,
+                                    const float *__restrict__ z, int n, float fx, float fy, float fz, double rlo,
+                                    double rhi, unsigned *__restrict__ nbcount, int *__restrict__ nbidx) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * 8 + warp;
+    if (i >= n) return;
+    const float xi = x[i], yi = y[i], zi = z[i];
+    unsigned Nb = 0;
+    for (int base = 0; base < n; base += 32) {
+        const int j = base + lane;
+        bool ok = false;
+        if (j < n && j != i) {
+            CvdPair g;
+            cvd_pair(xi, yi, zi, x[j], y[j], z[j], fx, fy, fz, g);
+            ok = (double)g.rr <= rhi && (double)g.rr >= rlo;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, ok);
+        if (ok) {
+            const unsigned slot = Nb + __popc(bal & ((1u << lane) - 1u));
+            if (slot < Q6_CN) nbidx[(long)Q6_CN * i + slot] = j;
+        }
+        Nb += __popc(bal);
+    }
+    if (lane == 0) nbcount[i] = Nb;
+}
+
+// Per record i (CVD:1435-1482): neighbour angles theta, fai and, for m = -6..6, the
+// neighbour average of Y_6m (qre, qim) and the float sum over m of |qlmb|^2 that gives
+// the local Q6.  Records with no neighbour or more than 24 contribute zeros.
+__global__ void k_cvd_q6_atoms(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
+                               int n, float fx, float fy, float fz, const unsigned *__restrict__ nbcount,
+                               const int *__restrict__ nbidx, double2 *__restrict__ qlmb, float *__restrict__ ql) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned Nb = nbcount[i];
+    const bool use = Nb > 0 && Nb <= (unsigned)Q6_CN;
+    float th[Q6_CN], fa[Q6_CN];
+    const float xi = x[i], yi = y[i], zi = z[i];
+    if (use) {
+        for (unsigned k = 0; k < Nb; ++k) {
+            const int j = nbidx[(long)Q6_CN * i + k];
+            CvdPair g;
+            cvd_pair(xi, yi, zi, x[j], y[j], z[j], fx, fy, fz, g);
+            // CoX/CoY/CoZ (CVD:1403-1412): the last image whose |offset| is within 1e-5
+            float rjx = 0.f, rjy = 0.f, rjz = 0.f;
+            for (int ii = 0; ii < 7; ii += 3)
+                if ((double)__fsub_rn(fabsf(g.r3[ii]), g.drx) < 1e-5) rjx = __fsub_rn(__fmul_rn(xi, fx), g.r3[ii]);
+            for (int ii = 1; ii < 8; ii += 3)
+                if ((double)__fsub_rn(fabsf(g.r3[ii]), g.dry) < 1e-5) rjy = __fsub_rn(__fmul_rn(yi, fy), g.r3[ii]);
+            for (int ii = 2; ii < 9; ii += 3)
+                if ((double)__fsub_rn(fabsf(g.r3[ii]), g.drz) < 1e-5) rjz = __fsub_rn(__fmul_rn(zi, fz), g.r3[ii]);
+            th[k] = acosf(__fdiv_rn(__fsub_rn(rjz, __fmul_rn(zi, fz)), g.rr));
+            const float dyv = __fsub_rn(rjy, __fmul_rn(yi, fy));
+            fa[k] = dyv == 0.f ? 0.f : atanf(__fdiv_rn(dyv, __fsub_rn(rjx, __fmul_rn(xi, fx))));
+        }
+    }
+    float acc = 0.f;
+    for (int mm = 0; mm < 13; ++mm) {
+        double re = 0.0, im = 0.0;
+        if (use) {
+            for (unsigned k = 0; k < Nb; ++k) {
+                re += (double)ylm_r(6, mm - 6, th[k], fa[k]);
+                im += (double)ylm_c(6, mm - 6, th[k], fa[k]);
+            }
+            re = re / (double)(float)Nb;
+            im = im / (double)(float)Nb;
+        }
+        qlmb[13L * i + mm] = make_double2(re, im);
+        acc = __double2float_rn(__dadd_rn((double)acc, __dadd_rn(__dmul_rn(re, re), __dmul_rn(im, im))));
+    }
+    const float xishu = __double2float_rn(4 * PI_REF / (double)(float)13);
+    ql[i] = __fsqrt_rn(__fmul_rn(xishu, acc));
+}
+
+// Global Q6 (CVD:1484-1497): for each m one thread adds the records in order, with
+// the reference's float accumulators; then the 13 terms are summed in m order.
+__global__ void k_cvd_q6_global(int n, const unsigned *__restrict__ nbcount, const double2 *__restrict__ qlmb,
+                                float *__restrict__ out) {
+    __shared__ float term[13];
+    const int mm = threadIdx.x;
+    if (mm < 13) {
+        float qr = 0.f, qc = 0.f, sum = 0.f;
+        for (int i = 0; i < n; ++i) {
+            const double2 q = qlmb[13L * i + mm];
+            const double nb = (double)nbcount[i];
+            qr = __double2float_rn(__dadd_rn((double)qr, __dmul_rn(nb, q.x)));
+            qc = __double2float_rn(__dadd_rn((double)qc, __dmul_rn(nb, q.y)));
+            sum = __fadd_rn(sum, (float)nbcount[i]);
+        }
+        qr = __fdiv_rn(qr, sum);
+        qc = __fdiv_rn(qc, sum);
+        term[mm] = __fadd_rn(__fmul_rn(qr, qr), __fmul_rn(qc, qc));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float qm = 0.f;
+        for (int k = 0; k < 13; ++k) qm = __fadd_rn(qm, term[k]);
+        const float xishu = __double2float_rn(4 * PI_REF / (double)(float)13);
+        out[0] = __fsqrt_rn(__fmul_rn(xishu, qm));
+    }
+}
+
+int cvd_atoms_dev(const float *d_phi, int L, int M, int N, float dx, float u0, double *d_out, int cap, int *count,
+                  float *stats_host, cudaStream_t st) {
+    float *stats = nullptr;
+    cudaError_t e = cudaMallocAsync(&stats, 2 * sizeof(float), st);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync CVD stats");
+    const long P = (long)L * M * N;
+    k_cvd_stats<<<1, 1024, 0, st>>>(d_phi, P, u0, stats);
+    CvdPeak f{d_phi, stats, L, M, N, dx};
+    int rc = compact(f, P, d_out, cap, count, st);
+    if (rc == PFC_OK) {
+        e = cudaMemcpyAsync(stats_host, stats, 2 * sizeof(float), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) rc = cuda_error(e, "CVD stats copy");
+    }
+    cudaFreeAsync(stats, st);
+    return rc;
+}
+
+// x, y, z: device records; hist: device [maxbin], zeroed here.
+int cvd_gr_dev(const float *x, const float *y, const float *z, int n, int L, int M, int N, float dx, unsigned *hist,
+               int maxbin, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(hist, 0, sizeof(unsigned) * (size_t)maxbin, st);
+    if (e != cudaSuccess) return cuda_error(e, "GR histogram clear");
+    if (n < 2) return PFC_OK;
+    const float fx = (float)L * dx, fy = (float)M * dx, fz = (float)N * dx;
+    const float delr = (float)(1.0f / 25.);
+    const int tiles = (n + GR_TILE - 1) / GR_TILE;
+    const long blocks = (long)tiles * (tiles + 1) / 2;
+    const size_t smem = sizeof(unsigned) * (size_t)maxbin + 3 * GR_TILE * sizeof(float);
+    static unsigned attr_mask = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (smem > 48 * 1024 && !(attr_mask & (1u << dev))) {
+        e = cudaFuncSetAttribute(k_cvd_gr, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (e != cudaSuccess) return cuda_error(e, "GR shared memory");
+        attr_mask |= 1u << dev;
+    }
+    if (smem > 200 * 1024) return set_error(PFC_E_INVALID, "GR histogram too large for shared memory");
+    k_cvd_gr<<<(unsigned)blocks, GR_TILE, smem, st>>>(x, y, z, n, tiles, fx, fy, fz, delr, maxbin,
+                                                     (double)1.0f / sqrt(2.) * 0.5, hist);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? PFC_OK : cuda_error(e, "k_cvd_gr");
+}
+
+// x, y, z: device records; nb, ql: device [n]; *ql_global_host receives the global Q6.
+int cvd_q6_dev(const float *x, const float *y, const float *z, int n, int L, int M, int N, float dx, unsigned *nb,
+               float *ql, float *ql_global_host, cudaStream_t st) {
+    if (n <= 0) return PFC_OK;
+    const float fx = (float)L * dx, fy = (float)M * dx, fz = (float)N * dx;
+    char *mem = nullptr;
+    const size_t bytes = (size_t)n * (Q6_CN * sizeof(int) + 13 * sizeof(double2)) + 256;
+    cudaError_t e = cudaMallocAsync(&mem, bytes, st);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMallocAsync Q6");
+    double2 *qlmb = (double2 *)mem;
+    int *nbidx = (int *)(qlmb + 13L * n);
+    float *glob = (float *)(nbidx + (long)Q6_CN * n);
+    const double rhi = (double)1.0f * sqrt(3.) / 2. * 1.2 + 1e-3, rlo = (double)1.0f * sqrt(3.) / 2. * 0.9 - 1e-3;
+    k_cvd_q6_neighbours<<<(n + 7) / 8, 256, 0, st>>>(x, y, z, n, fx, fy, fz, rlo, rhi, nb, nbidx);
+    k_cvd_q6_atoms<<<(n + 127) / 128, 128, 0, st>>>(x, y, z, n, fx, fy, fz, nb, nbidx, qlmb, ql);
+    k_cvd_q6_global<<<1, 32, 0, st>>>(n, nb, qlmb, glob);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ql_global_host, glob, sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFreeAsync(mem, st);
+    return e == cudaSuccess ? PFC_OK : cuda_error(e, "Q6 kernels");
+}
+
 }  // namespace pfc
 
 using namespace pfc;
@@ -679,6 +983,95 @@ extern "C" int pfc_phimax_elastic(const float *phi, int L, int M, int N, float d
     if (rc != PFC_OK) return rc;
     const int k = *count < cap ? *count : cap;
     if (k > 0) ATRY(cudaMemcpyAsync(out4, o.p, (size_t)k * 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ATRY(cudaStreamSynchronize(st));
+    return PFC_OK;
+}
+
+extern "C" int pfc_cvd_atoms(const float *phi, int L, int M, int N, float dx, float u0, float *out4, int cap,
+                             int *count, float *phic, float *phimax) {
+    if (!phi || !count || L <= 0 || M <= 0 || N <= 0 || cap < 1 || !out4)
+        return set_error(PFC_E_INVALID, "bad arguments to pfc_cvd_atoms");
+    cudaStream_t st;
+    int rc = host_ctx(&st);
+    if (rc != PFC_OK) return rc;
+    const long P = (long)L * M * N;
+    DevBuf f, o;
+    ATRY(cudaMalloc(&f.p, P * sizeof(float)));
+    ATRY(cudaMalloc(&o.p, (size_t)cap * 4 * sizeof(double)));
+    ATRY(cudaMemcpyAsync(f.p, phi, P * sizeof(float), cudaMemcpyHostToDevice, st));
+    float stats[2];
+    rc = cvd_atoms_dev((const float *)f.p, L, M, N, dx, u0, (double *)o.p, cap, count, stats, st);
+    if (rc != PFC_OK) return rc;
+    if (phic) *phic = stats[0];
+    if (phimax) *phimax = stats[1];
+    const int k = *count < cap ? *count : cap;
+    std::vector<double> rec((size_t)k * 4);
+    if (k > 0) ATRY(cudaMemcpyAsync(rec.data(), o.p, rec.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ATRY(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < rec.size(); ++i) out4[i] = (float)rec[i];  // the records hold float values
+    if (*count == 0) {  // the reference's "no atoms" record (CVD:1169)
+        out4[0] = out4[1] = out4[2] = -1.0f;
+        out4[3] = 0.0f;
+        *count = 1;
+    }
+    return PFC_OK;
+}
+
+static int upload_records(const float *x, const float *y, const float *z, int n, DevBuf &b, cudaStream_t st) {
+    ATRY(cudaMalloc(&b.p, (size_t)3 * n * sizeof(float) + 16));
+    float *d = (float *)b.p;
+    ATRY(cudaMemcpyAsync(d, x, n * sizeof(float), cudaMemcpyHostToDevice, st));
+    ATRY(cudaMemcpyAsync(d + n, y, n * sizeof(float), cudaMemcpyHostToDevice, st));
+    ATRY(cudaMemcpyAsync(d + 2 * n, z, n * sizeof(float), cudaMemcpyHostToDevice, st));
+    return PFC_OK;
+}
+
+extern "C" int pfc_cvd_gr_hist(const float *x, const float *y, const float *z, int n, int L, int M, int N, float dx,
+                               uint32_t *hist, int cap, int *maxbin) {
+    if (!x || !y || !z || n < 0 || !hist || !maxbin || L <= 0 || M <= 0 || N <= 0 || !(dx > 0.0f))
+        return set_error(PFC_E_INVALID, "bad arguments to pfc_cvd_gr_hist");
+    const float delr = (float)(1.0f / 25.);
+    const int mb = (int)(((float)L * dx) / delr);
+    if (mb > cap) return set_error(PFC_E_INVALID, "histogram capacity below maxbin");
+    cudaStream_t st;
+    int rc = host_ctx(&st);
+    if (rc != PFC_OK) return rc;
+    DevBuf r, h;
+    rc = upload_records(x, y, z, n > 0 ? n : 1, r, st);
+    if (rc != PFC_OK) return rc;
+    ATRY(cudaMalloc(&h.p, sizeof(unsigned) * (size_t)(mb > 0 ? mb : 1)));
+    const float *d = (const float *)r.p;
+    const int nn = n > 0 ? n : 1;
+    rc = cvd_gr_dev(d, d + nn, d + 2 * nn, n, L, M, N, dx, (unsigned *)h.p, mb, st);
+    if (rc != PFC_OK) return rc;
+    if (mb > 0) ATRY(cudaMemcpyAsync(hist, h.p, sizeof(unsigned) * mb, cudaMemcpyDeviceToHost, st));
+    ATRY(cudaStreamSynchronize(st));
+    *maxbin = mb;
+    return PFC_OK;
+}
+
+extern "C" int pfc_cvd_q6(const float *x, const float *y, const float *z, int n, int L, int M, int N, float dx,
+                          uint32_t *nb, float *ql, float *ql_global) {
+    if (!x || !y || !z || n < 0 || !nb || !ql || !ql_global || L <= 0 || M <= 0 || N <= 0)
+        return set_error(PFC_E_INVALID, "bad arguments to pfc_cvd_q6");
+    if (n == 0) {
+        *ql_global = std::numeric_limits<float>::quiet_NaN();  // the reference divides 0 by 0
+        return PFC_OK;
+    }
+    cudaStream_t st;
+    int rc = host_ctx(&st);
+    if (rc != PFC_OK) return rc;
+    DevBuf r, o;
+    rc = upload_records(x, y, z, n, r, st);
+    if (rc != PFC_OK) return rc;
+    ATRY(cudaMalloc(&o.p, (size_t)n * (sizeof(unsigned) + sizeof(float))));
+    const float *d = (const float *)r.p;
+    unsigned *dnb = (unsigned *)o.p;
+    float *dql = (float *)(dnb + n);
+    rc = cvd_q6_dev(d, d + n, d + 2 * n, n, L, M, N, dx, dnb, dql, ql_global, st);
+    if (rc != PFC_OK) return rc;
+    ATRY(cudaMemcpyAsync(nb, dnb, n * sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    ATRY(cudaMemcpyAsync(ql, dql, n * sizeof(float), cudaMemcpyDeviceToHost, st));
     ATRY(cudaStreamSynchronize(st));
     return PFC_OK;
 }

@@ -36,6 +36,12 @@ int phimax_misfit_dev(const float *d_phi, const float *d_con, int L, int M, floa
                       int cap, int *count, int *raw_count, cudaStream_t st);
 int phimax_elastic_dev(const float *d_phi, int L, int M, int N, float dx, double *d_out, int cap, int *count,
                        cudaStream_t st);
+int cvd_atoms_dev(const float *d_phi, int L, int M, int N, float dx, float u0, double *d_out, int cap, int *count,
+                  float *stats_host, cudaStream_t st);
+int cvd_gr_dev(const float *x, const float *y, const float *z, int n, int L, int M, int N, float dx, unsigned *hist,
+               int maxbin, cudaStream_t st);
+int cvd_q6_dev(const float *x, const float *y, const float *z, int n, int L, int M, int N, float dx, unsigned *nb,
+               float *ql, float *ql_global_host, cudaStream_t st);
 
 namespace ckpt {
 
@@ -397,6 +403,187 @@ inline int write_elastic_files(const std::string &outdir, int kd, const ElasticR
     diag << "q4q6_" << kd << ".txt: atoms=" << total << " x=[" << qMinX << "," << qMaxX << "] y=[" << qMinY << ","
          << qMaxY << "]" << std::endl;
     return total;
+}
+
+// ---------------------------------------------------------------------------
+// CVD checkpoint analysis (CVD:1067-1520): atompositionCFGC2's peak finder, GR, and
+// Q6_GLO at checkpoints with kd % 20 == 0.  The pair work runs on the GPU; the files
+// are formatted here with the reference's float arithmetic.
+// ---------------------------------------------------------------------------
+struct CvdAnalysis {
+    int kd = 0;
+    float phic = 0.f, phimax = 0.f;
+    int count = 0;             // records, including a (-1, -1, -1) "no atoms" record
+    std::vector<float> rec;    // 4 per record: pc_x, pc_y, pc_z, pc_phi
+    std::vector<unsigned> hist;
+    bool q6 = false;
+    std::vector<unsigned> nb;
+    std::vector<float> ql;
+    float ql_global = 0.f;
+};
+
+inline float cvd_delr() { return (float)(1.0f / 25.); }
+inline int cvd_maxbin(int L, float dx) { return (int)(((float)L * dx) / cvd_delr()); }
+
+// d_phi: device float field (layout n + N*(m + M*l)).
+inline int cvd_analyze(const float *d_phi, int L, int M, int N, float dx, float u0, int kd, cudaStream_t st,
+                       DevScratch &scratch, CvdAnalysis &r) {
+    const long P = (long)L * M * N;
+    const long cap = P + 1;
+    const int maxbin = cvd_maxbin(L, dx);
+    const size_t rec_bytes = ((size_t)cap * 4 * sizeof(double) + 255) / 256 * 256;
+    const size_t xyz_bytes = ((size_t)3 * cap * sizeof(float) + 255) / 256 * 256;
+    const size_t hist_bytes = ((size_t)(maxbin > 0 ? maxbin : 1) * sizeof(unsigned) + 255) / 256 * 256;
+    const size_t q_bytes = (size_t)cap * (sizeof(unsigned) + sizeof(float)) + 256;
+    if (!scratch.ensure(rec_bytes + xyz_bytes + hist_bytes + q_bytes)) return PFC_E_NOMEM;
+    char *base = (char *)scratch.p;
+    double *d_rec = (double *)base;
+    float *d_xyz = (float *)(base + rec_bytes);
+    unsigned *d_hist = (unsigned *)(base + rec_bytes + xyz_bytes);
+    unsigned *d_nb = (unsigned *)(base + rec_bytes + xyz_bytes + hist_bytes);
+    float *d_ql = (float *)(d_nb + cap);
+    r.kd = kd;
+    float stats[2];
+    int found = 0;
+    int rc = cvd_atoms_dev(d_phi, L, M, N, dx, u0, d_rec, (int)cap, &found, stats, st);
+    if (rc != PFC_OK) return rc;
+    r.phic = stats[0];
+    r.phimax = stats[1];
+    std::vector<double> rec((size_t)found * 4);
+    if (found > 0 &&
+        cudaMemcpyAsync(rec.data(), d_rec, rec.size() * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return PFC_E_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return PFC_E_CUDA;
+    r.count = found > 0 ? found : 1;
+    r.rec.assign((size_t)r.count * 4, 0.f);
+    for (size_t i = 0; i < rec.size(); ++i) r.rec[i] = (float)rec[i];
+    if (found == 0) r.rec[0] = r.rec[1] = r.rec[2] = -1.0f;  // CVD:1169
+    const int n = r.count;
+    std::vector<float> xyz((size_t)3 * n);
+    for (int i = 0; i < n; ++i) {
+        xyz[i] = r.rec[4 * i];
+        xyz[n + i] = r.rec[4 * i + 1];
+        xyz[2 * n + i] = r.rec[4 * i + 2];
+    }
+    if (cudaMemcpyAsync(d_xyz, xyz.data(), xyz.size() * sizeof(float), cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return PFC_E_CUDA;
+    rc = cvd_gr_dev(d_xyz, d_xyz + n, d_xyz + 2 * n, n, L, M, N, dx, d_hist, maxbin, st);
+    if (rc != PFC_OK) return rc;
+    r.hist.assign(maxbin > 0 ? maxbin : 0, 0u);
+    if (maxbin > 0 &&
+        cudaMemcpyAsync(r.hist.data(), d_hist, maxbin * sizeof(unsigned), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return PFC_E_CUDA;
+    r.q6 = kd >= 0 && kd % 20 == 0;  // CVD:1254
+    if (r.q6) {
+        rc = cvd_q6_dev(d_xyz, d_xyz + n, d_xyz + 2 * n, n, L, M, N, dx, d_nb, d_ql, &r.ql_global, st);
+        if (rc != PFC_OK) return rc;
+        r.nb.assign(n, 0u);
+        r.ql.assign(n, 0.f);
+        if (cudaMemcpyAsync(r.nb.data(), d_nb, n * sizeof(unsigned), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaMemcpyAsync(r.ql.data(), d_ql, n * sizeof(float), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+            return PFC_E_CUDA;
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess) return PFC_E_CUDA;
+    return PFC_OK;
+}
+
+// phimax.txt (appended), phiball_<kd>.cfg, Phimax_<kd>.txt, hist_<kd>.txt, Grq6_<kd>.txt
+// and, with Q6, Ql_<kd>.txt and HistQ_<kd>.txt, as rank 0 of the reference writes them.
+inline void write_cvd_files(const std::string &outdir, int L, int M, int N, float dx, const CvdAnalysis &r) {
+    const int kd = r.kd;
+    const float frame_x = (float)L * dx, frame_y = (float)M * dx, frame_z = (float)N * dx;
+    {
+        std::ofstream o(opath(outdir, "phimax.txt"), std::ios_base::out | std::ios_base::app);
+        o << kd << " , " << r.phic << " , " << r.phimax << " , " << 0 << std::endl;
+        o << "phimax is done" << " " << "myid=" << 0 << std::endl;
+        o << " buf is done " << std::endl;
+        o << " pc_xyz is initializing " << std::endl;
+        o << " pc_xyz is done " << std::endl;
+        o << " pc_xyz has been gathered " << std::endl;
+    }
+    const int n = r.count;
+    int total = 0;
+    for (int i = 0; i < n; ++i) total += r.rec[4 * i] >= 0 ? 1 : 0;
+    char fn[64];
+    {
+        snprintf(fn, sizeof(fn), "phiball_%d.cfg", kd);
+        std::ofstream f(opath(outdir, fn), std::ios_base::out);
+        f.setf(std::ios_base::fixed, std::ios_base::floatfield);
+        f.precision(4);
+        const float ai = 10.0f;
+        f << "Number of particles = " << total << std::endl;
+        f << "A = " << ai << " Angstrom (basic length-scale)" << std::endl;
+        f << "H0(1,1) = " << frame_y << " A " << std::endl;
+        f << "H0(1,2) = " << 0 << " A " << std::endl;
+        f << "H0(1,3) = " << 0 << " A " << std::endl;
+        f << "H0(2,1) = " << 0 << " A " << std::endl;
+        f << "H0(2,2) = " << frame_z << " A " << std::endl;
+        f << "H0(2,3) = " << 0 << " A " << std::endl;
+        f << "H0(3,1) = " << 0 << " A " << std::endl;
+        f << "H0(3,2) = " << 0 << " A " << std::endl;
+        f << "H0(3,3) = " << frame_x << " A " << std::endl;
+        f << ".NO_VELOCITY." << std::endl;
+        f << "entry_count = 3" << std::endl;
+        f << "63.546" << std::endl;
+        f << "Cu" << std::endl;
+        for (int i = 0; i < n; ++i)
+            if (r.rec[4 * i] >= 0) f << r.rec[4 * i] << " " << r.rec[4 * i + 1] << " " << r.rec[4 * i + 2] << std::endl;
+    }
+    {
+        snprintf(fn, sizeof(fn), "Phimax_%d.txt", kd);
+        std::ofstream f(opath(outdir, fn), std::ios_base::out);
+        f.setf(std::ios_base::fixed, std::ios_base::floatfield);
+        f.precision(4);
+        f << total << std::endl;
+        f << "Kommentar" << std::endl;
+        for (int i = 0; i < n; ++i)
+            if (r.rec[4 * i] >= 0)
+                f << r.rec[4 * i + 2] * frame_x << " " << r.rec[4 * i] * frame_y << " " << r.rec[4 * i + 1] * frame_z
+                  << " " << r.rec[4 * i + 3] << std::endl;
+    }
+    const int maxbin = (int)r.hist.size();
+    {
+        snprintf(fn, sizeof(fn), "hist_%d.txt", kd);
+        std::ofstream f(opath(outdir, fn), std::ios_base::out);
+        f.setf(std::ios_base::fixed, std::ios_base::floatfield);
+        f.precision(4);
+        for (int ii = 0; ii < maxbin; ii++) f << ii << " " << r.hist[ii] << " " << maxbin << std::endl;
+    }
+    {
+        const float delr = cvd_delr();
+        const float rho = float(total) / float((float)(L * M * N) * dx * dx * dx);
+        const float preco = (float)(4. * 3.1415926 * rho / 3.);
+        snprintf(fn, sizeof(fn), "Grq6_%d.txt", kd);
+        std::ofstream f(opath(outdir, fn), std::ios_base::out);
+        f.setf(std::ios_base::fixed, std::ios_base::floatfield);
+        f.precision(4);
+        for (int jj = 0; jj < maxbin; jj++) {
+            const float rlower = float(jj) * delr;
+            const float rupper = rlower + delr;
+            const float nideal = preco * (rupper * rupper * rupper - rlower * rlower * rlower);
+            const float gr = float(r.hist[jj]) / float(1) / float(total) / nideal;
+            f << jj * delr << " " << gr << " " << r.hist[jj] << " " << nideal << std::endl;
+        }
+    }
+    if (!r.q6) return;
+    const float delq = 0.05f;
+    unsigned histq[30] = {0};
+    {
+        snprintf(fn, sizeof(fn), "Ql_%d.txt", kd);
+        std::ofstream f(opath(outdir, fn), std::ios_base::out);
+        f.setf(std::ios_base::fixed, std::ios_base::floatfield);
+        f.precision(6);
+        for (int i = 0; i < n; i++) {
+            f << i << " " << r.nb[i] << " " << r.ql[i] << " " << r.ql_global << std::endl;
+            const unsigned bin = (unsigned)(int)(r.ql[i] / delq);
+            if (bin < 30) histq[bin] = histq[bin] + 1;
+        }
+    }
+    snprintf(fn, sizeof(fn), "HistQ_%d.txt", kd);
+    std::ofstream f(opath(outdir, fn), std::ios_base::out);
+    f.setf(std::ios_base::fixed, std::ios_base::floatfield);
+    f.precision(4);
+    for (int i = 0; i < 30; i++) f << (i + 1) * delq << " " << histq[i] << std::endl;
 }
 
 }  // namespace ckpt

@@ -540,6 +540,7 @@ int run_cvd_cli(int argc, char **argv) {
     pfc_run *r = g.r;
     const long P = (long)L * M * N;
     std::vector<float> phi(P), con(P);
+    DevScratch phi_dev, scratch;
     for (int t = 0; t < o.steps; t++) {
         fprintf(stderr, "PFC_PROGRESS step=%d total=%d\n", t + 1, o.steps);
         fflush(stderr);
@@ -548,6 +549,15 @@ int run_cvd_cli(int argc, char **argv) {
         if ((t % o.mod) == 0) {
             const int kd = t;
             if (pfc_run_get_fields_f32(r, phi.data(), con.data()) != PFC_OK) return gpu_fail("checkpoint fields");
+            // atompositionCFGC2 + GR + Q6_GLO (CVD:427, 1067-1520) on the checkpoint's phi
+            if (!phi_dev.ensure(P * sizeof(float)) ||
+                cudaMemcpyAsync(phi_dev.p, phi.data(), P * sizeof(float), cudaMemcpyHostToDevice, r->stream) !=
+                    cudaSuccess)
+                return gpu_fail("CVD analysis upload");
+            CvdAnalysis ca;
+            if (cvd_analyze((const float *)phi_dev.p, L, M, N, o.dx, o.u0, kd, r->stream, scratch, ca) != PFC_OK)
+                return gpu_fail("CVD analysis");
+            write_cvd_files(o.outdir, L, M, N, o.dx, ca);
             if (!write_checkpoint_fields(o.outdir, kd, phi.data(), con.data(), L, M, N)) {
                 cerr << "pfc-exp-cli: failed to write checkpoint files" << endl;
                 return 2;

@@ -122,7 +122,7 @@ struct pfc_engine {
     bool composition_changed = true;
     cudaGraphExec_t graph = nullptr;
     double reserved = 0.0;
-    DevScratch atoms_scratch;
+    DevScratch atoms_scratch, cvd_scratch;
     std::vector<cudaEvent_t> join_events;
     cudaEvent_t fork_event = nullptr;
     double *h_ehist = nullptr;  // pinned staging for CVD energy slots, one area per segment
@@ -423,10 +423,18 @@ int cvd_after_quantum(pfc_engine *e, Job *j, int q) {
         j->phi = phi;
         j->con = con;
     }
+    // the checkpoint's atom analysis (CVD:427, 1067-1520) on the resident field
+    auto ca = std::make_shared<CvdAnalysis>();
+    if (ckpt) {
+        const int rc = cvd_analyze(r->desc.psi_real, r->L, r->M, r->N, r->p.dx, r->p.u0, t_end - 1, e->main,
+                                   e->cvd_scratch, *ca);
+        if (rc != PFC_OK) return rc;
+    }
     const std::string outdir = j->outdir;
     const int L = r->L, M = r->M, N = r->N;
+    const float dx = r->p.dx;
     const JobTimes jt = j->times();
-    write_task(e, [e, outdir, first, q, lines, ckpt, phi, con, L, M, N, jt] {
+    write_task(e, [e, outdir, first, q, lines, ckpt, phi, con, L, M, N, dx, ca, jt] {
         int status = PFC_OK;
         // energy.txt gets one line per step, kd = the step's 0-based loop index (CVD:442);
         // the checkpoint's files come before its energy line, as in the CLI
@@ -434,12 +442,15 @@ int cvd_after_quantum(pfc_engine *e, Job *j, int q) {
             const int kd = first + s;
             if (outdir.empty()) continue;
             if (ckpt && s == q - 1) {
+                write_cvd_files(outdir, L, M, N, dx, *ca);
                 if (!write_checkpoint_fields(outdir, kd, phi->data(), con->data(), L, M, N)) status = PFC_E_IO;
                 timestamp_line(outdir, kd);
             }
             append_energy_line(outdir, kd, lines[s].first, lines[s].second);
         }
-        if (ckpt) post(e, jt, PFC_EV_CHECKPOINT, status, first + q - 1, 0, lines[q - 1].first, lines[q - 1].second);
+        int natoms = 0;
+        for (int i = 0; i < ca->count; ++i) natoms += ca->rec[4 * i] >= 0 ? 1 : 0;
+        if (ckpt) post(e, jt, PFC_EV_CHECKPOINT, status, first + q - 1, natoms, lines[q - 1].first, lines[q - 1].second);
     });
     return PFC_OK;
 }

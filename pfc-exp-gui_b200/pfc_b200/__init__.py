@@ -137,6 +137,11 @@ def lib():
                            P(C.c_uint32)], C.c_int),
         "pfc_cryst_order": ([dp, dp, dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, dp, dp], C.c_int),
         "pfc_dft3d": ([dp, dp, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
+        "pfc_cvd_atoms": ([fp, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, fp, C.c_int, P(C.c_int), fp, fp],
+                          C.c_int),
+        "pfc_cvd_gr_hist": ([fp, fp, fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, P(C.c_uint32), C.c_int,
+                             P(C.c_int)], C.c_int),
+        "pfc_cvd_q6": ([fp, fp, fp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, P(C.c_uint32), fp, fp], C.c_int),
         "pfc_batch_advance_timed": ([vp, C.c_int, P(C.c_float)], C.c_int),
         "pfc_batch_kernel_times": ([vp, C.c_int, dp, dp], C.c_int),
         "pfc_run_cli": ([C.c_int, P(C.c_char_p)], C.c_int),
@@ -383,6 +388,39 @@ def cryst_order(x, y, z, L, M, N, dx=0.125):
     q6 = np.zeros(n, np.float64)
     _check(lib().pfc_cryst_order(_dp(x), _dp(y), _dp(z), n, L, M, N, dx, _dp(q4), _dp(q6)), "pfc_cryst_order")
     return q4, q6
+
+
+def cvd_atoms(phi, u0, dx=0.125):
+    """CVD checkpoint peak finder (atompositionCFGC2) on a float32 field shaped (L, M, N).
+    Returns (phic, phimax, records[n, 4]) with records (x, y, z, phi) as the reference's pc_*."""
+    phi = np.ascontiguousarray(phi, np.float32)
+    L, M, N = phi.shape
+    cap = L * M * N + 1
+    out = np.zeros((cap, 4), np.float32)
+    n, phic, pmax = C.c_int(), C.c_float(), C.c_float()
+    _check(lib().pfc_cvd_atoms(_fp(phi), L, M, N, dx, u0, _fp(out), cap, C.byref(n), C.byref(phic), C.byref(pmax)),
+           "pfc_cvd_atoms")
+    return np.float32(phic.value), np.float32(pmax.value), out[: n.value].copy()
+
+
+def cvd_gr_hist(rec, L, M, N, dx=0.125):
+    x, y, z = (np.ascontiguousarray(rec[:, k], np.float32) for k in range(3))
+    hist = np.zeros(L * 8 + 16, np.uint32)
+    mb = C.c_int()
+    _check(lib().pfc_cvd_gr_hist(_fp(x), _fp(y), _fp(z), len(x), L, M, N, dx,
+                                 hist.ctypes.data_as(C.POINTER(C.c_uint32)), len(hist), C.byref(mb)), "pfc_cvd_gr_hist")
+    return hist[: mb.value].copy()
+
+
+def cvd_q6(rec, L, M, N, dx=0.125):
+    x, y, z = (np.ascontiguousarray(rec[:, k], np.float32) for k in range(3))
+    n = len(x)
+    nb = np.zeros(n, np.uint32)
+    ql = np.zeros(n, np.float32)
+    qg = C.c_float()
+    _check(lib().pfc_cvd_q6(_fp(x), _fp(y), _fp(z), n, L, M, N, dx, nb.ctypes.data_as(C.POINTER(C.c_uint32)),
+                            _fp(ql), C.byref(qg)), "pfc_cvd_q6")
+    return nb, ql, np.float32(qg.value)
 
 
 def dft3d(a, sign=-1):

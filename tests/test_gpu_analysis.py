@@ -104,3 +104,44 @@ def test_empty_and_single_atom_inputs():
     assert nb[0] == 0 and st[0] == 0.0
     q4, q6 = P.cryst_order([1.0], [1.0], [0.125], 8, 8, 1)
     assert q4[0] == 0.0 and q6[0] == 0.0
+
+
+CVD_CASES = ["cvd_64", "cvd_128", "cvd_32x32x8"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", CVD_CASES)
+def test_cvd_analysis_matches_oracle(name):
+    """atompositionCFGC2 / GR / Q6_GLO (CVD:1067-1520) on the reference's checkpoint
+    fields: threshold, atom records and histogram bit-exact; Q6 within 2e-6 (the GPU's
+    acosf/atanf/cosf/sinf differ from the C library's in the last bits)."""
+    from helpers import case_params
+    d, meta, fields = golden_case(name)
+    L, M, N = meta["grid"]
+    u0 = float(np.float32(case_params(meta).get("u0", 0.01)))
+    for kd in meta["checkpoints"]:
+        phi = fields[f"phi_{kd}"]
+        phic, pmax, rec = P.cvd_atoms(phi, u0)
+        ophic, opmax, orec = O.cvd_atoms(phi, u0)
+        assert phic == ophic and pmax == opmax
+        assert rec.shape == orec.shape and np.array_equal(rec.view(np.uint32), orec.view(np.uint32))
+        assert np.array_equal(P.cvd_gr_hist(rec, L, M, N), O.cvd_gr_hist(orec, L, M, N))
+        nb, ql, qg = P.cvd_q6(rec, L, M, N)
+        onb, oql, oqg, _ = O.cvd_q6(orec, L, M, N)
+        assert np.array_equal(nb, onb)
+        assert np.abs(ql - oql).max() <= 2e-6
+        assert abs(float(qg) - float(oqg)) <= 2e-6
+
+
+@pytest.mark.gpu
+def test_cvd_analysis_without_atoms():
+    """A field below the threshold everywhere: the reference's single (-1, -1, -1)
+    record, no pairs in the histogram, no neighbours."""
+    phi = np.full((32, 32, 1), -2.0, np.float32)
+    phic, pmax, rec = P.cvd_atoms(phi, 0.05)
+    ophic, opmax, orec = O.cvd_atoms(phi, 0.05)
+    assert phic == ophic and pmax == opmax == np.float32(-1.0)
+    assert rec.shape == (1, 4) and np.array_equal(rec, orec) and rec[0, 0] == -1.0
+    assert not P.cvd_gr_hist(rec, 32, 32, 1).any()
+    nb, ql, qg = P.cvd_q6(rec, 32, 32, 1)
+    assert nb[0] == 0 and ql[0] == 0.0 and np.isnan(qg)

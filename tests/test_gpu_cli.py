@@ -142,6 +142,41 @@ def test_cli_cvd_matches_reference(tmp_path):
     assert [g[0] for g in got] == [r_[0] for r_ in ref]
     for g, r_ in zip(got, ref):
         assert abs(float(g[1]) - float(r_[1])) <= 1e-5 * abs(float(r_[1])) + 1e-9
+    check_cvd_analysis_files(out, d, (0, 10, 20), 1e-4)
+
+
+def numbers(path):
+    return [[float(v) if v.replace(".", "", 1).replace("-", "", 1).isdigit() else v for v in l.replace(",", " ").split()]
+            for l in open(path).read().splitlines()]
+
+
+def same_numbers(a, b, tol):
+    if len(a) != len(b):
+        return False
+    for la, lb in zip(a, b):
+        if len(la) != len(lb):
+            return False
+        for x, y in zip(la, lb):
+            if isinstance(x, float) and isinstance(y, float):
+                if abs(x - y) > tol * max(1.0, abs(y)):
+                    return False
+            elif x != y:
+                return False
+    return True
+
+
+def check_cvd_analysis_files(out, d, kds, tol):
+    """The CVD checkpoint analysis files (CVD:1067-1520) against the reference run's:
+    the same atoms at the same grid positions (so the same pair histogram); values
+    printed from the (FP32-path) fields within tol."""
+    for kd in kds:
+        for f in (f"phiball_{kd}.cfg", f"hist_{kd}.txt", f"Grq6_{kd}.txt"):
+            assert (out / f).read_text() == open(f"{d}/{f}").read(), f
+        assert same_numbers(numbers(out / f"Phimax_{kd}.txt"), numbers(f"{d}/Phimax_{kd}.txt"), tol)
+        if kd % 20 == 0:
+            assert same_numbers(numbers(out / f"Ql_{kd}.txt"), numbers(f"{d}/Ql_{kd}.txt"), 1e-5)
+            assert (out / f"HistQ_{kd}.txt").read_text() == open(f"{d}/HistQ_{kd}.txt").read()
+    assert same_numbers(numbers(out / "phimax.txt"), numbers(f"{d}/phimax.txt"), tol)
 
 
 @pytest.mark.gpu
@@ -153,3 +188,4 @@ def test_cli_fp64_precision_3d(tmp_path):
     for kd in (0, 5, 10):
         vals, _, _ = read_vti(out / f"phi_{kd}_0.vti")
         assert np.abs(vals - fields[f"phi_{kd}"]).max() <= 1e-6
+    check_cvd_analysis_files(out, d, (0, 5, 10), 1e-5)
