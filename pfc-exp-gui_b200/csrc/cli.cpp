@@ -343,10 +343,6 @@ int run_misfit_cli(int argc, char **argv) {
         log << "# Checkpoint timestamps - Step number and milliseconds since epoch" << endl;
     else
         cerr << "Warning: Failed to open checkpoint_timestamps.txt for writing" << endl;
-    if (o.axx != 0.0f) {
-        cerr << "pfc-exp-cli: --axx > 0 (stochastic noise) is not supported by this engine" << endl;
-        return 2;
-    }
 
     pfc_run_params p;
     pfc_default_params(PFC_MODEL_MISFIT, &p);

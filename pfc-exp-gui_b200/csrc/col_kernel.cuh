@@ -36,6 +36,41 @@ struct GradientOf {
     }
 };
 
+// Spectrum of the noise field at mode (l, km) of step t.  The reference draws real-space
+// white noise with a sequential polar Box-Muller generator (Gauss, MIS:951-981) and
+// transforms it (p5); the transform of white noise is itself white, so the modes are
+// drawn here directly, with the distribution the reference's masks leave
+// (MIS:1002-1003): re and im independent N(0, P/4), except at the four self-conjugate
+// modes (l in {0, L/2}, km in {0, M/2}) where re ~ N(0, P) and im = 0; along the
+// self-conjugate columns km = 0 and M/2, mode L - l is the conjugate of mode l.
+// Stream: the two normals of canonical mode c = (t*L + l)*(M/2 + 1) + km come from
+// Box-Muller of the splitmix64 outputs at positions 2c and 2c + 1 of the run's key.
+__device__ __forceinline__ unsigned long long sm64_out(unsigned long long z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+__device__ float2 noise_mode(unsigned long long key, int t, int l, int km, int L, int M) {
+    const int H = M / 2;
+    bool conj = false;
+    if ((km == 0 || km == H) && l > L / 2) {
+        l = L - l;
+        conj = true;
+    }
+    const unsigned long long c = ((unsigned long long)t * L + l) * (unsigned long long)(H + 1) + km;
+    const unsigned long long g = 0x9E3779B97F4A7C15ULL;
+    const unsigned long long w1 = sm64_out(key + (2 * c + 1) * g), w2 = sm64_out(key + (2 * c + 2) * g);
+    const float u1 = ((float)(w1 >> 40) + 0.5f) * (1.0f / 16777216.0f);  // (0, 1)
+    const float u2 = (float)(w2 >> 40) * (1.0f / 16777216.0f);           // [0, 1)
+    const float rad = sqrtf(-2.0f * logf(u1));
+    float sn, cs;
+    sincospif(2.0f * u2, &sn, &cs);
+    const float P = (float)L * (float)M;
+    if ((l == 0 || l == L / 2) && (km == 0 || km == H)) return make_float2(sqrtf(P) * rad * cs, 0.0f);
+    const float s = 0.5f * sqrtf(P);
+    return make_float2(s * rad * cs, conj ? -s * rad * sn : s * rad * sn);
+}
+
 template <int L, int C, int NT> __device__ __forceinline__ void tile_in(const float2 *__restrict__ g, float2 *sm) {
     __syncthreads();
     const float4 *g4 = reinterpret_cast<const float4 *>(g);
@@ -78,17 +113,29 @@ __global__ void __launch_bounds__(ColCfg<L>::NT, 3) k_col_step(const RunDesc *__
         tile_in<L, C, NT>(d.inn + tile, s);
         fft<L, C, NT, true, SP_SMEM, SP_SMEM>(s, s, s, tw, b);
     }
+    const int nstep = (MODE != COL_PREPARE && d.noise_amp != 0.0f) ? *d.step_ctr : -1;
     for (int e = threadIdx.x; e < L * C; e += NT) {
         const int l = e / C, c = e % C, km = km0 + c;
         const int pi = spad(e);
         float2 v = Pk[pi];
         if (MODE != COL_PREPARE) {
-            // (psi^ - Mn dt k^2 N^) / (1 + Mn dt k^2) / L; the FP64-built factor is 0 at k = 0
+            // (psi^ - Mn dt k^2 N^ [+ dt b0 xi^ |k| lowpass]) / (1 + Mn dt k^2) / L; the
+            // FP64-built factor is 0 at k = 0
             const float kl = d.krefl[l], kmv = d.krefm[km <= H ? km : 0];
-            const float an = mn_dt * (kl * kl + kmv * kmv);
+            const float ks = kl * kl + kmv * kmv;
+            const float an = mn_dt * ks;
             const float2 nh = s[pi];
             const float f = d.kden[tile + e].x;
-            v = make_float2((v.x - an * nh.x) * f, (v.y - an * nh.y) * f);
+            float rx = v.x - an * nh.x, ry = v.y - an * nh.y;
+            if (nstep >= 0 && km <= H) {
+                // MAINEQUATIONC2_NOI's noise term (MIS:1002-1003), lowpass at |k| = 2 pi
+                const float2 xi = noise_mode(d.noise_key, nstep, l, km, L, d.M);
+                const float sk = sqrtf(ks);
+                const float w = d.noise_amp * sk * (0.5f - 0.5f * tanhf((sk - 6.2831852f) / 0.1f));
+                rx += w * xi.x;
+                ry += w * xi.y;
+            }
+            v = make_float2(rx * f, ry * f);
         } else {
             v = (l == 0 && km == 0) ? make_float2(0.f, 0.f) : cscale(v, invL);
         }

@@ -267,13 +267,21 @@ bool is_supported_len(int n) { return n >= 32 && n <= 2048 && (n & (n - 1)) == 0
 
 static int round_up(int x, int a) { return (x + a - 1) / a * a; }
 
+// Key of a run's noise stream: splitmix64's output function of the base seed.
+static unsigned long long noise_key(uint32_t seed) {
+    uint64_t z = (uint64_t)seed + 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
 // Bytes of a run's own device allocation: 8 row-space arrays (FP32 path) + 2 real
 // fields + k tables + partials + result slots + descriptor.
 static size_t run_state_bytes(int L, int M, int N, bool fp32) {
     const int Hp = round_up(M / 2 + 1, col_tile_width(L));
     const size_t rs = (size_t)L * Hp * sizeof(float2);
     const size_t real = (size_t)L * M * N * sizeof(float);
-    const size_t ktab = (size_t)(L + M + N) * sizeof(float);
+    const size_t ktab = (size_t)(L + M + N + 1) * sizeof(float);  // k-vectors + the step counter
     const size_t parts = (size_t)(2 * analysis_partials(L, M) + 4096) * sizeof(double);
     return (fp32 ? 8 * rs : 0) + 2 * real + round_up((int)ktab, 256) + parts + sizeof(RunDesc) + 1024;
 }
@@ -367,6 +375,9 @@ extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) {
     if (p->model == PFC_MODEL_MISFIT &&
         (p->grainx <= 0 || p->grainy <= 0 || p->grainz <= 0 || p->grainx > p->L || p->grainy > p->M || p->grainz > p->N))
         return set_error(PFC_E_INVALID, "grain counts must be in [1, grid extent]");
+    if (!(p->axx >= 0.0f)) return set_error(PFC_E_INVALID, "axx must be >= 0");
+    if (p->axx > 0.0f && p->model == PFC_MODEL_MISFIT && p->precision != PFC_PRECISION_FP32)
+        return set_error(PFC_E_INVALID, "stochastic noise (axx > 0) runs on the FP32 path only");
     Context *ctx = nullptr;
     int rc = get_context(p->device, &ctx);
     if (rc != PFC_OK) return rc;
@@ -397,7 +408,7 @@ extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) {
     const size_t real = (size_t)r->P * sizeof(float);
     const int nparts = analysis_partials(r->L, r->M);
     r->nparts = nparts;
-    const size_t ktab = (size_t)(r->L + r->M + r->N) * sizeof(float);
+    const size_t ktab = (size_t)(r->L + r->M + r->N + 1) * sizeof(float);
     const size_t parts = (size_t)(2 * nparts + 4096) * sizeof(double);
     const bool fp32 = p->precision == PFC_PRECISION_FP32;
     const size_t bytes = run_state_bytes(r->L, r->M, r->N, fp32);
@@ -426,6 +437,7 @@ extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) {
     d.krefl = kt;
     d.krefm = kt + r->L;
     r->d_krefn = kt + r->L + r->M;
+    d.step_ctr = (int *)(kt + r->L + r->M + r->N);
     d.partials = (double *)m;
     r->d_scratch = (double *)m + 2 * nparts;
     m += parts;
@@ -446,6 +458,9 @@ extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) {
     d.k = r->k;
     d.c2a = r->c2a;
     d.c2b = r->c2b;
+    // noise (MIS:490-491, 983-1014): amplitude dt * b0 in float, as the reference's product
+    d.noise_amp = (p->model == PFC_MODEL_MISFIT && r->b0 != 0.0f) ? p->dt * r->b0 : 0.0f;
+    d.noise_key = noise_key(p->seed);
     if (fp32) {
         cudaError_t ce = cudaMemcpyAsync(r->d_desc, &d, sizeof(RunDesc), cudaMemcpyHostToDevice, r->stream);
         if (ce != cudaSuccess) {
@@ -570,6 +585,9 @@ static int fp32_from_real(pfc_run *r, bool means_from_device) {
     d.psi_mean_f = (float)r->psi_mean;
     d.con_mean_f = (float)r->con_mean;
     PFC_CUDA_TRY(cudaMemcpyAsync(r->d_desc, &d, sizeof(RunDesc), cudaMemcpyHostToDevice, r->stream));
+    // the row kernel of step t advances the counter to t before the column kernel reads it
+    r->step_ctr_init = r->t - 1;
+    PFC_CUDA_TRY(cudaMemcpyAsync(d.step_ctr, &r->step_ctr_init, sizeof(int), cudaMemcpyHostToDevice, r->stream));
     PFC_CUDA_TRY(launch_row_forward(r->d_desc, 1, r->L, r->M, r->ctx->tw, r->stream));
     PFC_CUDA_TRY(launch_col_step(r->d_desc, 1, r->L, r->M, COL_PREPARE, r->ctx->tw, r->stream));
     PFC_CUDA_TRY(cudaStreamSynchronize(r->stream));

@@ -54,6 +54,7 @@ struct pfc_run {
     double *d_scratch = nullptr;
     double psi_mean = 0.0, con_mean = 0.0;
     int t = 0;
+    int step_ctr_init = -1;  // host staging of the device step counter
     bool fields_valid = false;
     bool energy_valid = false;
     pfc::Fp64State *f64 = nullptr;

@@ -57,6 +57,12 @@ struct RunDesc {
     double *partials;
     // batched runs only: slots of (energy sum, mass sum) that launch_reduce_runs fills
     double *ehist;
+    // stochastic noise (axx > 0): amplitude dt * b0 (0 = off), stream key, and the
+    // device step counter the row kernel advances once per step (the column kernel of
+    // step t reads t)
+    float noise_amp;
+    unsigned long long noise_key;
+    int *step_ctr;
 };
 
 // Twiddle tables exp(-2 pi i j / n) for n = 2^1 .. 2^11, FP32 and FP64.

@@ -830,7 +830,6 @@ extern "C" int pfc_submit(pfc_engine *e, const pfc_job *job, uint64_t *id) {
         p.model = job->kind;
         if (p.precision != PFC_PRECISION_FP32) return set_error(PFC_E_INVALID, "engine runs use the FP32 path");
         if (p.N != 1) return set_error(PFC_E_INVALID, "engine runs are 2-D (N = 1)");
-        if (p.axx != 0.0f) return set_error(PFC_E_INVALID, "stochastic noise (axx > 0) is not supported");
         if (job->steps <= 0 || job->mod <= 0) return set_error(PFC_E_INVALID, "steps and mod must be > 0");
         double b = 0.0;
         const int rc = pfc_run_bytes(&p, &b);

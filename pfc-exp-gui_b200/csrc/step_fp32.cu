@@ -222,6 +222,8 @@ __global__ void __launch_bounds__(RowCfg<M>::NT, 2) k_row_step(const RunDesc *__
     const RunDesc &d = runs[blockIdx.y];
     const int L = d.L;
     const int l0 = blockIdx.x * RPC;
+    // the noise stream's step index: advanced once per step, read by this step's column kernel
+    if (d.noise_amp != 0.0f && blockIdx.x == 0 && threadIdx.x == 0) *d.step_ctr += 1;
     float mp = 0.f, mc = 0.f;
     ROW_TILE_LOOP(RPC, H, NT, {
         float2 P = make_float2(0.f, 0.f), Cc = P, A = P, B = P;

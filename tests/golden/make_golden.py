@@ -47,6 +47,9 @@ CASES = [
     dict(name="misfit_128_s7", model="misfit", grid=(128, 128, 1),
          args=["--steps", "40", "--mod", "20", "--seed", "7", "--u0", "0.08", "--con0", "0.3"],
          keep=None, raw=[], elastic=[[]]),
+    # stochastic noise (Gauss + MAINEQUATIONC2_NOI, MIS:490-491, 951-1014)
+    dict(name="misfit_64_noise", model="misfit", grid=(64, 64, 1),
+         args=["--steps", "6", "--mod", "3", "--axx", "0.005", "--seed", "11"], keep=None, raw=[], elastic=[]),
     # CVD, 2-D and a small 3-D grid
     dict(name="cvd_64", model="cvd", grid=(64, 64, 1), args=["--steps", "21", "--mod", "10"],
          keep=None, raw=[], elastic=[]),

@@ -13,7 +13,7 @@ from helpers import (case_params, cvd_phimax_lines, cvd_phimax_txt_lines, energy
                      hist_lines, histq_lines, phimax_elastic_lines, phimax_misfit_lines, phiball_lines, q4q6_lines,
                      ql_lines, strain_lines)
 
-MISFIT_CASES = ["misfit_64", "misfit_128_s7", "misfit_256_c1"]
+MISFIT_CASES = ["misfit_64", "misfit_128_s7", "misfit_256_c1", "misfit_64_noise"]
 CVD_CASES = ["cvd_64", "cvd_32x32x8", "cvd_128"]
 
 
@@ -22,7 +22,7 @@ def oracle_params(meta, exact=1):
     L, M, N = meta["grid"]
     p = O.default_params(model, L=L, M=M, N=N, exact=exact)
     kv = case_params(meta)
-    for k in ("u0", "con0", "sig", "dt", "dx"):
+    for k in ("u0", "con0", "sig", "dt", "dx", "axx"):
         if k in kv:
             setattr(p, k, float(np.float32(kv[k])))
     if "seed" in kv:
