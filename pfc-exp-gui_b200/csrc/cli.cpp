@@ -25,6 +25,7 @@
 #include <filesystem>
 #include <fstream>
 #include <iostream>
+#include <iterator>
 #include <limits>
 #include <set>
 #include <string>
@@ -34,6 +35,7 @@
 #include "pfc_b200.h"
 #include "checkpoint.h"
 #include "pfc_engine.h"
+#include "sweep.h"
 
 namespace pfc {
 int phimax_misfit_dev(const float *d_phi, const float *d_con, int L, int M, float dx, float con0, double *d_out,
@@ -146,8 +148,37 @@ struct SimOpts {
     int grainx, grainy, grainz;
     int L = 256, M = 256, N = 1;
     int precision = PFC_PRECISION_FP32;
+    int resume = -1;  // --resume <kd>: continue from the run's own checkpoint kd
     std::string outdir;
 };
+
+// --resume <kd> (additive option): the state of checkpoint kd is read back from
+// phi_<kd>_0.vti / con_<kd>_0.vti in --outdir (the reference's own reader,
+// READPHIVTIN / READPHIVTIC at MIS:3019-3190, reads a fixed step only), and the run
+// continues with t_state steps taken.  The FP32 state is rebuilt from the Float32
+// files, so the continuation equals an uninterrupted run to within rounding; the
+// noise stream, counted by step, continues exactly.
+int resume_run(pfc_run *r, const SimOpts &o, int kd, int t_state) {
+    std::vector<float> f[2];
+    const char *pre[2] = {"phi_", "con_"};
+    for (int k = 0; k < 2; ++k) {
+        int l = 0, m = 0, n = 0;
+        const std::string path = opath(o.outdir, input_file("", pre[k], kd));
+        if (!read_vti(path, l, m, n, f[k])) {
+            cerr << "can't open input file: " << path << endl;
+            return 2;
+        }
+        if (l != o.L || m != o.M || n != o.N) {
+            cerr << "pfc-exp-cli: " << path << " holds a " << l << "x" << m << "x" << n << " grid, not " << o.L << "x"
+                 << o.M << "x" << o.N << endl;
+            return 2;
+        }
+    }
+    std::vector<double> phi(f[0].begin(), f[0].end()), con(f[1].begin(), f[1].end());
+    r->t = t_state;
+    if (pfc_run_set_fields(r, phi.data(), con.data()) != PFC_OK) return gpu_fail("resume");
+    return 0;
+}
 
 // ---------------------------------------------------------------------------
 // Misfit (MIS:17-309, 311-531)
@@ -168,6 +199,8 @@ void misfit_usage(const char *argv0) {
          << "  --grainz <int>      Initial grains in z (default: 1)\n"
          << "  --axx <float>       Noise base intensity (default: 0)\n"
          << "  --outdir <path>     Output directory (default: current dir)\n"
+         << "  --grid <LxMxN>      Grid (default: 256x256x1)\n"
+         << "  --resume <kd>       Continue from checkpoint kd in --outdir\n"
          << "  -h, --help          Show this help\n";
 }
 
@@ -272,6 +305,7 @@ int run_misfit_cli(int argc, char **argv) {
         else if (is("--axx")) bad = !parse_float(value("--axx"), o.axx);
         else if (is("--grid")) bad = !parse_grid(value("--grid"), o.L, o.M, o.N);
         else if (is("--precision")) bad = !parse_precision(value("--precision"), o.precision);
+        else if (is("--resume")) bad = !parse_int(value("--resume"), o.resume) || o.resume < 0;
         else if (is("--outdir")) {
             const char *v = value("--outdir");
             if (!v || *v == '\0') bad = true;
@@ -338,11 +372,13 @@ int run_misfit_cli(int argc, char **argv) {
             c << "b0 " << b0 << "\n";
         }
     }
-    std::ofstream log(opath(o.outdir, "checkpoint_timestamps.txt"), std::ios::out | std::ios::trunc);
-    if (log.is_open())
-        log << "# Checkpoint timestamps - Step number and milliseconds since epoch" << endl;
-    else
+    std::ofstream log(opath(o.outdir, "checkpoint_timestamps.txt"),
+                      std::ios::out | (o.resume >= 0 ? std::ios::app : std::ios::trunc));
+    if (log.is_open()) {
+        if (o.resume < 0) log << "# Checkpoint timestamps - Step number and milliseconds since epoch" << endl;
+    } else {
         cerr << "Warning: Failed to open checkpoint_timestamps.txt for writing" << endl;
+    }
 
     pfc_run_params p;
     pfc_default_params(PFC_MODEL_MISFIT, &p);
@@ -365,14 +401,19 @@ int run_misfit_cli(int argc, char **argv) {
     pfc_run *r = g.r;
     const long P = (long)L * M * N;
     std::vector<float> phi(P), con(P);
-    if (pfc_run_get_fields_f32(r, phi.data(), con.data()) != PFC_OK) return gpu_fail("initial fields");
-    if (!write_checkpoint_fields(o.outdir, 0, phi.data(), con.data(), L, M, N)) {
-        cerr << "pfc-exp-cli: failed to write checkpoint files" << endl;
-        return 2;
+    if (o.resume >= 0) {
+        const int rc = resume_run(r, o, o.resume, o.resume);
+        if (rc != 0) return rc;
+    } else {
+        if (pfc_run_get_fields_f32(r, phi.data(), con.data()) != PFC_OK) return gpu_fail("initial fields");
+        if (!write_checkpoint_fields(o.outdir, 0, phi.data(), con.data(), L, M, N)) {
+            cerr << "pfc-exp-cli: failed to write checkpoint files" << endl;
+            return 2;
+        }
     }
     DevScratch scratch;
     const int progress_every = std::max(1, o.steps / 200);
-    int t = 0;
+    int t = o.resume >= 0 ? o.resume : 0;
     while (t < o.steps) {
         // next step at which something is printed or written
         int next = t + 1;
@@ -422,6 +463,8 @@ void cvd_usage(const char *argv0) {
          << "  --mod <int>         Output/analysis interval (default: 200)\n"
          << "  --seed <uint>       Random seed base (default: 20200604)\n"
          << "  --outdir <path>     Output directory (default: current dir)\n"
+         << "  --grid <LxMxN>      Grid (default: 256x256x1)\n"
+         << "  --resume <kd>       Continue from checkpoint kd in --outdir\n"
          << "  -h, --help          Show this help\n";
 }
 
@@ -477,6 +520,7 @@ int run_cvd_cli(int argc, char **argv) {
         else if (is("--seed")) bad = !parse_uint(value("--seed"), o.seed);
         else if (is("--grid")) bad = !parse_grid(value("--grid"), o.L, o.M, o.N);
         else if (is("--precision")) bad = !parse_precision(value("--precision"), o.precision);
+        else if (is("--resume")) bad = !parse_int(value("--resume"), o.resume) || o.resume < 0;
         else if (is("--outdir")) {
             const char *v = value("--outdir");
             if (!v || *v == '\0') bad = true;
@@ -516,8 +560,9 @@ int run_cvd_cli(int argc, char **argv) {
             c << "N " << N << "\n";
         }
     }
-    std::ofstream log(opath(o.outdir, "checkpoint_timestamps.txt"), std::ios::out | std::ios::trunc);
-    if (log.is_open()) log << "# Checkpoint timestamps - Step number and milliseconds since epoch" << endl;
+    std::ofstream log(opath(o.outdir, "checkpoint_timestamps.txt"),
+                      std::ios::out | (o.resume >= 0 ? std::ios::app : std::ios::trunc));
+    if (log.is_open() && o.resume < 0) log << "# Checkpoint timestamps - Step number and milliseconds since epoch" << endl;
 
     pfc_run_params p;
     pfc_default_params(PFC_MODEL_CVD, &p);
@@ -537,7 +582,12 @@ int run_cvd_cli(int argc, char **argv) {
     const long P = (long)L * M * N;
     std::vector<float> phi(P), con(P);
     DevScratch phi_dev, scratch;
-    for (int t = 0; t < o.steps; t++) {
+    // CVD checkpoint kd holds the state after step kd + 1 (CVD:425)
+    if (o.resume >= 0) {
+        const int rc = resume_run(r, o, o.resume, o.resume + 1);
+        if (rc != 0) return rc;
+    }
+    for (int t = o.resume >= 0 ? o.resume + 1 : 0; t < o.steps; t++) {
         fprintf(stderr, "PFC_PROGRESS step=%d total=%d\n", t + 1, o.steps);
         fflush(stderr);
         // ENERGYC2 runs every step (CVD:442), so every step ends with the analysis
@@ -758,13 +808,112 @@ void global_usage(const char *argv0) {
          << "  misfit    Phase-field crystal with misfit strain (default)\n"
          << "  cvd       Controlled vapor deposition / two-phase growth\n"
          << "  elastic   Post-processing: elastic strain & crystallographic order\n\n"
-         << "Use --model <name> --help for model-specific options.\n";
+         << "Use --model <name> --help for model-specific options.\n"
+         << "--batch <file.json> runs a whole parameter sweep (Fixed / Range / List per parameter)\n"
+         << "on one GPU, each run in its own folder.\n";
 }
 
 }  // namespace
 
 // main_cli.cpp:24-88
+namespace {
+
+// A value as the GUI hands it to pfc-exp-cli: QString::number(v, 'g', 10) on the
+// command line (MainWindow.cpp:2402), read back with strtof.
+float as_cli_float(double v) {
+    char b[64];
+    snprintf(b, sizeof(b), "%.10g", v);
+    return strtof(b, nullptr);
+}
+
+// pfc-exp-cli --batch <file>: a whole GUI sweep (sweep.h) through the engine, each
+// run writing into its own folder what pfc-exp-cli would write there.  Progress lines
+// count finished runs.  Exit code 0 when every run finished, else 2.
+int run_batch_cli(const std::string &path) {
+    std::ifstream in(path);
+    if (!in.is_open()) {
+        cerr << "can't open batch file: " << path << endl;
+        return 2;
+    }
+    const std::string text((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+    sweep::SweepSpec sp;
+    std::string err;
+    if (!sweep::parse_sweep(text, sp, err)) {
+        cerr << "batch file " << path << ": " << err << endl;
+        return 2;
+    }
+    pfc_engine_opts eo{};
+    eo.hbm_budget_bytes = sp.budget_gb * 1e9;
+    eo.max_active = sp.max_active;
+    pfc_engine *eng = nullptr;
+    if (pfc_engine_create(&eo, &eng) != PFC_OK) return gpu_fail("engine");
+    const bool ela = sp.model == "elastic";
+    const int model = sp.model == "cvd" ? PFC_MODEL_CVD : PFC_MODEL_MISFIT;
+    int failed = 0, done = 0;
+    const int total = (int)sp.runs.size();
+    std::vector<uint64_t> ids;
+    for (const auto &r : sp.runs) {
+        std::string why;
+        if (!make_dir(r.out_dir, &why)) {
+            cerr << "Failed to create --outdir '" << r.out_dir << "': " << why << endl;
+            ++failed;
+            continue;
+        }
+        {
+            std::ofstream pj(opath(r.out_dir, "params.json"), std::ios::out | std::ios::trunc);
+            pj << sweep::params_json(sp, r);
+        }
+        pfc_job j{};
+        pfc_default_params(model, &j.params);
+        j.params.L = sp.L;
+        j.params.M = sp.M;
+        j.params.N = sp.N;
+        j.params.u0 = as_cli_float(r.u0);
+        j.params.con0 = as_cli_float(r.con0);
+        j.params.sig = as_cli_float(r.sig);
+        j.params.dt = as_cli_float(r.dt);
+        j.params.dx = as_cli_float(r.dx);
+        j.params.seed = r.seed;
+        j.kind = ela ? PFC_JOB_ELASTIC : model;
+        j.steps = r.steps;
+        j.mod = r.mod;
+        j.outdir = r.out_dir.c_str();
+        j.input_dir = ela ? sp.input_dir.c_str() : nullptr;
+        j.benchel = as_cli_float(r.benchel);
+        uint64_t id = 0;
+        if (pfc_submit(eng, &j, &id) != PFC_OK) {
+            cerr << "run " << r.index << ": " << pfc_last_error() << endl;
+            ++failed;
+            continue;
+        }
+        ids.push_back(id);
+    }
+    std::vector<pfc_event> ev(64);
+    size_t finished = 0;
+    while (finished < ids.size()) {
+        int n = 0;
+        if (pfc_wait(eng, ev.data(), (int)ev.size(), &n, 1000) != PFC_OK) break;
+        for (int i = 0; i < n; ++i) {
+            const pfc_event &e = ev[i];
+            if (e.type != PFC_EV_DONE && e.type != PFC_EV_FAILED && e.type != PFC_EV_CANCELLED) continue;
+            ++finished;
+            if (e.type == PFC_EV_DONE) ++done;
+            else ++failed;
+            cout << "PFC_PROGRESS step=" << done + failed << " total=" << total << endl;
+        }
+    }
+    pfc_engine_destroy(eng);
+    cerr << "batch: " << done << " of " << total << " runs finished" << (failed ? ", some failed" : "") << endl;
+    return failed == 0 && done == total ? 0 : 2;
+}
+
+}  // namespace
+
 extern "C" int pfc_run_cli(int argc, char **argv) {
+    for (int i = 1; i + 1 < argc; ++i)
+        if (argv[i] && std::string_view(argv[i]) == "--batch") return run_batch_cli(argv[i + 1]);
+    for (int i = 1; i < argc; ++i)
+        if (argv[i] && std::string_view(argv[i]).substr(0, 8) == "--batch=") return run_batch_cli(argv[i] + 8);
     std::string model = "misfit";
     std::vector<char *> nv;
     nv.push_back(argc > 0 ? argv[0] : (char *)"pfc-exp-cli");

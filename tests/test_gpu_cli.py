@@ -189,3 +189,78 @@ def test_cli_fp64_precision_3d(tmp_path):
         vals, _, _ = read_vti(out / f"phi_{kd}_0.vti")
         assert np.abs(vals - fields[f"phi_{kd}"]).max() <= 1e-6
     check_cvd_analysis_files(out, d, (0, 5, 10), 1e-5)
+
+
+def test_cli_batch_file_errors(tmp_path):
+    """--batch: a malformed or incomplete sweep file is reported before any GPU work."""
+    bad = tmp_path / "bad.json"
+    bad.write_text('{"model": "misfit", "params": {"u0": {"range": [0.1, 0.05, 0.01]}}, "out_dir": "x"}')
+    r = run_cli(["--batch", str(bad)])
+    assert r.returncode == 2 and "End must be >= start." in r.stderr
+    bad.write_text('{"model": "misfit", "params": {"u0": 0.1}')
+    r = run_cli(["--batch", str(bad)])
+    assert r.returncode == 2 and "batch file" in r.stderr
+    bad.write_text('{"model": "misfit", "params": {"nope": 1}, "out_dir": "x"}')
+    r = run_cli(["--batch", str(bad)])
+    assert r.returncode == 2 and "unknown parameter nope" in r.stderr
+    r = run_cli(["--batch", str(tmp_path / "missing.json")])
+    assert r.returncode == 2 and "can't open batch file" in r.stderr
+
+
+@pytest.mark.gpu
+def test_cli_batch_sweep_equals_single_runs(tmp_path):
+    """A 2 x 2 sweep (u0 list x seed range) through the engine: runs in the GUI's
+    odometer order (last parameter fastest), each folder with params.json and the same
+    files pfc-exp-cli writes for that run alone."""
+    import json
+    root = tmp_path / "exp"
+    spec = {"model": "misfit", "out_dir": str(root), "grid": [64, 64, 1],
+            "params": {"u0": {"list": [0.05, 0.08]}, "steps": 20, "mod": 10, "seed": {"range": [3, 4, 1]}}}
+    f = tmp_path / "sweep.json"
+    f.write_text(json.dumps(spec))
+    r = run_cli(["--batch", str(f)])
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.count("PFC_PROGRESS") == 4 and "step=4 total=4" in r.stdout
+    runs = sorted(os.listdir(root))
+    assert runs == ["run_0001", "run_0002", "run_0003", "run_0004"]
+    order = [(0.05, 3), (0.05, 4), (0.08, 3), (0.08, 4)]
+    for name, (u0, seed) in zip(runs, order):
+        pj = json.load(open(root / name / "params.json"))
+        assert pj["mode"] == "experiment" and pj["run_total"] == 4 and pj["out_dir"] == str(root / name)
+        assert pj["params"]["u0"] == u0 and pj["params"]["seed"] == seed and pj["params"]["model"] == "misfit"
+    single = tmp_path / "single"
+    r = run_cli(["--model", "misfit", "--grid", "64x64x1", "--u0", "0.08", "--seed", "4", "--steps", "20",
+                 "--mod", "10", "--outdir", str(single)])
+    assert r.returncode == 0
+    names = sorted(n for n in os.listdir(single) if n != "checkpoint_timestamps.txt")
+    assert names == sorted(n for n in os.listdir(root / "run_0004") if n not in ("checkpoint_timestamps.txt",
+                                                                               "params.json"))
+    for n in names:
+        assert (single / n).read_bytes() == (root / "run_0004" / n).read_bytes(), n
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("model", ["misfit", "cvd"])
+def test_cli_resume_continues_a_run(tmp_path, model):
+    """--resume <kd>: continue from the run's own checkpoint files.  The FP32 state is
+    rebuilt from Float32 fields, so the continuation matches the uninterrupted run to
+    within rounding (1e-5 after 20 more steps)."""
+    full, part = tmp_path / "full", tmp_path / "part"
+    kd = 20 if model == "misfit" else 10
+    base = ["--model", model, "--grid", "64x64x1", "--mod", "10", "--seed", "5"]
+    assert run_cli([*base, "--steps", "40", "--outdir", str(full)]).returncode == 0
+    # the first leg ends at checkpoint kd (CVD's checkpoint kd follows step kd + 1)
+    first = kd if model == "misfit" else kd + 1
+    assert run_cli([*base, "--steps", str(first), "--outdir", str(part)]).returncode == 0
+    r = run_cli([*base, "--steps", "40", "--resume", str(kd), "--outdir", str(part)])
+    assert r.returncode == 0, r.stderr
+    last = 40 if model == "misfit" else 30
+    a, _, _ = read_vti(full / f"phi_{last}_0.vti")
+    b, _, _ = read_vti(part / f"phi_{last}_0.vti")
+    assert np.abs(a - b).max() <= 1e-5
+    kds = [int(l.split()[0]) for l in (part / "energy.txt").read_text().splitlines()]
+    full_kds = [int(l.split()[0]) for l in (full / "energy.txt").read_text().splitlines()]
+    # the first leg's energy lines, then the continuation's: the same steps as one run
+    assert kds == full_kds
+    r = run_cli([*base, "--steps", "40", "--resume", "7", "--outdir", str(part)])
+    assert r.returncode == 2 and "can't open input file" in r.stderr
