@@ -184,7 +184,7 @@ int pfc_run_cli(int argc, char **argv);
 /* ------------------------------------------------------------------------------
  * Engine: many Misfit / CVD runs and Elastic analyses on one GPU, submitted and
  * polled from any thread.  It replaces the GUI's one-process-per-run queue
- * (src/gui/mainwindow.cpp:3453-3522 starts pfc-exp-cli once per parameter set) and
+ * (src/gui/MainWindow.cpp:3453-3522 starts pfc-exp-cli once per parameter set) and
  * has no direct counterpart in the reference.  Runs whose memory fits the HBM
  * budget are admitted in submission order and advanced together (continuous
  * batching: runs join and leave between scheduling quanta); each run's kernels

@@ -2,7 +2,7 @@
 // thread, admitted by device-memory budget and advanced together on one GPU.
 //
 // The reference runs one pfc-exp-cli process per parameter set, one after the other
-// (src/gui/mainwindow.cpp:3453-3522, the sweep queue built at mainwindow.cpp:2632-2770).
+// (src/gui/MainWindow.cpp:3453-3522, the sweep queue built at MainWindow.cpp:2632-2770).
 // Here one scheduler thread owns the GPU:
 //   * admission: queued jobs are admitted in submission order while their device bytes
 //     (pfc_run_bytes) fit the budget and the active-run limit; a job that does not fit
