@@ -1,19 +1,22 @@
 // col_kernel.cuh -- the column kernel of the fused FP32 step (included by step_fp32.cu).
 //
-// One CTA per tile of L rows x C packed columns of one run (a contiguous block of
-// the row-space layout).  For phi and then con:
-//   the field's tile is copied HBM -> parked buffer P (float4, coalesced) and
-//     transformed forward in place (scratch s for the intermediate stages),
-//   its nonlinear term's tile is copied HBM -> s and transformed forward in place,
+// Work item: a tile of L rows x C packed columns of one run (a contiguous block of
+// the row-space layout).  CTAs are persistent and take items in turn.  For phi and
+// then con:
+//   the field's tile is transformed forward into the parked buffer P,
+//   its nonlinear term's tile is transformed forward in place in the scratch s,
 //   the semi-implicit update runs in place in P (MAINEQUATIONC2_NOI / C2MIX,
 //     MIS:983-1014, CVD:865-886) with the FP64-built factors of the shared
-//     coefficient table,
+//     coefficient table (and the noise term when axx > 0),
 //   each output is an inverse transform whose first stage reads P through a
 //     multiplier (1, C2A, C2B for phi, MIS:807-810; 1 and the -i k gradients for
 //     con at checkpoints, MIS:884-889) into s, copied s -> HBM (float4).
-// Staging the tiles through shared memory keeps every transform shared-memory to
-// shared-memory, which fits 80 registers per thread without spills: three CTAs of
-// 256 threads (3 x 69 KB of shared memory) per SM.
+// Inputs arrive by asynchronous 16-byte copies (cp.async) into an unpadded staging
+// buffer Q, which a transform's first stage reads directly.  Each load is issued as
+// soon as the previous transform's first stage has consumed Q, so it streams in
+// while that transform, the update and the output transforms run; the next item's
+// phi tile streams in during the current item's con work.  Two CTAs of 256 threads
+// per SM (2 x 100 KB of shared memory, 128 registers).
 
 // multiplier applied by an inverse transform's first stage: P * g(l, km)
 struct ScaleByTable {
@@ -71,16 +74,29 @@ __device__ float2 noise_mode(unsigned long long key, int t, int l, int km, int L
     return make_float2(s * rad * cs, conj ? -s * rad * sn : s * rad * sn);
 }
 
-template <int L, int C, int NT> __device__ __forceinline__ void tile_in(const float2 *__restrict__ g, float2 *sm) {
-    __syncthreads();
-    const float4 *g4 = reinterpret_cast<const float4 *>(g);
-    for (int i = threadIdx.x; i < L * C / 2; i += NT) {
-        const float4 v = g4[i];
-        sm[spad(2 * i)] = make_float2(v.x, v.y);
-        sm[spad(2 * i + 1)] = make_float2(v.z, v.w);
-    }
+// Asynchronous copy of one tile (L*C float2, 16-byte aligned) into the staging buffer q:
+// 16 bytes per instruction, tracked per thread by a commit group.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src) : "memory");
+}
+template <int L, int C, int NT> __device__ __forceinline__ void tile_prefetch(const float2 *__restrict__ g, float2 *q) {
+    for (int i = threadIdx.x; i < L * C / 2; i += NT) cp_async16(q + 2 * i, g + 2 * i);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+// this thread's copies have landed; the barrier makes every thread's visible
+__device__ __forceinline__ void tile_wait() {
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
 }
+template <int L, int C, int NT> struct Prefetch {
+    const float2 *src;
+    float2 *q;
+    __device__ __forceinline__ void operator()() const {
+        if (src) tile_prefetch<L, C, NT>(src, q);
+    }
+};
+
 template <int L, int C, int NT> __device__ __forceinline__ void tile_out(const float2 *sm, float2 *__restrict__ g) {
     float4 *g4 = reinterpret_cast<float4 *>(g);
     for (int i = threadIdx.x; i < L * C / 2; i += NT) {
@@ -90,91 +106,105 @@ template <int L, int C, int NT> __device__ __forceinline__ void tile_out(const f
 }
 
 template <int L, int MODE>
-__global__ void __launch_bounds__(ColCfg<L>::NT, 3) k_col_step(const RunDesc *__restrict__ runs,
+__global__ void __launch_bounds__(ColCfg<L>::NT, 2) k_col_step(const RunDesc *__restrict__ runs, int nruns,
                                                                 const float2 *__restrict__ tw) {
     constexpr int C = ColCfg<L>::C, NT = ColCfg<L>::NT;
     constexpr int SPAD = padded_len<C * L>::value;
     typedef RegOut<L, C, NT> RO;  // register scratch the transforms need for their last stage
-    extern __shared__ float2 smem[];
-    float2 *s = smem;          // FFT scratch
-    float2 *Pk = smem + SPAD;  // parked spectrum
-    const RunDesc &d = runs[blockIdx.y];
-    const int H = d.M / 2;
-    const long tile = (long)blockIdx.x * L * C;
-    const int km0 = blockIdx.x * C;
-    const float invL = 1.0f / (float)L;
-    const float mn_dt = d.k.dynamic_mn * d.dt, mc_dt = d.k.dynamic_mc * d.dt;
+    extern __shared__ __align__(16) float2 smem[];
+    float2 *s = smem;               // FFT scratch
+    float2 *Pk = smem + SPAD;       // parked spectrum
+    float2 *Q = smem + 2 * SPAD;    // staging buffer (16-byte aligned: 2*SPAD float2)
+    const int T = runs[0].T;        // all runs of a launch share L and M
+    const int items = nruns * T;
     float2 b[RO::PER_T][RO::R];
+    int item = blockIdx.x;
+    if (item >= items) return;
+    auto tile_of = [&](int it) { return (long)(it % T) * L * C; };
+    tile_prefetch<L, C, NT>(runs[item / T].psi + tile_of(item), Q);
+    for (; item < items; item += gridDim.x) {
+        const RunDesc &d = runs[item / T];
+        const int H = d.M / 2;
+        const long tile = tile_of(item);
+        const int km0 = (item % T) * C;
+        const int next = item + gridDim.x;
+        const float2 *next_psi = next < items ? runs[next / T].psi + tile_of(next) : nullptr;
+        const float invL = 1.0f / (float)L;
+        const float mn_dt = d.k.dynamic_mn * d.dt, mc_dt = d.k.dynamic_mc * d.dt;
 
-    // ---- phi ----
-    tile_in<L, C, NT>(d.psi + tile, Pk);
-    fft<L, C, NT, true, SP_SMEM, SP_SMEM>(Pk, s, Pk, tw, b);
-    if (MODE != COL_PREPARE) {
-        tile_in<L, C, NT>(d.inn + tile, s);
-        fft<L, C, NT, true, SP_SMEM, SP_SMEM>(s, s, s, tw, b);
-    }
-    const int nstep = (MODE != COL_PREPARE && d.noise_amp != 0.0f) ? *d.step_ctr : -1;
-    for (int e = threadIdx.x; e < L * C; e += NT) {
-        const int l = e / C, c = e % C, km = km0 + c;
-        const int pi = spad(e);
-        float2 v = Pk[pi];
-        if (MODE != COL_PREPARE) {
-            // (psi^ - Mn dt k^2 N^ [+ dt b0 xi^ |k| lowpass]) / (1 + Mn dt k^2) / L; the
-            // FP64-built factor is 0 at k = 0
-            const float kl = d.krefl[l], kmv = d.krefm[km <= H ? km : 0];
-            const float ks = kl * kl + kmv * kmv;
-            const float an = mn_dt * ks;
-            const float2 nh = s[pi];
-            const float f = d.kden[tile + e].x;
-            float rx = v.x - an * nh.x, ry = v.y - an * nh.y;
-            if (nstep >= 0 && km <= H) {
-                // MAINEQUATIONC2_NOI's noise term (MIS:1002-1003), lowpass at |k| = 2 pi
-                const float2 xi = noise_mode(d.noise_key, nstep, l, km, L, d.M);
-                const float sk = sqrtf(ks);
-                const float w = d.noise_amp * sk * (0.5f - 0.5f * tanhf((sk - 6.2831852f) / 0.1f));
-                rx += w * xi.x;
-                ry += w * xi.y;
-            }
-            v = make_float2(rx * f, ry * f);
+        // ---- phi ----
+        tile_wait();
+        if (MODE == COL_PREPARE) {
+            fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, Pk, tw, b, Identity(), Prefetch<L, C, NT>{next_psi, Q});
         } else {
-            v = (l == 0 && km == 0) ? make_float2(0.f, 0.f) : cscale(v, invL);
+            fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, Pk, tw, b, Identity(), Prefetch<L, C, NT>{d.inn + tile, Q});
+            tile_wait();
+            fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, s, tw, b, Identity(), Prefetch<L, C, NT>{d.con + tile, Q});
         }
-        Pk[pi] = v;
-    }
-    __syncthreads();
-    if (MODE != COL_PREPARE) {
-        fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b);
-        tile_out<L, C, NT>(s, d.psi + tile);
-    }
-    fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, ScaleByTable{d.kc2 + tile, C, 0});
-    tile_out<L, C, NT>(s, d.ca + tile);
-    fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, ScaleByTable{d.kc2 + tile, C, 1});
-    tile_out<L, C, NT>(s, d.cb + tile);
-    if (MODE == COL_PREPARE) return;
+        const int nstep = (MODE != COL_PREPARE && d.noise_amp != 0.0f) ? *d.step_ctr : -1;
+        for (int e = threadIdx.x; e < L * C; e += NT) {
+            const int l = e / C, c = e % C, km = km0 + c;
+            const int pi = spad(e);
+            float2 v = Pk[pi];
+            if (MODE != COL_PREPARE) {
+                // (psi^ - Mn dt k^2 N^ [+ dt b0 xi^ |k| lowpass]) / (1 + Mn dt k^2) / L; the
+                // FP64-built factor is 0 at k = 0
+                const float kl = d.krefl[l], kmv = d.krefm[km <= H ? km : 0];
+                const float ks = kl * kl + kmv * kmv;
+                const float an = mn_dt * ks;
+                const float2 nh = s[pi];
+                const float f = d.kden[tile + e].x;
+                float rx = v.x - an * nh.x, ry = v.y - an * nh.y;
+                if (nstep >= 0 && km <= H) {
+                    // MAINEQUATIONC2_NOI's noise term (MIS:1002-1003), lowpass at |k| = 2 pi
+                    const float2 xi = noise_mode(d.noise_key, nstep, l, km, L, d.M);
+                    const float sk = sqrtf(ks);
+                    const float w = d.noise_amp * sk * (0.5f - 0.5f * tanhf((sk - 6.2831852f) / 0.1f));
+                    rx += w * xi.x;
+                    ry += w * xi.y;
+                }
+                v = make_float2(rx * f, ry * f);
+            } else {
+                v = (l == 0 && km == 0) ? make_float2(0.f, 0.f) : cscale(v, invL);
+            }
+            Pk[pi] = v;
+        }
+        __syncthreads();
+        if (MODE != COL_PREPARE) {
+            fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b);
+            tile_out<L, C, NT>(s, d.psi + tile);
+        }
+        fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, ScaleByTable{d.kc2 + tile, C, 0});
+        tile_out<L, C, NT>(s, d.ca + tile);
+        fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, ScaleByTable{d.kc2 + tile, C, 1});
+        tile_out<L, C, NT>(s, d.cb + tile);
+        if (MODE == COL_PREPARE) continue;
 
-    // ---- con ----
-    tile_in<L, C, NT>(d.con + tile, Pk);
-    fft<L, C, NT, true, SP_SMEM, SP_SMEM>(Pk, s, Pk, tw, b);
-    tile_in<L, C, NT>(d.inc + tile, s);
-    fft<L, C, NT, true, SP_SMEM, SP_SMEM>(s, s, s, tw, b);
-    for (int e = threadIdx.x; e < L * C; e += NT) {
-        const int l = e / C, c = e % C, km = km0 + c;
-        const int pi = spad(e);
-        // (c^ - Mc dt k^2 I^) / (1 + Mc dt alpha k^4) / L; the FP64-built factor is 0 at k = 0
-        const float kl = d.krefl[l], kmv = d.krefm[km <= H ? km : 0];
-        const float ac = mc_dt * (kl * kl + kmv * kmv);
-        const float f = d.kden[tile + e].y;
-        const float2 ih = s[pi];
-        const float2 v = Pk[pi];
-        Pk[pi] = make_float2((v.x - ac * ih.x) * f, (v.y - ac * ih.y) * f);
+        // ---- con ----
+        tile_wait();
+        fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, Pk, tw, b, Identity(), Prefetch<L, C, NT>{d.inc + tile, Q});
+        tile_wait();
+        fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, s, tw, b, Identity(), Prefetch<L, C, NT>{next_psi, Q});
+        for (int e = threadIdx.x; e < L * C; e += NT) {
+            const int l = e / C, c = e % C, km = km0 + c;
+            const int pi = spad(e);
+            // (c^ - Mc dt k^2 I^) / (1 + Mc dt alpha k^4) / L; the FP64-built factor is 0 at k = 0
+            const float kl = d.krefl[l], kmv = d.krefm[km <= H ? km : 0];
+            const float ac = mc_dt * (kl * kl + kmv * kmv);
+            const float f = d.kden[tile + e].y;
+            const float2 ih = s[pi];
+            const float2 v = Pk[pi];
+            Pk[pi] = make_float2((v.x - ac * ih.x) * f, (v.y - ac * ih.y) * f);
+        }
+        __syncthreads();
+        fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b);
+        tile_out<L, C, NT>(s, d.con + tile);
+        if (MODE == COL_STEP_CHECKPOINT) {
+            fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, GradientOf{d.krefl, d.krefm, km0, H, 0});
+            tile_out<L, C, NT>(s, d.gx + tile);
+            fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, GradientOf{d.krefl, d.krefm, km0, H, 1});
+            tile_out<L, C, NT>(s, d.gy + tile);
+        }
     }
-    __syncthreads();
-    fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b);
-    tile_out<L, C, NT>(s, d.con + tile);
-    if (MODE == COL_STEP_CHECKPOINT) {
-        fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, GradientOf{d.krefl, d.krefm, km0, H, 0});
-        tile_out<L, C, NT>(s, d.gx + tile);
-        fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, GradientOf{d.krefl, d.krefm, km0, H, 1});
-        tile_out<L, C, NT>(s, d.gy + tile);
-    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");  // no copy outlives the CTA
 }

@@ -23,6 +23,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace pfc {
 
 // ---------------------------------------------------------------------------
@@ -330,27 +332,41 @@ __device__ __forceinline__ void middle_stages(C *s, const C *__restrict__ tw,
     }
 }
 
+// Work a transform runs right after its first stage (the first stage ends with a
+// barrier, so `src` is free then): e.g. start loading the next input into it.
+struct NoHook {
+    __device__ __forceinline__ void operator()() const {}
+};
+
 // Full transform of NB interleaved length-N sequences.
-//   IN  = SP_GLOBAL: the first stage reads global `src`; SP_SMEM: reads the padded
-//         shared array `src` (which may be `s` itself or another buffer).  Every
-//         value it loads passes through xf(e, b, v).
+//   IN  = SP_GLOBAL: the first stage reads the unpadded array `src` (global memory,
+//         or a shared staging buffer); SP_SMEM: reads the padded shared array `src`
+//         (which may be `s` itself or another buffer).  Every value it loads passes
+//         through xf(e, b, v).
 //   OUT = SP_GLOBAL: the last stage writes global `dst`; SP_SMEM: writes the padded
 //         shared array `dst`; SP_REGS: the output stays in `last` (RegOut layout).
-// Intermediate stages run in place in the padded shared scratch `s`.  Callers must
-// __syncthreads() before a transform that reads shared data they wrote; a
-// transform whose last stage writes shared memory synchronises before returning.
-template <int N, int NB, int NT, bool FWD, int IN, int OUT, typename C, typename XF = Identity>
+// Intermediate stages run in place in the padded shared scratch `s`; after the first
+// stage af() runs.  Callers must __syncthreads() before a transform that reads
+// shared data they wrote; a transform whose last stage writes shared memory
+// synchronises before returning.
+template <int N, int NB, int NT, bool FWD, int IN, int OUT, typename C, typename XF = Identity, typename AF = NoHook>
 __device__ __forceinline__ void fft(const typename nodeduce<C>::type *src, C *s, typename nodeduce<C>::type *dst,
                                     const C *__restrict__ tw,
-                                    C (&last)[RegOut<N, NB, NT>::PER_T][RegOut<N, NB, NT>::R], XF xf = XF()) {
+                                    C (&last)[RegOut<N, NB, NT>::PER_T][RegOut<N, NB, NT>::R], XF xf = XF(),
+                                    AF af = AF()) {
     typedef radix_plan<N> P;
     if constexpr (P::stages == 1) {
         stage<N, NB, NT, P::last_radix, 1, FWD, IN, OUT>(src, dst, tw, last, xf);
+        if constexpr (!std::is_same<AF, NoHook>::value) {
+            __syncthreads();  // every thread has read src
+            af();
+        }
     } else {
         typedef StageShape<N, NB, NT, 16> S16;
         C v[S16::PER_T][16];
         // first stage (radix 16): src -> scratch
         stage<N, NB, NT, 16, 1, FWD, IN, SP_SMEM>(src, s, tw, v, xf);
+        af();
         middle_stages<N, NB, NT, 16, RegOut<N, NB, NT>::NS, FWD>(s, tw, v);
         // last stage: scratch -> dst / registers
         stage<N, NB, NT, P::last_radix, RegOut<N, NB, NT>::NS, FWD, SP_SMEM, OUT>(s, dst, tw, last);

@@ -498,17 +498,31 @@ static cudaError_t row_analysis_impl(const RunDesc *d_runs, int nruns, int L, co
     return cudaGetLastError();
 }
 
+// Streaming multiprocessors of the current device (the persistent grid's width).
+static int sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!cached[dev]) {
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        cached[dev] = n > 0 ? n : 148;
+    }
+    return cached[dev];
+}
+
 template <int L, int MODE>
 static cudaError_t col_impl(const RunDesc *d_runs, int nruns, int M, const TwiddleSet &tw, cudaStream_t st) {
     constexpr int C = ColCfg<L>::C, NT = ColCfg<L>::NT;
-    constexpr size_t smem = 2 * smem_bytes<C * L>();
+    constexpr size_t smem = 2 * smem_bytes<C * L>() + sizeof(float2) * C * L;  // s, P (padded) and Q
     static unsigned mask = 0;
     cudaError_t e = set_smem(k_col_step<L, MODE>, smem, mask);
     if (nruns == 0) return e;
     if (e != cudaSuccess) return e;
     const int H = M / 2;
-    dim3 grid((H + 1 + C - 1) / C, nruns);
-    k_col_step<L, MODE><<<grid, NT, smem, st>>>(d_runs, tw.f32[log2i(L)]);
+    const int items = ((H + 1 + C - 1) / C) * nruns;
+    const int grid = items < 2 * sm_count() ? items : 2 * sm_count();
+    k_col_step<L, MODE><<<grid, NT, smem, st>>>(d_runs, nruns, tw.f32[log2i(L)]);
     return cudaGetLastError();
 }
 
