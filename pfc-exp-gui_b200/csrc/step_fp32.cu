@@ -24,6 +24,7 @@
 // kernel reads 4 and writes 4; a row-space array is 4 bytes per grid point, so one
 // step moves 56 bytes per point.
 #include "fft_core.cuh"
+#include "tile_io.cuh"
 #include "pfc_internal.h"
 
 namespace pfc {
