@@ -90,6 +90,9 @@ cudaError_t launch_build_kcoef(const RunDesc *d_run, float2 *kden, float2 *kc2, 
 // column-kernel modes
 enum ColMode : int { COL_STEP = 0, COL_PREPARE = 1, COL_STEP_CHECKPOINT = 2 };
 
+// Kernel attribute setup (before graph capture) of the row kernels of row length M.
+cudaError_t prepare_rows(int M);
+
 // Number of partial-sum slots the analysis kernel writes per run (2 doubles each).
 int analysis_partials(int L, int M);
 // Column-tile width of the row-space layout for a grid with L rows.

@@ -23,24 +23,16 @@
 // Compulsory HBM traffic: row kernel reads 4 and writes 2 row-space arrays, column
 // kernel reads 4 and writes 4; a row-space array is 4 bytes per grid point, so one
 // step moves 56 bytes per point.
-#include "fft_core.cuh"
-#include "tile_io.cuh"
-#include "pfc_internal.h"
+#include "step_common.cuh"
 
 namespace pfc {
 
 constexpr int ROW_TILE = 8192;  // complex elements per row-kernel CTA (64 KB in FP32)
-constexpr int COL_TILE = 4096;  // complex elements per column-kernel tile (32 KB in FP32)
 
 template <int M> struct RowCfg {
     static constexpr int RPC = (ROW_TILE / 2) / M >= 1 ? (ROW_TILE / 2) / M : 1;  // rows per CTA
     static constexpr int NB = 2 * RPC;
     static constexpr int NT = (NB * M / 16) < 512 ? (NB * M / 16) : 512;
-};
-
-template <int L> struct ColCfg {
-    static constexpr int C = (COL_TILE / L) > 16 ? 16 : (COL_TILE / L);  // packed columns per tile
-    static constexpr int NT = (C * L / 16) < 32 ? 32 : (C * L / 16);
 };
 
 int col_tile_width(int L) {
@@ -50,18 +42,6 @@ int col_tile_width(int L) {
 
 __device__ __forceinline__ long rs_index(const RunDesc &d, int l, int km) {
     return ((long)(km >> d.lct) * d.L + l) * d.CT + (km & (d.CT - 1));
-}
-
-// C2 correlation kernel at |k| = sqrtf(ks), as the reference builds its float table
-// (misfit_uniform_time_seed_fftw_early.cpp:700-750): exp in double of float arguments.
-__device__ __forceinline__ float c2_ref(const C2Params &p, float ks) {
-    const float s = __fsqrt_rn(ks);
-    if (s <= p.kc) {
-        const double d = (double)__fsub_rn(s, p.k1);
-        return (float)(exp(-(double)p.q1 * (double)p.q1) * exp(-(d * d) / (double)p.gg1));
-    }
-    const double d = (double)__fsub_rn(s, p.k2);
-    return (float)(exp(-(double)p.q2 * (double)p.q2) * exp(-(d * d) / (double)p.gg2));
 }
 
 // Per k-point coefficients of one run (RunDesc::kcoef), built once in FP64 and rounded.
@@ -438,27 +418,6 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_analysis(const RunDesc *_
 // ---------------------------------------------------------------------------
 // Launchers
 // ---------------------------------------------------------------------------
-static int log2i(int n) {
-    int l = 0;
-    while ((1 << l) < n) ++l;
-    return l;
-}
-
-// Opt in to more than 48 KB of dynamic shared memory, once per kernel and device
-// (the attribute call is not a stream operation, so it is also done before any
-// graph capture through prepare_size()).
-template <typename K> static cudaError_t set_smem(K kernel, size_t bytes, unsigned &mask) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    if (mask & (1u << dev)) return cudaSuccess;
-    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e == cudaSuccess) mask |= 1u << dev;
-    return e;
-}
-
-template <int n> static constexpr size_t smem_bytes() { return sizeof(float2) * padded_len<n>::value; }
-
 template <int M>
 static cudaError_t row_step_impl(const RunDesc *d_runs, int nruns, int L, const TwiddleSet &tw, cudaStream_t st) {
     constexpr int RPC = RowCfg<M>::RPC, NT = RowCfg<M>::NT;
@@ -499,19 +458,6 @@ static cudaError_t row_analysis_impl(const RunDesc *d_runs, int nruns, int L, co
     return cudaGetLastError();
 }
 
-// Streaming multiprocessors of the current device (the persistent grid's width).
-static int sm_count() {
-    static int cached[64] = {0};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
-    if (!cached[dev]) {
-        int n = 0;
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        cached[dev] = n > 0 ? n : 148;
-    }
-    return cached[dev];
-}
-
 template <int L, int MODE>
 static cudaError_t col_impl(const RunDesc *d_runs, int nruns, int M, const TwiddleSet &tw, cudaStream_t st) {
     constexpr int C = ColCfg<L>::C, NT = ColCfg<L>::NT;
@@ -526,18 +472,6 @@ static cudaError_t col_impl(const RunDesc *d_runs, int nruns, int M, const Twidd
     k_col_step<L, MODE><<<grid, NT, smem, st>>>(d_runs, nruns, tw.f32[log2i(L)]);
     return cudaGetLastError();
 }
-
-#define PFC_SIZE_SWITCH(n, FN, ...)             \
-    switch (n) {                                \
-        case 32: return FN<32>(__VA_ARGS__);    \
-        case 64: return FN<64>(__VA_ARGS__);    \
-        case 128: return FN<128>(__VA_ARGS__);  \
-        case 256: return FN<256>(__VA_ARGS__);  \
-        case 512: return FN<512>(__VA_ARGS__);  \
-        case 1024: return FN<1024>(__VA_ARGS__); \
-        case 2048: return FN<2048>(__VA_ARGS__); \
-        default: return cudaErrorInvalidValue;  \
-    }
 
 cudaError_t launch_row_step(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw, cudaStream_t s) {
     PFC_SIZE_SWITCH(M, row_step_impl, d_runs, nruns, L, tw, s)
@@ -568,13 +502,19 @@ cudaError_t launch_col_step(const RunDesc *d_runs, int nruns, int L, int M, int 
     PFC_SIZE_SWITCH(L, col_dispatch, d_runs, nruns, M, mode, tw, s)
 }
 
-cudaError_t prepare_size(int L, int M) {
+cudaError_t prepare_rows(int M) {
     // nruns == 0: only the shared-memory attributes are set, nothing is launched
     TwiddleSet none{};
     cudaError_t e;
-    if ((e = launch_row_step(nullptr, 0, L, M, none, 0)) != cudaSuccess) return e;
-    if ((e = launch_row_forward(nullptr, 0, L, M, none, 0)) != cudaSuccess) return e;
-    if ((e = launch_row_analysis(nullptr, 0, L, M, none, 0)) != cudaSuccess) return e;
+    if ((e = launch_row_step(nullptr, 0, 0, M, none, 0)) != cudaSuccess) return e;
+    if ((e = launch_row_forward(nullptr, 0, 0, M, none, 0)) != cudaSuccess) return e;
+    return launch_row_analysis(nullptr, 0, 0, M, none, 0);
+}
+
+cudaError_t prepare_size(int L, int M) {
+    TwiddleSet none{};
+    cudaError_t e;
+    if ((e = prepare_rows(M)) != cudaSuccess) return e;
     for (int mode = 0; mode < 3; ++mode)
         if ((e = launch_col_step(nullptr, 0, L, M, mode, none, 0)) != cudaSuccess) return e;
     return cudaSuccess;

@@ -1,5 +1,6 @@
-// tile_io.cuh -- tile staging and transform multipliers shared by the column kernels
-// of the 2-D step (col_kernel.cuh) and the 3-D step (step3d.cu).
+// tile_io.cuh -- tile staging (cp.async into shared memory, float4 stores out) and the
+// multipliers an inverse transform's first stage applies, used by the column kernel
+// (col_kernel.cuh).
 #pragma once
 
 #include "fft_core.cuh"
