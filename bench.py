@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--no-sweep", action="store_true", help="skip the 64-run mixed-size sweep measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving (Poisson arrivals) measurement")
     ap.add_argument("--serve-requests", type=int, default=48)
+    ap.add_argument("--no-cvd3d", action="store_true", help="skip the 3-D CVD (256x256x64) step measurement")
     return ap.parse_args()
 
 
@@ -463,6 +464,23 @@ def run_ours(args):
                               "what": "one Misfit run, plain FP64 path (13 complex-double 3-D DFTs + pointwise "
                                       "kernels per step, reference roundings), CUDA events",
                               "batched_fp32_over_fp64_plain": round(value / dist.world / fp64_sps, 2)}
+    # the 3-D CVD workload (256 x 256 x 64): 3-D runs take the plain FP64 path
+    if not args.no_cvd3d:
+        r3 = P.Run(P.default_params(P.MODEL_CVD, L=256, M=256, N=64, device=dev, precision=P.FP64))
+        r3.advance(2)
+        n3 = 10
+        ms3 = r3.advance_timed(n3)
+        t0 = time.perf_counter()
+        for _ in range(3):  # the CLI's per-step pattern: one step, then ENERGYC2 for energy.txt
+            r3.advance(1)
+            r3.energy()
+        cli_ms = (time.perf_counter() - t0) / 3 * 1e3
+        r3.close()
+        line["cvd3d"] = {"workload": "CVD 256x256x64 (u0 0.01, con0 0.2, dt 0.05, dx 0.125), plain FP64 path",
+                         "ms_per_step": round(ms3 / n3, 4), "steps_per_s": round(n3 / (ms3 / 1000.0), 2),
+                         "cli_step_with_energy_ms": round(cli_ms, 3),
+                         "what": "pfc_run_advance_timed (CUDA events) of 10 steps; cli_step_with_energy_ms is wall "
+                                 "time of advance(1) + pfc_run_energy"}
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(G)

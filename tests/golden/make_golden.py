@@ -38,7 +38,7 @@ CASES = [
     # small Misfit run: every checkpoint kept, Elastic on all of them
     dict(name="misfit_64", model="misfit", grid=(64, 64, 1), args=["--steps", "50", "--mod", "25"],
          keep=None, raw=[25], elastic=[[], ["--benchel", "1.3"]]),
-    # C1: Misfit 256^2, 200 steps, checkpoint every 25; the last
+    # the plain CPU reference workload: Misfit 256^2, 200 steps, checkpoint every 25; the last
     # checkpoint's fields are kept, Elastic runs on it
     dict(name="misfit_256_c1", model="misfit", grid=(256, 256, 1),
          args=["--steps", "200", "--mod", "25", "--seed", "20200604", "--u0", "0.05", "--con0", "0.2"],
