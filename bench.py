@@ -33,7 +33,7 @@ METRIC = "PFC Misfit steps/s at 1024^2 (FP32 fused step, batched; run-steps/s)"
 UNIT = "steps/s"
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
@@ -47,39 +47,47 @@ def parse():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving (Poisson arrivals) measurement")
     ap.add_argument("--serve-requests", type=int, default=48)
     ap.add_argument("--no-cvd3d", action="store_true", help="skip the 3-D CVD (256x256x64) step measurement")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 # ---------------------------------------------------------------------------
 # distributed plumbing (torch.distributed over NCCL: barrier and max-over-ranks)
 # ---------------------------------------------------------------------------
 class Dist:
-    def __init__(self, n):
+    """One process per GPU (torchrun env); NCCL on GPUs, gloo on CPU-only hosts."""
+
+    def __init__(self, n, backend=None):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.dev = "cpu"
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            if backend is None:
+                backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+                self.dev = f"cuda:{self.local}"
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
             self.pg = dist
 
     def barrier(self):
         if self.pg:
             import torch
-            t = torch.zeros(1, device=f"cuda:{self.local}")
+            t = torch.zeros(1, device=self.dev)
             self.pg.all_reduce(t)
-            torch.cuda.synchronize()
+            if self.dev != "cpu":
+                torch.cuda.synchronize()
 
     def max(self, v: float) -> float:
         if not self.pg:
             return v
         import torch
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
+        t = torch.tensor([v], dtype=torch.float64, device=self.dev)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
@@ -87,7 +95,7 @@ class Dist:
         if not self.pg:
             return v
         import torch
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
+        t = torch.tensor([v], dtype=torch.float64, device=self.dev)
         self.pg.all_reduce(t)
         return float(t.item())
 
