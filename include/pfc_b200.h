@@ -46,11 +46,12 @@ extern "C" {
  * (misfit_uniform_time_seed_fftw_early.cpp:17-35, 125-143; cvd.cpp:111-125, 33-53). */
 typedef struct pfc_run_params {
     int model;      /* PFC_MODEL_MISFIT or PFC_MODEL_CVD */
-    int L, M, N;    /* grid; L, M powers of two in [32, 2048]; N = 1 (2-D) */
+    int L, M, N;    /* grid; L, M powers of two in [32, 2048]; N = 1 (2-D) on the FP32 path,
+                       a power of two <= 2048 on the FP64 paths (3-D CVD runs) */
     float u0, con0, sig, dt, dx, axx;
     int grainx, grainy, grainz; /* Misfit initial grains */
     uint32_t seed;
-    int precision;  /* PFC_PRECISION_FP32 or PFC_PRECISION_FP64 */
+    int precision;  /* PFC_PRECISION_FP32, PFC_PRECISION_FP64 or PFC_PRECISION_FP64_PURE */
     int device;     /* CUDA device ordinal */
 } pfc_run_params;
 
