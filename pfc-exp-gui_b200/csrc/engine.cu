@@ -7,6 +7,7 @@
 // src/experiment/cvd.cpp:26-53, 351-377.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -14,6 +15,7 @@
 #include <tuple>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "pfc_b200.h"
@@ -697,22 +699,86 @@ extern "C" int pfc_run_get_fields(pfc_run *r, double *phi, double *con) {
     return PFC_OK;
 }
 
+// FP64 host fields -> FP32 copies and the FP64 sums.  The fields are cut into 16 fixed
+// chunks, each summed with four accumulators, and the chunk sums are added in chunk
+// order, so the result does not depend on how many host threads share the chunks.
+static void convert_fields(const double *phi, const double *con, long P, float *a, float *b, double &sa,
+                           double &sb) {
+    constexpr int CH = 16;
+    double ps[CH], cs[CH];
+    auto work = [&](int c) {
+        const long lo = P * c / CH, hi = P * (c + 1) / CH;
+        double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0, c0 = 0.0, c1 = 0.0, c2 = 0.0, c3 = 0.0;
+        long i = lo;
+        for (; i + 4 <= hi; i += 4) {
+            a[i] = (float)phi[i];
+            a[i + 1] = (float)phi[i + 1];
+            a[i + 2] = (float)phi[i + 2];
+            a[i + 3] = (float)phi[i + 3];
+            b[i] = (float)con[i];
+            b[i + 1] = (float)con[i + 1];
+            b[i + 2] = (float)con[i + 2];
+            b[i + 3] = (float)con[i + 3];
+            p0 += phi[i];
+            p1 += phi[i + 1];
+            p2 += phi[i + 2];
+            p3 += phi[i + 3];
+            c0 += con[i];
+            c1 += con[i + 1];
+            c2 += con[i + 2];
+            c3 += con[i + 3];
+        }
+        for (; i < hi; ++i) {
+            a[i] = (float)phi[i];
+            b[i] = (float)con[i];
+            p0 += phi[i];
+            c0 += con[i];
+        }
+        ps[c] = (p0 + p1) + (p2 + p3);
+        cs[c] = (c0 + c1) + (c2 + c3);
+    };
+    const unsigned hc = std::thread::hardware_concurrency();
+    const int nt = P >= (1L << 18) ? (int)std::min(8u, hc ? hc : 1u) : 1;
+    if (nt <= 1) {
+        for (int c = 0; c < CH; ++c) work(c);
+    } else {
+        std::vector<std::thread> th;
+        for (int t = 0; t < nt; ++t)
+            th.emplace_back([&work, t, nt] {
+                for (int c = t; c < CH; c += nt) work(c);
+            });
+        for (auto &x : th) x.join();
+    }
+    sa = 0.0;
+    sb = 0.0;
+    for (int c = 0; c < CH; ++c) {
+        sa += ps[c];
+        sb += cs[c];
+    }
+}
+
 extern "C" int pfc_run_set_fields(pfc_run *r, const double *phi, const double *con) {
     if (!r || !phi || !con) return set_error(PFC_E_INVALID, "null argument");
     PFC_CUDA_TRY(cudaSetDevice(r->p.device));
     if (r->p.precision != PFC_PRECISION_FP32) return fp64_set_fields(r, phi, con);
-    std::vector<float> a(r->P), b(r->P);
-    double sa = 0.0, sb = 0.0;
-    for (long i = 0; i < r->P; ++i) {
-        a[i] = (float)phi[i];
-        b[i] = (float)con[i];
-        sa += phi[i];
-        sb += con[i];
+    // converted into the context's pinned staging buffer and uploaded from there; the
+    // buffer is held until fp32_from_real has synchronised the stream
+    Context *ctx = r->ctx;
+    std::lock_guard<std::mutex> lk(ctx->stage_mu);
+    if (ctx->stage_floats < 2 * (size_t)r->P) {
+        if (ctx->stage) cudaFreeHost(ctx->stage);
+        ctx->stage = nullptr;
+        ctx->stage_floats = 0;
+        PFC_CUDA_TRY(cudaMallocHost(&ctx->stage, 2 * (size_t)r->P * sizeof(float)));
+        ctx->stage_floats = 2 * (size_t)r->P;
     }
+    float *a = ctx->stage, *b = ctx->stage + r->P;
+    double sa = 0.0, sb = 0.0;
+    convert_fields(phi, con, r->P, a, b, sa, sb);
     r->psi_mean = sa / (double)r->P;
     r->con_mean = sb / (double)r->P;
-    PFC_CUDA_TRY(cudaMemcpyAsync(r->desc.psi_real, a.data(), r->P * sizeof(float), cudaMemcpyHostToDevice, r->stream));
-    PFC_CUDA_TRY(cudaMemcpyAsync(r->desc.con_real, b.data(), r->P * sizeof(float), cudaMemcpyHostToDevice, r->stream));
+    PFC_CUDA_TRY(cudaMemcpyAsync(r->desc.psi_real, a, r->P * sizeof(float), cudaMemcpyHostToDevice, r->stream));
+    PFC_CUDA_TRY(cudaMemcpyAsync(r->desc.con_real, b, r->P * sizeof(float), cudaMemcpyHostToDevice, r->stream));
     return fp32_from_real(r, false);
 }
 

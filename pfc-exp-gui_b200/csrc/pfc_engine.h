@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -18,6 +19,10 @@ struct Context {
     cudaStream_t stream = nullptr;
     TwiddleSet tw{};
     void *tw_mem = nullptr;
+    // pinned host staging for field uploads (pfc_run_set_fields), grown on demand
+    std::mutex stage_mu;
+    float *stage = nullptr;
+    size_t stage_floats = 0;
 };
 
 int set_error(int code, const std::string &msg);
