@@ -16,7 +16,8 @@
 // soon as the previous transform's first stage has consumed Q, so it streams in
 // while that transform, the update and the output transforms run; the next item's
 // phi tile streams in during the current item's con work.  Two CTAs of 256 threads
-// per SM (2 x 100 KB of shared memory, 128 registers).
+// per SM at C*L = 4096 (2 x 100 KB of shared memory, 128 registers); the tile width C
+// of a grid is chosen per device by the autotuner (engine.cu).
 
 // Tile staging (cp_async16, tile_prefetch, tile_wait, Prefetch, tile_out) and the
 // ScaleByTable / GradientOf multipliers come from tile_io.cuh.
@@ -56,10 +57,10 @@ __device__ float2 noise_mode(unsigned long long key, int t, int l, int km, int L
     return make_float2(s * rad * cs, conj ? -s * rad * sn : s * rad * sn);
 }
 
-template <int L, int MODE>
-__global__ void __launch_bounds__(ColCfg<L>::NT, 2) k_col_step(const RunDesc *__restrict__ runs, int nruns,
-                                                                const float2 *__restrict__ tw) {
-    constexpr int C = ColCfg<L>::C, NT = ColCfg<L>::NT;
+template <int L, int C, int MODE>
+__global__ void __launch_bounds__(ColCfg<L, C>::NT, ColCfg<L, C>::MINB)
+    k_col_step(const RunDesc *__restrict__ runs, int nruns, const float2 *__restrict__ tw) {
+    constexpr int NT = ColCfg<L, C>::NT;
     constexpr int SPAD = padded_len<C * L>::value;
     typedef RegOut<L, C, NT> RO;  // register scratch the transforms need for their last stage
     extern __shared__ __align__(16) float2 smem[];

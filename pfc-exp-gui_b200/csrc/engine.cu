@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <tuple>
@@ -186,10 +187,11 @@ static C2Params c2_params(float sig, float g1, float g2, float k1, float k2, flo
 // and dx use one table, so a batch of such runs reads it from L2.
 // ---------------------------------------------------------------------------
 struct KcoefKey {
-    int device, model, L, M;
+    int device, model, L, M, CT;
     uint32_t sig, dt, dx;
     bool operator<(const KcoefKey &o) const {
-        return std::tie(device, model, L, M, sig, dt, dx) < std::tie(o.device, o.model, o.L, o.M, o.sig, o.dt, o.dx);
+        return std::tie(device, model, L, M, CT, sig, dt, dx) <
+               std::tie(o.device, o.model, o.L, o.M, o.CT, o.sig, o.dt, o.dx);
     }
 };
 struct KcoefEntry {
@@ -206,7 +208,7 @@ static uint32_t fbits(float f) {
 }
 
 static KcoefKey kcoef_key(const pfc_run *r) {
-    return KcoefKey{r->p.device, r->p.model, r->L, r->M, fbits(r->p.sig), fbits(r->p.dt), fbits(r->p.dx)};
+    return KcoefKey{r->p.device, r->p.model, r->L, r->M, r->desc.CT, fbits(r->p.sig), fbits(r->p.dt), fbits(r->p.dx)};
 }
 
 // Table for run r (its descriptor must already be on the device); built on first use.
@@ -277,10 +279,10 @@ static unsigned long long noise_key(uint32_t seed) {
     return z ^ (z >> 31);
 }
 
-// Bytes of a run's own device allocation: 8 row-space arrays (FP32 path) + 2 real
-// fields + k tables + partials + result slots + descriptor.
-static size_t run_state_bytes(int L, int M, int N, bool fp32) {
-    const int Hp = round_up(M / 2 + 1, col_tile_width(L));
+// Bytes of a run's own device allocation with column tile width ct: 8 row-space
+// arrays (FP32 path) + 2 real fields + k tables + partials + result slots + descriptor.
+static size_t run_state_bytes(int L, int M, int N, bool fp32, int ct) {
+    const int Hp = round_up(M / 2 + 1, ct);
     const size_t rs = (size_t)L * Hp * sizeof(float2);
     const size_t real = (size_t)L * M * N * sizeof(float);
     const size_t ktab = (size_t)(L + M + N + 1) * sizeof(float);  // k-vectors + the step counter
@@ -299,9 +301,13 @@ extern "C" int pfc_run_bytes(const pfc_run_params *p, double *bytes) {
     if (!is_supported_len(p->L) || !is_supported_len(p->M) || p->N < 1)
         return set_error(PFC_E_INVALID, "unsupported grid");
     const bool fp32 = p->precision == PFC_PRECISION_FP32;
-    double b = (double)run_state_bytes(p->L, p->M, p->N, fp32);
+    // the widest tile the autotuner may choose (the most padding)
+    int cand[3];
+    const int nc = col_tile_candidates(p->L, cand);
+    const int ct = nc ? cand[nc - 1] : col_tile_width(p->L);
+    double b = (double)run_state_bytes(p->L, p->M, p->N, fp32, ct);
     const double P = (double)p->L * p->M * p->N;
-    if (fp32) b += 2.0 * (double)p->L * round_up(p->M / 2 + 1, col_tile_width(p->L)) * sizeof(float2);
+    if (fp32) b += 2.0 * (double)p->L * round_up(p->M / 2 + 1, ct) * sizeof(float2);
     else b += P * (22.0 * 16.0 + 6.0 * 8.0);
     *bytes = b;
     return PFC_OK;
@@ -361,7 +367,11 @@ static void free_run(pfc_run *r) {
     delete r;
 }
 
-extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) {
+static int tile_width_for(int device, int L, int M, int *width);
+
+// Create a run; ct_force > 0 fixes the column tile width of an FP32 run (the
+// autotuner's trial runs), 0 takes the grid's tuned width.
+static int run_create(const pfc_run_params *p, int ct_force, pfc_run **out) {
     if (!p || !out) return set_error(PFC_E_INVALID, "null argument");
     *out = nullptr;
     if (p->model != PFC_MODEL_MISFIT && p->model != PFC_MODEL_CVD) return set_error(PFC_E_INVALID, "unknown model");
@@ -384,6 +394,15 @@ extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) {
     int rc = get_context(p->device, &ctx);
     if (rc != PFC_OK) return rc;
     PFC_CUDA_TRY(cudaSetDevice(p->device));
+    int ct = col_tile_width(p->L);
+    if (p->precision == PFC_PRECISION_FP32) {
+        if (ct_force > 0) {
+            ct = ct_force;
+        } else {
+            rc = tile_width_for(p->device, p->L, p->M, &ct);
+            if (rc != PFC_OK) return rc;
+        }
+    }
 
     pfc_run *r = new pfc_run();
     r->p = *p;
@@ -393,7 +412,6 @@ extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) {
     r->M = p->M;
     r->N = p->N;
     r->P = (long)p->L * p->M * p->N;
-    const int ct = col_tile_width(p->L);
     r->Hp = round_up(p->M / 2 + 1, ct);
     model_coefs(p->model, &r->k);
     const ModelCoefs &k = r->k;
@@ -413,7 +431,7 @@ extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) {
     const size_t ktab = (size_t)(r->L + r->M + r->N + 1) * sizeof(float);
     const size_t parts = (size_t)(2 * nparts + 4096) * sizeof(double);
     const bool fp32 = p->precision == PFC_PRECISION_FP32;
-    const size_t bytes = run_state_bytes(r->L, r->M, r->N, fp32);
+    const size_t bytes = run_state_bytes(r->L, r->M, r->N, fp32, ct);
     cudaError_t e = cudaMalloc(&r->dev_mem, bytes);
     if (e != cudaSuccess) {
         free_run(r);
@@ -451,7 +469,7 @@ extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) {
     d.M = r->M;
     d.N = r->N;
     d.Hp = r->Hp;
-    d.CT = col_tile_width(r->L);
+    d.CT = ct;
     d.lct = 0;
     while ((1 << d.lct) < d.CT) ++d.lct;
     d.T = r->Hp / d.CT;
@@ -489,6 +507,146 @@ extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) {
         return rc;
     }
     *out = r;
+    return PFC_OK;
+}
+
+extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) { return run_create(p, 0, out); }
+
+// ---------------------------------------------------------------------------
+// Autotuner: the column tile width of FP32 runs of an L x M grid.  A run's row-space
+// layout and its column kernel's tile both follow the width; every column's transform
+// is the same arithmetic whatever the width, so the choice changes speed, not results.
+// On the first FP32 run of a grid on a device, each candidate width
+// (col_tile_candidates: the default, half and twice it, where the tile fits) runs a
+// batch of Misfit runs of at least 2 M points in all (4 to 16 runs): 3 warm-up steps,
+// then 8 steps of the row and column sweeps timed with CUDA events.  The fastest
+// width is kept for the rest of the process.  PFC_AUTOTUNE=0 in the environment keeps
+// the default widths; pfc_set_tile_width fixes one.
+// ---------------------------------------------------------------------------
+struct TileChoice {
+    int width = 0;
+    int n = 0;
+    int cand[3] = {0, 0, 0};
+    float ms[3] = {0.f, 0.f, 0.f};
+};
+static std::mutex g_tile_mu;
+static std::map<std::tuple<int, int, int>, TileChoice> g_tile;
+
+// Device time of 8 steps of a trial batch with tile width ct.
+static int time_tile_width(int device, int L, int M, int ct, float *ms) {
+    const long pts = (long)L * M;
+    const int nruns = (int)std::max(4L, std::min(16L, (2L << 20) / pts));
+    std::vector<pfc_run *> runs;
+    int rc = PFC_OK;
+    for (int i = 0; i < nruns && rc == PFC_OK; ++i) {
+        pfc_run_params p;
+        pfc_default_params(PFC_MODEL_MISFIT, &p);
+        p.L = L;
+        p.M = M;
+        p.device = device;
+        p.seed = 1000u + (uint32_t)i;
+        pfc_run *r = nullptr;
+        rc = run_create(&p, ct, &r);
+        if (rc == PFC_OK) runs.push_back(r);
+    }
+    RunDesc *d = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (rc == PFC_OK) {
+        const int n = (int)runs.size();
+        std::vector<RunDesc> h;
+        for (auto *r : runs) h.push_back(r->desc);
+        cudaStream_t st = runs[0]->stream;
+        const TwiddleSet &tw = runs[0]->ctx->tw;
+        auto step = [&]() {
+            cudaError_t x = launch_row_step(d, n, L, M, tw, st);
+            if (x == cudaSuccess) x = launch_col_step(d, n, L, M, ct, COL_STEP, tw, st);
+            return x;
+        };
+        cudaError_t ce = cudaMalloc(&d, h.size() * sizeof(RunDesc));
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(d, h.data(), h.size() * sizeof(RunDesc), cudaMemcpyHostToDevice, st);
+        if (ce == cudaSuccess) ce = cudaEventCreate(&e0);
+        if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+        for (int i = 0; i < 3 && ce == cudaSuccess; ++i) ce = step();
+        if (ce == cudaSuccess) ce = cudaEventRecord(e0, st);
+        for (int i = 0; i < 8 && ce == cudaSuccess; ++i) ce = step();
+        if (ce == cudaSuccess) ce = cudaEventRecord(e1, st);
+        if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+        if (ce == cudaSuccess) ce = cudaEventElapsedTime(ms, e0, e1);
+        if (ce == cudaErrorMemoryAllocation) rc = set_error(PFC_E_NOMEM, "tile width trial: out of memory");
+        else if (ce != cudaSuccess) rc = cuda_error(ce, "tile width trial");
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (d) cudaFree(d);
+    for (auto *r : runs) pfc_run_destroy(r);
+    return rc;
+}
+
+static int tile_width_for(int device, int L, int M, int *width) {
+    std::lock_guard<std::mutex> lk(g_tile_mu);
+    const auto key = std::make_tuple(device, L, M);
+    auto it = g_tile.find(key);
+    if (it != g_tile.end()) {
+        *width = it->second.width;
+        return PFC_OK;
+    }
+    TileChoice c;
+    c.width = col_tile_width(L);
+    int cand[3];
+    const int nc = col_tile_candidates(L, cand);
+    const char *env = std::getenv("PFC_AUTOTUNE");
+    if (nc > 1 && !(env && env[0] == '0')) {
+        float best = 0.f;
+        for (int i = 0; i < nc; ++i) {
+            float ms = 0.f;
+            const int rc = time_tile_width(device, L, M, cand[i], &ms);
+            if (rc == PFC_E_NOMEM) {  // no room for trial runs: keep the default width
+                c = TileChoice{};
+                c.width = col_tile_width(L);
+                break;
+            }
+            if (rc != PFC_OK) return rc;
+            c.cand[c.n] = cand[i];
+            c.ms[c.n++] = ms;
+            if (i == 0 || ms < best) {
+                best = ms;
+                c.width = cand[i];
+            }
+        }
+    }
+    g_tile[key] = c;
+    *width = c.width;
+    return PFC_OK;
+}
+
+extern "C" int pfc_tile_width(int device, int L, int M, int *width, int *candidates, float *trial_ms, int *ntrials) {
+    if (!width) return set_error(PFC_E_INVALID, "null argument");
+    if (!is_supported_len(L) || !is_supported_len(M)) return set_error(PFC_E_INVALID, "unsupported grid");
+    Context *ctx = nullptr;
+    int rc = get_context(device, &ctx);
+    if (rc != PFC_OK) return rc;
+    PFC_CUDA_TRY(cudaSetDevice(device));
+    rc = tile_width_for(device, L, M, width);
+    if (rc != PFC_OK) return rc;
+    std::lock_guard<std::mutex> lk(g_tile_mu);
+    const TileChoice &c = g_tile[std::make_tuple(device, L, M)];
+    if (ntrials) *ntrials = c.n;
+    for (int i = 0; i < c.n; ++i) {
+        if (candidates) candidates[i] = c.cand[i];
+        if (trial_ms) trial_ms[i] = c.ms[i];
+    }
+    return PFC_OK;
+}
+
+extern "C" int pfc_set_tile_width(int device, int L, int M, int width) {
+    if (!is_supported_len(L) || !is_supported_len(M)) return set_error(PFC_E_INVALID, "unsupported grid");
+    int cand[3];
+    const int nc = col_tile_candidates(L, cand);
+    bool ok = false;
+    for (int i = 0; i < nc; ++i) ok = ok || cand[i] == width;
+    if (!ok) return set_error(PFC_E_INVALID, "tile width not available for this grid");
+    std::lock_guard<std::mutex> lk(g_tile_mu);
+    g_tile[std::make_tuple(device, L, M)].width = width;  // a trial record, if any, is kept
     return PFC_OK;
 }
 
@@ -591,7 +749,7 @@ static int fp32_from_real(pfc_run *r, bool means_from_device) {
     r->step_ctr_init = r->t - 1;
     PFC_CUDA_TRY(cudaMemcpyAsync(d.step_ctr, &r->step_ctr_init, sizeof(int), cudaMemcpyHostToDevice, r->stream));
     PFC_CUDA_TRY(launch_row_forward(r->d_desc, 1, r->L, r->M, r->ctx->tw, r->stream));
-    PFC_CUDA_TRY(launch_col_step(r->d_desc, 1, r->L, r->M, COL_PREPARE, r->ctx->tw, r->stream));
+    PFC_CUDA_TRY(launch_col_step(r->d_desc, 1, r->L, r->M, r->desc.CT, COL_PREPARE, r->ctx->tw, r->stream));
     PFC_CUDA_TRY(cudaStreamSynchronize(r->stream));
     r->fields_valid = true;
     r->energy_valid = false;
@@ -619,7 +777,8 @@ static int fp32_advance(pfc_run *r, int nsteps, int analysis) {
     for (int i = 0; i < nsteps; ++i) {
         const bool last = i == nsteps - 1;
         PFC_CUDA_TRY(launch_row_step(r->d_desc, 1, r->L, r->M, r->ctx->tw, r->stream));
-        PFC_CUDA_TRY(launch_col_step(r->d_desc, 1, r->L, r->M, (last && analysis) ? COL_STEP_CHECKPOINT : COL_STEP,
+        PFC_CUDA_TRY(launch_col_step(r->d_desc, 1, r->L, r->M, r->desc.CT,
+                                     (last && analysis) ? COL_STEP_CHECKPOINT : COL_STEP,
                                      r->ctx->tw, r->stream));
     }
     r->t += nsteps;
@@ -807,7 +966,7 @@ extern "C" int pfc_run_means(const pfc_run *r, double *phi_mean, double *con_mea
 // captured once into a CUDA graph per step count.
 // ---------------------------------------------------------------------------
 struct SizeClass {
-    int L, M;
+    int L, M, CT;
     std::vector<pfc_run *> runs;
     RunDesc *d_descs = nullptr;
 };
@@ -838,9 +997,9 @@ extern "C" int pfc_batch_create(pfc_run *const *runs, int nruns, pfc_batch **out
     for (int i = 0; i < nruns; ++i) {
         SizeClass *sc = nullptr;
         for (auto &c : b->classes)
-            if (c.L == runs[i]->L && c.M == runs[i]->M) sc = &c;
+            if (c.L == runs[i]->L && c.M == runs[i]->M && c.CT == runs[i]->desc.CT) sc = &c;
         if (!sc) {
-            b->classes.push_back(SizeClass{runs[i]->L, runs[i]->M, {}, nullptr});
+            b->classes.push_back(SizeClass{runs[i]->L, runs[i]->M, runs[i]->desc.CT, {}, nullptr});
             sc = &b->classes.back();
         }
         sc->runs.push_back(runs[i]);
@@ -874,7 +1033,8 @@ static int batch_enqueue(pfc_batch *b, int nsteps) {
         for (auto &c : b->classes)
             PFC_CUDA_TRY(launch_row_step(c.d_descs, (int)c.runs.size(), c.L, c.M, b->ctx->tw, b->stream));
         for (auto &c : b->classes)
-            PFC_CUDA_TRY(launch_col_step(c.d_descs, (int)c.runs.size(), c.L, c.M, COL_STEP, b->ctx->tw, b->stream));
+            PFC_CUDA_TRY(
+                launch_col_step(c.d_descs, (int)c.runs.size(), c.L, c.M, c.CT, COL_STEP, b->ctx->tw, b->stream));
     }
     return PFC_OK;
 }
@@ -914,7 +1074,8 @@ extern "C" int pfc_batch_kernel_times(pfc_batch *b, int reps, double *row_ms, do
             PFC_CUDA_TRY(launch_row_step(c.d_descs, (int)c.runs.size(), c.L, c.M, b->ctx->tw, b->stream));
         PFC_CUDA_TRY(cudaEventRecord(ev[3 * i + 1], b->stream));
         for (auto &c : b->classes)
-            PFC_CUDA_TRY(launch_col_step(c.d_descs, (int)c.runs.size(), c.L, c.M, COL_STEP, b->ctx->tw, b->stream));
+            PFC_CUDA_TRY(
+                launch_col_step(c.d_descs, (int)c.runs.size(), c.L, c.M, c.CT, COL_STEP, b->ctx->tw, b->stream));
         PFC_CUDA_TRY(cudaEventRecord(ev[3 * i + 2], b->stream));
     }
     PFC_CUDA_TRY(cudaStreamSynchronize(b->stream));
@@ -950,7 +1111,7 @@ extern "C" int pfc_batch_advance(pfc_batch *b, int nsteps) {
             b->graph = nullptr;
         }
         // kernel attribute setup (max dynamic shared memory) happens outside the capture
-        for (auto &c : b->classes) PFC_CUDA_TRY(prepare_size(c.L, c.M));
+        for (auto &c : b->classes) PFC_CUDA_TRY(prepare_size(c.L, c.M, c.CT));
         int rc = PFC_OK;
         cudaGraph_t g = nullptr;
         PFC_CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));

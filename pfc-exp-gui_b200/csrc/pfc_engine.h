@@ -76,5 +76,5 @@ int fp64_get_fields(pfc_run *r, double *phi, double *con);
 int fp64_set_fields(pfc_run *r, const double *phi, const double *con);
 int fp64_energy(pfc_run *r, double *e_over_p, double *mass_over_p);
 // Kernel attribute setup for one grid size (must precede graph capture).
-cudaError_t prepare_size(int L, int M);
+cudaError_t prepare_size(int L, int M, int C);
 }  // namespace pfc

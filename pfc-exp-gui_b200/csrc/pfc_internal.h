@@ -73,7 +73,8 @@ struct TwiddleSet {
 
 // FP32 fused step (step_fp32.cu).  All runs of one call share (L, M).
 cudaError_t launch_row_step(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw, cudaStream_t s);
-cudaError_t launch_col_step(const RunDesc *d_runs, int nruns, int L, int M, int mode, const TwiddleSet &tw,
+// C: column tile width of the runs' layout (RunDesc::CT, the same for all nruns runs)
+cudaError_t launch_col_step(const RunDesc *d_runs, int nruns, int L, int M, int C, int mode, const TwiddleSet &tw,
                             cudaStream_t s);
 cudaError_t launch_row_forward(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw, cudaStream_t s);
 cudaError_t launch_row_analysis(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw,
@@ -95,7 +96,9 @@ cudaError_t prepare_rows(int M);
 
 // Number of partial-sum slots the analysis kernel writes per run (2 doubles each).
 int analysis_partials(int L, int M);
-// Column-tile width of the row-space layout for a grid with L rows.
+// Default column-tile width of the row-space layout for a grid with L rows, and the
+// widths the autotuner may choose from (out[] holds up to 3; returns their number).
 int col_tile_width(int L);
+int col_tile_candidates(int L, int *out);
 
 }  // namespace pfc

@@ -92,7 +92,7 @@ int steps_to_event(const Job &j) {
 }
 
 struct Cohort {
-    int model = 0, L = 0, M = 0;
+    int model = 0, L = 0, M = 0, CT = 0;  // runs of one model, grid and column tile width
     std::vector<Job *> jobs;
     RunDesc *d_descs = nullptr;
     double *d_ehist = nullptr;  // [n][SEG][2] (CVD)
@@ -211,13 +211,14 @@ int build_cohorts(pfc_engine *e) {
     for (Job *j : e->active) {
         Cohort *c = nullptr;
         for (auto &x : e->cohorts)
-            if (x.model == j->spec.kind && x.L == j->L && x.M == j->M) c = &x;
+            if (x.model == j->spec.kind && x.L == j->L && x.M == j->M && x.CT == j->run->desc.CT) c = &x;
         if (!c) {
             e->cohorts.push_back(Cohort{});
             c = &e->cohorts.back();
             c->model = j->spec.kind;
             c->L = j->L;
             c->M = j->M;
+            c->CT = j->run->desc.CT;
         }
         c->jobs.push_back(j);
     }
@@ -236,7 +237,7 @@ int build_cohorts(pfc_engine *e) {
             h[i].ehist = c.d_ehist ? c.d_ehist + (size_t)i * SEG * 2 : nullptr;
         }
         PFC_CUDA_TRY(cudaMemcpyAsync(c.d_descs, h.data(), n * sizeof(RunDesc), cudaMemcpyHostToDevice, e->main));
-        PFC_CUDA_TRY(prepare_size(c.L, c.M));
+        PFC_CUDA_TRY(prepare_size(c.L, c.M, c.CT));
         cudaEvent_t ev;
         PFC_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         e->join_events.push_back(ev);
@@ -263,9 +264,9 @@ int cohort_step(pfc_engine *e, Cohort &c, int slot, cudaStream_t st) {
     const TwiddleSet &tw = e->ctx->tw;
     PFC_CUDA_TRY(launch_row_step(c.d_descs, n, c.L, c.M, tw, st));
     if (c.model == PFC_JOB_MISFIT) {
-        PFC_CUDA_TRY(launch_col_step(c.d_descs, n, c.L, c.M, COL_STEP, tw, st));
+        PFC_CUDA_TRY(launch_col_step(c.d_descs, n, c.L, c.M, c.CT, COL_STEP, tw, st));
     } else {
-        PFC_CUDA_TRY(launch_col_step(c.d_descs, n, c.L, c.M, COL_STEP_CHECKPOINT, tw, st));
+        PFC_CUDA_TRY(launch_col_step(c.d_descs, n, c.L, c.M, c.CT, COL_STEP_CHECKPOINT, tw, st));
         PFC_CUDA_TRY(launch_row_analysis(c.d_descs, n, c.L, c.M, tw, st));
         PFC_CUDA_TRY(launch_reduce_runs(c.d_descs, n, analysis_partials(c.L, c.M), slot, st));
     }
@@ -614,7 +615,7 @@ int quantum(pfc_engine *e) {
             for (Job *j : c.jobs) {
                 const bool ck = std::find(ckpt.begin(), ckpt.end(), j) != ckpt.end();
                 PFC_CUDA_TRY(
-                    launch_col_step(j->run->d_desc, 1, c.L, c.M, ck ? COL_STEP_CHECKPOINT : COL_STEP, tw, e->main));
+                    launch_col_step(j->run->d_desc, 1, c.L, c.M, c.CT, ck ? COL_STEP_CHECKPOINT : COL_STEP, tw, e->main));
             }
         }
         const int rc = copy_energy_slots(e, (int)seg_len.size());

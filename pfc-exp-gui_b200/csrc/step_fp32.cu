@@ -40,6 +40,14 @@ int col_tile_width(int L) {
     return c > 16 ? 16 : (c < 1 ? 1 : c);
 }
 
+int col_tile_candidates(int L, int *out) {
+    const int d = col_tile_width(L);
+    int n = 0;
+    for (int c : {d / 2, d, 2 * d})
+        if (col_tile_ok(L, c)) out[n++] = c;
+    return n;
+}
+
 __device__ __forceinline__ long rs_index(const RunDesc &d, int l, int km) {
     return ((long)(km >> d.lct) * d.L + l) * d.CT + (km & (d.CT - 1));
 }
@@ -458,18 +466,19 @@ static cudaError_t row_analysis_impl(const RunDesc *d_runs, int nruns, int L, co
     return cudaGetLastError();
 }
 
-template <int L, int MODE>
+template <int L, int C, int MODE>
 static cudaError_t col_impl(const RunDesc *d_runs, int nruns, int M, const TwiddleSet &tw, cudaStream_t st) {
-    constexpr int C = ColCfg<L>::C, NT = ColCfg<L>::NT;
+    constexpr int NT = ColCfg<L, C>::NT;
     constexpr size_t smem = 2 * smem_bytes<C * L>() + sizeof(float2) * C * L;  // s, P (padded) and Q
     static unsigned mask = 0;
-    cudaError_t e = set_smem(k_col_step<L, MODE>, smem, mask);
+    cudaError_t e = set_smem(k_col_step<L, C, MODE>, smem, mask);
     if (nruns == 0) return e;
     if (e != cudaSuccess) return e;
     const int H = M / 2;
     const int items = ((H + 1 + C - 1) / C) * nruns;
-    const int grid = items < 2 * sm_count() ? items : 2 * sm_count();
-    k_col_step<L, MODE><<<grid, NT, smem, st>>>(d_runs, nruns, tw.f32[log2i(L)]);
+    const int cap = ColCfg<L, C>::MINB * sm_count();
+    const int grid = items < cap ? items : cap;
+    k_col_step<L, C, MODE><<<grid, NT, smem, st>>>(d_runs, nruns, tw.f32[log2i(L)]);
     return cudaGetLastError();
 }
 
@@ -486,20 +495,41 @@ cudaError_t launch_row_analysis(const RunDesc *d_runs, int nruns, int L, int M, 
     PFC_SIZE_SWITCH(M, row_analysis_impl, d_runs, nruns, L, tw, s)
 }
 
-template <int L>
-static cudaError_t col_dispatch(const RunDesc *d_runs, int nruns, int M, int mode, const TwiddleSet &tw,
-                                cudaStream_t s) {
+template <int L, int C>
+static cudaError_t col_modes(const RunDesc *d_runs, int nruns, int M, int mode, const TwiddleSet &tw,
+                             cudaStream_t s) {
     switch (mode) {
-        case COL_STEP: return col_impl<L, COL_STEP>(d_runs, nruns, M, tw, s);
-        case COL_PREPARE: return col_impl<L, COL_PREPARE>(d_runs, nruns, M, tw, s);
-        case COL_STEP_CHECKPOINT: return col_impl<L, COL_STEP_CHECKPOINT>(d_runs, nruns, M, tw, s);
+        case COL_STEP: return col_impl<L, C, COL_STEP>(d_runs, nruns, M, tw, s);
+        case COL_PREPARE: return col_impl<L, C, COL_PREPARE>(d_runs, nruns, M, tw, s);
+        case COL_STEP_CHECKPOINT: return col_impl<L, C, COL_STEP_CHECKPOINT>(d_runs, nruns, M, tw, s);
         default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t launch_col_step(const RunDesc *d_runs, int nruns, int L, int M, int mode, const TwiddleSet &tw,
+template <int L>
+static cudaError_t col_dispatch(const RunDesc *d_runs, int nruns, int M, int C, int mode, const TwiddleSet &tw,
+                                cudaStream_t s) {
+    switch (C) {
+        case 2:
+            if constexpr (col_tile_ok(L, 2)) return col_modes<L, 2>(d_runs, nruns, M, mode, tw, s);
+            break;
+        case 4:
+            if constexpr (col_tile_ok(L, 4)) return col_modes<L, 4>(d_runs, nruns, M, mode, tw, s);
+            break;
+        case 8:
+            if constexpr (col_tile_ok(L, 8)) return col_modes<L, 8>(d_runs, nruns, M, mode, tw, s);
+            break;
+        case 16:
+            if constexpr (col_tile_ok(L, 16)) return col_modes<L, 16>(d_runs, nruns, M, mode, tw, s);
+            break;
+        default: break;
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_col_step(const RunDesc *d_runs, int nruns, int L, int M, int C, int mode, const TwiddleSet &tw,
                             cudaStream_t s) {
-    PFC_SIZE_SWITCH(L, col_dispatch, d_runs, nruns, M, mode, tw, s)
+    PFC_SIZE_SWITCH(L, col_dispatch, d_runs, nruns, M, C, mode, tw, s)
 }
 
 cudaError_t prepare_rows(int M) {
@@ -511,12 +541,12 @@ cudaError_t prepare_rows(int M) {
     return launch_row_analysis(nullptr, 0, 0, M, none, 0);
 }
 
-cudaError_t prepare_size(int L, int M) {
+cudaError_t prepare_size(int L, int M, int C) {
     TwiddleSet none{};
     cudaError_t e;
     if ((e = prepare_rows(M)) != cudaSuccess) return e;
     for (int mode = 0; mode < 3; ++mode)
-        if ((e = launch_col_step(nullptr, 0, L, M, mode, none, 0)) != cudaSuccess) return e;
+        if ((e = launch_col_step(nullptr, 0, L, M, C, mode, none, 0)) != cudaSuccess) return e;
     return cudaSuccess;
 }
 

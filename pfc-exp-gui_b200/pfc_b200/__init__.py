@@ -154,6 +154,8 @@ def lib():
         "pfc_job_fields": ([vp, C.c_uint64, fp, fp], C.c_int),
         "pfc_release": ([vp, C.c_uint64], C.c_int),
         "pfc_run_bytes": ([P(RunParams), dp], C.c_int),
+        "pfc_tile_width": ([C.c_int, C.c_int, C.c_int, P(C.c_int), P(C.c_int), fp, P(C.c_int)], C.c_int),
+        "pfc_set_tile_width": ([C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -341,6 +343,21 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+
+def tile_width(L: int, M: int, device: int = 0):
+    """Column tile width FP32 runs of an L x M grid use (tuned on the device on first
+    use) and the autotuner's trials: (width, {candidate: ms per 8 steps})."""
+    w, n = C.c_int(), C.c_int()
+    cand = (C.c_int * 3)()
+    ms = (C.c_float * 3)()
+    _check(lib().pfc_tile_width(device, L, M, C.byref(w), cand, ms, C.byref(n)), "pfc_tile_width")
+    return w.value, {cand[i]: ms[i] for i in range(n.value)}
+
+
+def set_tile_width(L: int, M: int, width: int, device: int = 0):
+    """Fix the column tile width of an L x M grid for the rest of the process."""
+    _check(lib().pfc_set_tile_width(device, L, M, width), "pfc_set_tile_width")
 
 
 def run_bytes(params) -> float:
