@@ -47,6 +47,8 @@ def parse(argv=None):
     ap.add_argument("--no-serve", action="store_true", help="skip the serving (Poisson arrivals) measurement")
     ap.add_argument("--serve-requests", type=int, default=48)
     ap.add_argument("--no-cvd3d", action="store_true", help="skip the 3-D CVD (256x256x64) step measurement")
+    ap.add_argument("--tile-width", type=int, default=0,
+                    help="fix the column tile width instead of the autotuner's choice (reproducible profiles)")
     return ap.parse_args(argv)
 
 
@@ -167,13 +169,13 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(grid, batch):
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, scaled to this batch."""
+def profiled_traffic(grid, batch, kernel):
+    """DRAM bytes per launch of `kernel` ("col" or "row") from the committed ncu summary, scaled to this batch."""
     p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     if not os.path.exists(p):
         return None
     j = json.load(open(p))
-    per_run = j.get("col_kernel_dram_bytes_per_run", {}).get(str(grid))
+    per_run = j.get(f"{kernel}_kernel_dram_bytes_per_run", {}).get(str(grid))
     return None if per_run is None else per_run * batch
 
 
@@ -409,6 +411,8 @@ def run_ours(args):
     import pfc_b200 as P
     dev = dist.local
     G, B = args.grid, args.batch
+    if args.tile_width:
+        P.set_tile_width(G, G, args.tile_width, device=dev)
     runs = []
     for i in range(B):
         p = P.default_params(P.MODEL_MISFIT, L=G, M=G, N=1, seed=1000 + i + 100000 * dist.rank, device=dev)
@@ -436,7 +440,7 @@ def run_ours(args):
         dom, dom_ms, dom_bytes = "k_row_step", row_ms, bytes_row
     peak, peak_kind = measured_peak()
     achieved = dom_bytes / (dom_ms / 1000.0) / 1e9
-    traffic = profiled_traffic(G, B) if dom == "k_col_step" else None
+    traffic = profiled_traffic(G, B, "col" if dom == "k_col_step" else "row")
 
     # end to end through the public API: host initial fields in, B runs x K steps, host fields out
     phi0, con0 = runs[0].fields()
