@@ -48,3 +48,31 @@ def test_tuner_reports_its_trials():
     assert P.tile_width(1024, 1024)[0] == w
     with pytest.raises(P.PfcError):
         P.set_tile_width(1024, 1024, 16)  # the tile would not fit
+
+
+def test_batch_mixing_tile_widths_equals_single_runs():
+    """Runs of one grid created before and after the width is changed keep their own
+    layouts; a batch holding both advances each with its own width."""
+    L = M = 256
+    tuned, trials = P.tile_width(L, M)
+    widths = sorted(trials) if len(trials) > 1 else [8, 16]
+    try:
+        runs = []
+        for i, w in enumerate(widths):
+            P.set_tile_width(L, M, w)
+            runs.append(P.Run(P.default_params(P.MODEL_MISFIT, L=L, M=M, seed=100 + i)))
+        batch = P.Batch(runs)
+        batch.advance(20)
+        singles = []
+        for i, w in enumerate(widths):
+            P.set_tile_width(L, M, w)
+            r = P.Run(P.default_params(P.MODEL_MISFIT, L=L, M=M, seed=100 + i))
+            r.advance(20)
+            singles.append(r)
+        for a, b in zip(runs, singles):
+            fa, ca = a.fields_f32()
+            fb, cb = b.fields_f32()
+            assert np.array_equal(fa, fb) and np.array_equal(ca, cb)
+        batch.close()
+    finally:
+        P.set_tile_width(L, M, tuned)
