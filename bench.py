@@ -313,9 +313,13 @@ def sweep_bench(P, dev, nruns=64, steps=2000, master_seed=4242):
 
     def run(max_active):
         eng = P.Engine(device=dev, max_active=max_active)
-        warm = eng.submit(P.JOB_MISFIT, P.default_params(P.MODEL_MISFIT, L=128, M=128, device=dev), steps=40, mod=40)
-        drain_engine(P, eng, 1)
-        eng.release(warm)
+        # warm-up: one short job per grid, with a checkpoint, so that neither arm pays the
+        # first use of a grid's kernels (module loading) inside its timed region
+        warm = [eng.submit(P.JOB_MISFIT, P.default_params(P.MODEL_MISFIT, L=g, M=g, device=dev), steps=40, mod=20)
+                for g in widths]
+        drain_engine(P, eng, len(warm))
+        for w in warm:
+            eng.release(w)
         t0 = time.perf_counter()
         ids = [eng.submit(P.JOB_MISFIT, p, steps=steps, mod=steps) for p in jobs]
         done = drain_engine(P, eng, len(ids))
