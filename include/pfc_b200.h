@@ -77,12 +77,12 @@ int pfc_run_advance(pfc_run *r, int nsteps, int analysis);
  * *ms receives the device time.  (Measurement hook; no reference counterpart.) */
 int pfc_run_advance_timed(pfc_run *r, int nsteps, float *ms);
 
-/* Column tile width (packed columns per column-kernel tile, 2..16) that FP32 runs of
+/* Column tile width (packed columns per column-kernel tile, 1..16) that FP32 runs of
  * an L x M grid use on `device`.  The first FP32 run of a grid times each candidate
  * width on the device (a batch of Misfit runs, row and column sweeps, CUDA events) and
  * keeps the fastest for the process; the width changes the speed of a step, not its
  * results.  This call tunes the grid if it has not been tuned, returns the width and,
- * when the pointers are not NULL, the candidates and their trial times (ms per 8
+ * when the pointers are not NULL, the candidates (up to 4) and their trial times (ms per 8
  * steps; *ntrials is 0 when no trial ran).  PFC_AUTOTUNE=0 in the environment keeps
  * the default widths.  (Autotuner of the batched FFT sweeps; the reference uses FFTW
  * and has no counterpart.) */

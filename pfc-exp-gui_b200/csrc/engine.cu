@@ -302,7 +302,7 @@ extern "C" int pfc_run_bytes(const pfc_run_params *p, double *bytes) {
         return set_error(PFC_E_INVALID, "unsupported grid");
     const bool fp32 = p->precision == PFC_PRECISION_FP32;
     // the widest tile the autotuner may choose (the most padding)
-    int cand[3];
+    int cand[4];
     const int nc = col_tile_candidates(p->L, cand);
     const int ct = nc ? cand[nc - 1] : col_tile_width(p->L);
     double b = (double)run_state_bytes(p->L, p->M, p->N, fp32, ct);
@@ -517,7 +517,7 @@ extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) { return r
 // layout and its column kernel's tile both follow the width; every column's transform
 // is the same arithmetic whatever the width, so the choice changes speed, not results.
 // On the first FP32 run of a grid on a device, each candidate width
-// (col_tile_candidates: the default, half and twice it, where the tile fits) runs a
+// (col_tile_candidates: the default, a quarter, half and twice it, where the tile fits) runs a
 // batch of Misfit runs of at least 2 M points in all (4 to 16 runs): 3 warm-up steps,
 // then 8 steps of the row and column sweeps timed with CUDA events.  The fastest
 // width is kept for the rest of the process.  PFC_AUTOTUNE=0 in the environment keeps
@@ -526,8 +526,8 @@ extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) { return r
 struct TileChoice {
     int width = 0;
     int n = 0;
-    int cand[3] = {0, 0, 0};
-    float ms[3] = {0.f, 0.f, 0.f};
+    int cand[4] = {0, 0, 0, 0};
+    float ms[4] = {0.f, 0.f, 0.f, 0.f};
 };
 static std::mutex g_tile_mu;
 static std::map<std::tuple<int, int, int>, TileChoice> g_tile;
@@ -592,7 +592,7 @@ static int tile_width_for(int device, int L, int M, int *width) {
     }
     TileChoice c;
     c.width = col_tile_width(L);
-    int cand[3];
+    int cand[4];
     const int nc = col_tile_candidates(L, cand);
     const char *env = std::getenv("PFC_AUTOTUNE");
     if (nc > 1 && !(env && env[0] == '0')) {
@@ -640,7 +640,7 @@ extern "C" int pfc_tile_width(int device, int L, int M, int *width, int *candida
 
 extern "C" int pfc_set_tile_width(int device, int L, int M, int width) {
     if (!is_supported_len(L) || !is_supported_len(M)) return set_error(PFC_E_INVALID, "unsupported grid");
-    int cand[3];
+    int cand[4];
     const int nc = col_tile_candidates(L, cand);
     bool ok = false;
     for (int i = 0; i < nc; ++i) ok = ok || cand[i] == width;

@@ -97,7 +97,7 @@ cudaError_t prepare_rows(int M);
 // Number of partial-sum slots the analysis kernel writes per run (2 doubles each).
 int analysis_partials(int L, int M);
 // Default column-tile width of the row-space layout for a grid with L rows, and the
-// widths the autotuner may choose from (out[] holds up to 3; returns their number).
+// widths the autotuner may choose from (out[] holds up to 4; returns their number).
 int col_tile_width(int L);
 int col_tile_candidates(int L, int *out);
 

@@ -11,9 +11,9 @@ namespace pfc {
 
 constexpr int COL_TILE = 4096;  // complex elements per column-kernel tile (32 KB in FP32)
 
-// Column-kernel tile: L rows x C packed columns, C a power of two in [2, 16] with
-// 512 <= C*L <= 8192 complex elements (three such buffers per CTA: 25 KB to 204 KB).
-constexpr bool col_tile_ok(int L, int C) { return C >= 2 && C <= 16 && C * L >= 512 && C * L <= 8192; }
+// Column-kernel tile: L rows x C packed columns, C a power of two in [1, 16] with
+// 512 <= C*L <= 8192 complex elements (three such buffers per CTA: 13 KB to 204 KB).
+constexpr bool col_tile_ok(int L, int C) { return C >= 1 && C <= 16 && C * L >= 512 && C * L <= 8192; }
 template <int L, int C> struct ColCfg {
     static constexpr int NT = (C * L / 16) < 32 ? 32 : (C * L / 16);
     // CTAs per SM that the shared memory leaves room for (two at C*L = 4096)

@@ -43,7 +43,7 @@ int col_tile_width(int L) {
 int col_tile_candidates(int L, int *out) {
     const int d = col_tile_width(L);
     int n = 0;
-    for (int c : {d / 2, d, 2 * d})
+    for (int c : {d / 4, d / 2, d, 2 * d})
         if (col_tile_ok(L, c)) out[n++] = c;
     return n;
 }
@@ -510,6 +510,9 @@ template <int L>
 static cudaError_t col_dispatch(const RunDesc *d_runs, int nruns, int M, int C, int mode, const TwiddleSet &tw,
                                 cudaStream_t s) {
     switch (C) {
+        case 1:
+            if constexpr (col_tile_ok(L, 1)) return col_modes<L, 1>(d_runs, nruns, M, mode, tw, s);
+            break;
         case 2:
             if constexpr (col_tile_ok(L, 2)) return col_modes<L, 2>(d_runs, nruns, M, mode, tw, s);
             break;

@@ -349,8 +349,8 @@ def tile_width(L: int, M: int, device: int = 0):
     """Column tile width FP32 runs of an L x M grid use (tuned on the device on first
     use) and the autotuner's trials: (width, {candidate: ms per 8 steps})."""
     w, n = C.c_int(), C.c_int()
-    cand = (C.c_int * 3)()
-    ms = (C.c_float * 3)()
+    cand = (C.c_int * 4)()
+    ms = (C.c_float * 4)()
     _check(lib().pfc_tile_width(device, L, M, C.byref(w), cand, ms, C.byref(n)), "pfc_tile_width")
     return w.value, {cand[i]: ms[i] for i in range(n.value)}
 
