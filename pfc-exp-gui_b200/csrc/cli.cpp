@@ -12,7 +12,8 @@
 // Files are byte-compatible with the reference writers (VTI/PVTI at
 // misfit_uniform_time_seed_fftw_early.cpp:1588-1810, text files with std::fixed and
 // precision(4)).  Additive options: --grid LxMxN (runtime grid; default 256x256x1)
-// and --precision fp32|fp64|fp64-pure.  Output paths are prefixed with --outdir
+// and --precision fp32|fp64|fp64-pure (default fp32 on 2-D grids, fp64 on 3-D grids,
+// which the FP32 path does not take).  Output paths are prefixed with --outdir
 // instead of changing the process working directory.
 #include <algorithm>
 #include <cerrno>
@@ -147,7 +148,7 @@ struct SimOpts {
     unsigned int seed;
     int grainx, grainy, grainz;
     int L = 256, M = 256, N = 1;
-    int precision = PFC_PRECISION_FP32;
+    int precision = -1;  // -1: FP32 on 2-D grids, FP64 on 3-D grids
     int resume = -1;  // --resume <kd>: continue from the run's own checkpoint kd
     std::string outdir;
 };
@@ -200,6 +201,7 @@ void misfit_usage(const char *argv0) {
          << "  --axx <float>       Noise base intensity (default: 0)\n"
          << "  --outdir <path>     Output directory (default: current dir)\n"
          << "  --grid <LxMxN>      Grid (default: 256x256x1)\n"
+         << "  --precision <p>     fp32, fp64 or fp64-pure (default: fp32 on 2-D grids, fp64 on 3-D)\n"
          << "  --resume <kd>       Continue from checkpoint kd in --outdir\n"
          << "  -h, --help          Show this help\n";
 }
@@ -395,7 +397,7 @@ int run_misfit_cli(int argc, char **argv) {
     p.grainy = o.grainy;
     p.grainz = o.grainz;
     p.seed = o.seed;
-    p.precision = o.precision;
+    p.precision = o.precision >= 0 ? o.precision : (N == 1 ? PFC_PRECISION_FP32 : PFC_PRECISION_FP64);
     RunGuard g;
     if (pfc_run_create(&p, &g.r) != PFC_OK) return gpu_fail("run setup");
     pfc_run *r = g.r;
@@ -464,6 +466,7 @@ void cvd_usage(const char *argv0) {
          << "  --seed <uint>       Random seed base (default: 20200604)\n"
          << "  --outdir <path>     Output directory (default: current dir)\n"
          << "  --grid <LxMxN>      Grid (default: 256x256x1)\n"
+         << "  --precision <p>     fp32, fp64 or fp64-pure (default: fp32 on 2-D grids, fp64 on 3-D)\n"
          << "  --resume <kd>       Continue from checkpoint kd in --outdir\n"
          << "  -h, --help          Show this help\n";
 }
@@ -575,7 +578,7 @@ int run_cvd_cli(int argc, char **argv) {
     p.dt = o.dt;
     p.dx = o.dx;
     p.seed = o.seed;
-    p.precision = o.precision;
+    p.precision = o.precision >= 0 ? o.precision : (N == 1 ? PFC_PRECISION_FP32 : PFC_PRECISION_FP64);
     RunGuard g;
     if (pfc_run_create(&p, &g.r) != PFC_OK) return gpu_fail("run setup");
     pfc_run *r = g.r;

@@ -189,6 +189,13 @@ def test_cli_fp64_precision_3d(tmp_path):
         vals, _, _ = read_vti(out / f"phi_{kd}_0.vti")
         assert np.abs(vals - fields[f"phi_{kd}"]).max() <= 1e-6
     check_cvd_analysis_files(out, d, (0, 5, 10), 1e-5)
+    # without --precision a 3-D grid runs on the FP64 path (the FP32 path takes 2-D grids)
+    out2 = tmp_path / "cvd3_default"
+    r = run_cli(["--model", "cvd", "--grid", "32x32x8", *meta["args"], "--outdir", str(out2)])
+    assert r.returncode == 0, r.stderr
+    a, _, _ = read_vti(out / "phi_10_0.vti")
+    b, _, _ = read_vti(out2 / "phi_10_0.vti")
+    assert np.array_equal(a, b)
 
 
 def test_cli_batch_file_errors(tmp_path):
