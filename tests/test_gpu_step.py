@@ -121,7 +121,9 @@ def reference_rounding_noise(model, L, M, steps, **kw):
 @pytest.mark.parametrize("model,L,M,steps", [(P.MODEL_MISFIT, 64, 64, 100), (P.MODEL_MISFIT, 128, 128, 25),
                                              (P.MODEL_MISFIT, 256, 256, 25), (P.MODEL_CVD, 64, 64, 20),
                                              (P.MODEL_MISFIT, 128, 64, 25), (P.MODEL_MISFIT, 64, 256, 25),
-                                             (P.MODEL_MISFIT, 512, 512, 20)])
+                                             (P.MODEL_MISFIT, 512, 512, 20), (P.MODEL_MISFIT, 256, 32, 25),
+                                             (P.MODEL_MISFIT, 32, 256, 25), (P.MODEL_CVD, 32, 32, 20),
+                                             (P.MODEL_MISFIT, 2048, 64, 10), (P.MODEL_MISFIT, 64, 2048, 10)])
 def test_fp32_path_matches_fp64_oracle(model, L, M, steps):
     """Absolute 1e-5 against the CPU pure-FP64 oracle before chaotic amplification sets in."""
     r = gpu_run(model, L, M)
