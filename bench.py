@@ -49,6 +49,8 @@ def parse(argv=None):
     ap.add_argument("--no-cvd3d", action="store_true", help="skip the 3-D CVD (256x256x64) step measurement")
     ap.add_argument("--tile-width", type=int, default=0,
                     help="fix the column tile width instead of the autotuner's choice (reproducible profiles)")
+    ap.add_argument("--staging", choices=["auto", "async", "bulk"], default="auto",
+                    help="fix the column kernel's tile staging (cp.async or TMA bulk copies) instead of the autotuner's")
     return ap.parse_args(argv)
 
 
@@ -417,12 +419,15 @@ def run_ours(args):
     G, B = args.grid, args.batch
     if args.tile_width:
         P.set_tile_width(G, G, args.tile_width, device=dev)
+    if args.staging != "auto":
+        P.set_col_staging(G, G, P.STAGE_ASYNC if args.staging == "async" else P.STAGE_BULK, device=dev)
     runs = []
     for i in range(B):
         p = P.default_params(P.MODEL_MISFIT, L=G, M=G, N=1, seed=1000 + i + 100000 * dist.rank, device=dev)
         runs.append(P.Run(p))
     batch = P.Batch(runs)
     tile_w, tile_trials = P.tile_width(G, G, device=dev)  # chosen by the autotuner at the first run
+    stage, stage_trials = P.col_staging(G, G, device=dev)
     batch.advance(max(3, args.warmup))
     dist.barrier()
     clocks = Clocks(dev)
@@ -480,7 +485,9 @@ def run_ours(args):
                    "grid": [G, G, 1], "runs_per_gpu": B, "parallelism": f"replicas x{dist.world}",
                    "l2": "inputs larger than L2 (resident state ~26 MB/run x batch)",
                    "column_tile_width": tile_w,
-                   "autotuner_trials_ms_per_8_steps": {str(k): round(v, 4) for k, v in tile_trials.items()}},
+                   "column_staging": "async" if stage == P.STAGE_ASYNC else "bulk",
+                   "autotuner_trials_ms_per_8_steps": {str(k): {"async": round(a, 4), "bulk": round(b, 4)}
+                                                       for k, (a, b) in stage_trials.items()}},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                      "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes,

@@ -79,17 +79,38 @@ int pfc_run_advance_timed(pfc_run *r, int nsteps, float *ms);
 
 /* Column tile width (packed columns per column-kernel tile, 1..16) that FP32 runs of
  * an L x M grid use on `device`.  The first FP32 run of a grid times each candidate
- * width on the device (a batch of Misfit runs, row and column sweeps, CUDA events) and
- * keeps the fastest for the process; the width changes the speed of a step, not its
- * results.  This call tunes the grid if it has not been tuned, returns the width and,
- * when the pointers are not NULL, the candidates (up to 4) and their trial times (ms per 8
- * steps; *ntrials is 0 when no trial ran).  PFC_AUTOTUNE=0 in the environment keeps
- * the default widths.  (Autotuner of the batched FFT sweeps; the reference uses FFTW
- * and has no counterpart.) */
+ * width with each tile staging method (a batch of Misfit runs, row and column sweeps,
+ * CUDA events) and keeps the fastest pair for the process; neither changes the
+ * results of a step, only its speed.  This call tunes the grid if it has not been
+ * tuned, returns the width and, when the pointers are not NULL, the candidates (up to
+ * 4) and their trial times (ms per 8 steps, the faster staging; *ntrials is 0 when no
+ * trial ran).  PFC_AUTOTUNE=0 in the environment keeps the default widths with bulk
+ * staging.  (Autotuner of the batched FFT sweeps; the reference uses FFTW and has no
+ * counterpart.) */
 int pfc_tile_width(int device, int L, int M, int *width, int *candidates, float *trial_ms, int *ntrials);
-/* Fix the tile width of a grid for the rest of the process (one of the candidates);
- * runs created before keep their own. */
+/* Fix the tile width of a grid for the rest of the process (one of the candidates;
+ * the staging becomes the faster one of that width's trial, bulk without one); runs
+ * created before keep their own. */
 int pfc_set_tile_width(int device, int L, int M, int width);
+
+#define PFC_STAGE_ASYNC 0 /* column kernel stages tiles by 16-byte cp.async copies */
+#define PFC_STAGE_BULK 1  /* ... by one TMA bulk copy per tile, completing on an mbarrier */
+/* Tile staging method (PFC_STAGE_*) that FP32 runs of an L x M grid use, tuning the
+ * grid first if needed; when not NULL, ms_async / ms_bulk receive each candidate
+ * width's trial time with either method (order of pfc_tile_width's candidates). */
+int pfc_col_staging(int device, int L, int M, int *stage, float *ms_async, float *ms_bulk, int *ntrials);
+/* Fix the staging method of a grid for the rest of the process; runs created before
+ * keep their own. */
+int pfc_set_col_staging(int device, int L, int M, int stage);
+
+/* Self-test of the column kernel's tile staging on one device (not a reference
+ * interface; the reference has no device code).  With issue = 1, n complex floats
+ * (even, 2..8192) are staged into shared memory by one TMA bulk copy, waited for on
+ * an mbarrier and written back; *match = 1 when they came back unchanged.  With
+ * issue = 0 no copy is started, so the bounded wait runs out after limit_ms and the
+ * kernel reports it (*timed_out = 1) and returns; the device stays usable.  *ms is
+ * the kernel's device time.  Uses its own fault word, not the device's. */
+int pfc_selftest_tile_stage(int device, int issue, int n, double limit_ms, int *timed_out, int *match, double *ms);
 
 /* Steps taken so far. */
 int pfc_run_steps(const pfc_run *r, int *steps);

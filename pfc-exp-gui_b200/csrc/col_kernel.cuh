@@ -11,15 +11,18 @@
 //   each output is an inverse transform whose first stage reads P through a
 //     multiplier (1, C2A, C2B for phi, MIS:807-810; 1 and the -i k gradients for
 //     con at checkpoints, MIS:884-889) into s, copied s -> HBM (float4).
-// Inputs arrive by asynchronous 16-byte copies (cp.async) into an unpadded staging
-// buffer Q, which a transform's first stage reads directly.  Each load is issued as
-// soon as the previous transform's first stage has consumed Q, so it streams in
-// while that transform, the update and the output transforms run; the next item's
-// phi tile streams in during the current item's con work.  Two CTAs of 256 threads
+// Inputs are staged into an unpadded buffer Q, which a transform's first stage reads
+// directly, by 16-byte cp.async copies (STAGE_ASYNC) or by one TMA bulk copy per tile
+// completing on a shared-memory mbarrier (STAGE_BULK; waits bounded in time, a CTA
+// whose copy does not arrive sets the context's fault word and returns); the
+// autotuner picks the method with the width.  Each load is issued as soon as the
+// previous transform's first stage has consumed Q, so it streams in while that
+// transform, the update and the output transforms run; the next item's phi tile
+// streams in during the current item's con work.  Two CTAs of 256 threads
 // per SM at C*L = 4096 (2 x 100 KB of shared memory, 128 registers); the tile width C
 // of a grid is chosen per device by the autotuner (engine.cu).
 
-// Tile staging (cp_async16, tile_prefetch, tile_wait, Prefetch, tile_out) and the
+// Tile staging (Stager, Prefetch, tile_out) and the
 // ScaleByTable / GradientOf multipliers come from tile_io.cuh.
 
 // Spectrum of the noise field at mode (l, km) of step t.  The reference draws real-space
@@ -57,13 +60,14 @@ __device__ float2 noise_mode(unsigned long long key, int t, int l, int km, int L
     return make_float2(s * rad * cs, conj ? -s * rad * sn : s * rad * sn);
 }
 
-template <int L, int C, int MODE>
+template <int L, int C, int MODE, int STAGE>
 __global__ void __launch_bounds__(ColCfg<L, C>::NT, ColCfg<L, C>::MINB)
-    k_col_step(const RunDesc *__restrict__ runs, int nruns, const float2 *__restrict__ tw) {
+    k_col_step(const RunDesc *__restrict__ runs, int nruns, const float2 *__restrict__ tw, int *fault) {
     constexpr int NT = ColCfg<L, C>::NT;
     constexpr int SPAD = padded_len<C * L>::value;
     typedef RegOut<L, C, NT> RO;  // register scratch the transforms need for their last stage
     extern __shared__ __align__(16) float2 smem[];
+    __shared__ __align__(8) unsigned long long stage_bar;  // completion barrier of the tile copies
     float2 *s = smem;               // FFT scratch
     float2 *Pk = smem + SPAD;       // parked spectrum
     float2 *Q = smem + 2 * SPAD;    // staging buffer (16-byte aligned: 2*SPAD float2)
@@ -72,8 +76,11 @@ __global__ void __launch_bounds__(ColCfg<L, C>::NT, ColCfg<L, C>::MINB)
     float2 b[RO::PER_T][RO::R];
     int item = blockIdx.x;
     if (item >= items) return;
+    typedef Stager<L, C, NT, STAGE> ST;
+    const ST st{smem_u32(&stage_bar), Q};
+    st.init();
     auto tile_of = [&](int it) { return (long)(it % T) * L * C; };
-    tile_prefetch<L, C, NT>(runs[item / T].psi + tile_of(item), Q);
+    st.issue(runs[item / T].psi + tile_of(item));
     for (; item < items; item += gridDim.x) {
         const RunDesc &d = runs[item / T];
         const int H = d.M / 2;
@@ -82,16 +89,19 @@ __global__ void __launch_bounds__(ColCfg<L, C>::NT, ColCfg<L, C>::MINB)
         const int next = item + gridDim.x;
         const float2 *next_psi = next < items ? runs[next / T].psi + tile_of(next) : nullptr;
         const float invL = 1.0f / (float)L;
+        // barrier phase of this item's first wait: an item of the step modes waits four
+        // times (phases 0, 1, 0, 1), a COL_PREPARE item once (the iteration's parity)
+        const unsigned p0 = MODE == COL_PREPARE ? (unsigned)((item - (int)blockIdx.x) / (int)gridDim.x) & 1u : 0u;
         const float mn_dt = d.k.dynamic_mn * d.dt, mc_dt = d.k.dynamic_mc * d.dt;
 
         // ---- phi ----
-        tile_wait();
+        if (!st.wait(p0, fault)) return;
         if (MODE == COL_PREPARE) {
-            fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, Pk, tw, b, Identity(), Prefetch<L, C, NT>{next_psi, Q});
+            fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, Pk, tw, b, Identity(), Prefetch<ST>{st, next_psi});
         } else {
-            fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, Pk, tw, b, Identity(), Prefetch<L, C, NT>{d.inn + tile, Q});
-            tile_wait();
-            fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, s, tw, b, Identity(), Prefetch<L, C, NT>{d.con + tile, Q});
+            fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, Pk, tw, b, Identity(), Prefetch<ST>{st, d.inn + tile});
+            if (!st.wait(1u, fault)) return;
+            fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, s, tw, b, Identity(), Prefetch<ST>{st, d.con + tile});
         }
         const int nstep = (MODE != COL_PREPARE && d.noise_amp != 0.0f) ? *d.step_ctr : -1;
         for (int e = threadIdx.x; e < L * C; e += NT) {
@@ -133,10 +143,10 @@ __global__ void __launch_bounds__(ColCfg<L, C>::NT, ColCfg<L, C>::MINB)
         if (MODE == COL_PREPARE) continue;
 
         // ---- con ----
-        tile_wait();
-        fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, Pk, tw, b, Identity(), Prefetch<L, C, NT>{d.inc + tile, Q});
-        tile_wait();
-        fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, s, tw, b, Identity(), Prefetch<L, C, NT>{next_psi, Q});
+        if (!st.wait(0u, fault)) return;
+        fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, Pk, tw, b, Identity(), Prefetch<ST>{st, d.inc + tile});
+        if (!st.wait(1u, fault)) return;
+        fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, s, tw, b, Identity(), Prefetch<ST>{st, next_psi});
         for (int e = threadIdx.x; e < L * C; e += NT) {
             const int l = e / C, c = e % C, km = km0 + c;
             const int pi = spad(e);
@@ -158,5 +168,5 @@ __global__ void __launch_bounds__(ColCfg<L, C>::NT, ColCfg<L, C>::MINB)
             tile_out<L, C, NT>(s, d.gy + tile);
         }
     }
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");  // no copy outlives the CTA
+    st.finish();  // every copy issued has been waited for: the last item issues none (next_psi = null)
 }

@@ -53,6 +53,12 @@ static constexpr double PI_REF = 3.1415926;  // pfc_common.h:152
 static std::mutex g_ctx_mu;
 static std::map<int, Context *> g_ctx;
 
+int fault_status(const Context *c) {
+    if (c && c->fault && *c->fault != 0)
+        return set_error(PFC_E_CUDA, "column kernel: a tile copy did not arrive within its bounded wait");
+    return PFC_OK;
+}
+
 int get_context(int device, Context **out) {
     std::lock_guard<std::mutex> lk(g_ctx_mu);
     auto it = g_ctx.find(device);
@@ -69,6 +75,14 @@ int get_context(int device, Context **out) {
     Context *c = new Context();
     c->device = device;
     PFC_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    {
+        int *f = nullptr, *fd = nullptr;
+        PFC_CUDA_TRY(cudaHostAlloc(reinterpret_cast<void **>(&f), sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable));
+        *f = 0;
+        PFC_CUDA_TRY(cudaHostGetDevicePointer(reinterpret_cast<void **>(&fd), f, 0));
+        c->fault = f;
+        c->tw.fault = fd;
+    }
     // twiddles for n = 2^1 .. 2^11 in the stage layout of the transforms (twiddle_offset,
     // fft_core.cuh): stage (Ns, R) entry k*R + r = exp(-2 pi i j / n), j = r*k*n/(Ns*R),
     // in double, rounded once for FP32.  Each length gets 2n entries (enough for every
@@ -367,11 +381,11 @@ static void free_run(pfc_run *r) {
     delete r;
 }
 
-static int tile_width_for(int device, int L, int M, int *width);
+static int tile_width_for(int device, int L, int M, int *width, int *stage);
 
 // Create a run; ct_force > 0 fixes the column tile width of an FP32 run (the
 // autotuner's trial runs), 0 takes the grid's tuned width.
-static int run_create(const pfc_run_params *p, int ct_force, pfc_run **out) {
+static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pfc_run **out) {
     if (!p || !out) return set_error(PFC_E_INVALID, "null argument");
     *out = nullptr;
     if (p->model != PFC_MODEL_MISFIT && p->model != PFC_MODEL_CVD) return set_error(PFC_E_INVALID, "unknown model");
@@ -394,12 +408,13 @@ static int run_create(const pfc_run_params *p, int ct_force, pfc_run **out) {
     int rc = get_context(p->device, &ctx);
     if (rc != PFC_OK) return rc;
     PFC_CUDA_TRY(cudaSetDevice(p->device));
-    int ct = col_tile_width(p->L);
+    int ct = col_tile_width(p->L), stage = COL_STAGE_BULK;
     if (p->precision == PFC_PRECISION_FP32) {
         if (ct_force > 0) {
             ct = ct_force;
+            stage = stage_force;
         } else {
-            rc = tile_width_for(p->device, p->L, p->M, &ct);
+            rc = tile_width_for(p->device, p->L, p->M, &ct, &stage);
             if (rc != PFC_OK) return rc;
         }
     }
@@ -470,6 +485,7 @@ static int run_create(const pfc_run_params *p, int ct_force, pfc_run **out) {
     d.N = r->N;
     d.Hp = r->Hp;
     d.CT = ct;
+    d.stage = stage;
     d.lct = 0;
     while ((1 << d.lct) < d.CT) ++d.lct;
     d.T = r->Hp / d.CT;
@@ -510,30 +526,40 @@ static int run_create(const pfc_run_params *p, int ct_force, pfc_run **out) {
     return PFC_OK;
 }
 
-extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) { return run_create(p, 0, out); }
+extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) { return run_create(p, 0, 0, out); }
 
 // ---------------------------------------------------------------------------
-// Autotuner: the column tile width of FP32 runs of an L x M grid.  A run's row-space
-// layout and its column kernel's tile both follow the width; every column's transform
-// is the same arithmetic whatever the width, so the choice changes speed, not results.
-// On the first FP32 run of a grid on a device, each candidate width
-// (col_tile_candidates: the default, a quarter, half and twice it, where the tile fits) runs a
-// batch of Misfit runs of at least 2 M points in all (4 to 16 runs): 3 warm-up steps,
-// then 8 steps of the row and column sweeps timed with CUDA events.  The fastest
-// width is kept for the rest of the process.  PFC_AUTOTUNE=0 in the environment keeps
-// the default widths; pfc_set_tile_width fixes one.
+// Autotuner: the column tile width of FP32 runs of an L x M grid, and how the column
+// kernel stages its input tiles.  A run's row-space layout and its column kernel's tile
+// both follow the width; every column's transform is the same arithmetic whatever the
+// width or the staging, so the choice changes speed, not results.  On the first FP32
+// run of a grid on a device, each candidate width (col_tile_candidates: the default, a
+// quarter, half and twice it, where the tile fits) runs a batch of Misfit runs of at
+// least 2 M points in all (4 to 16 runs) with each staging method: 3 warm-up steps,
+// then 8 steps of the row and column sweeps timed with CUDA events.  The fastest pair
+// is kept for the rest of the process.  PFC_AUTOTUNE=0 in the environment keeps the
+// default width with bulk-copy staging; pfc_set_tile_width and pfc_set_col_staging fix
+// them.
 // ---------------------------------------------------------------------------
 struct TileChoice {
     int width = 0;
+    int stage = COL_STAGE_BULK;
     int n = 0;
     int cand[4] = {0, 0, 0, 0};
-    float ms[4] = {0.f, 0.f, 0.f, 0.f};
+    float ms[4][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};  // [candidate][staging]
+    // fastest staging of a candidate width
+    int best_stage(int w) const {
+        for (int i = 0; i < n; ++i)
+            if (cand[i] == w) return ms[i][COL_STAGE_ASYNC] < ms[i][COL_STAGE_BULK] ? COL_STAGE_ASYNC : COL_STAGE_BULK;
+        return COL_STAGE_BULK;
+    }
 };
 static std::mutex g_tile_mu;
 static std::map<std::tuple<int, int, int>, TileChoice> g_tile;
 
-// Device time of 8 steps of a trial batch with tile width ct.
-static int time_tile_width(int device, int L, int M, int ct, float *ms) {
+// Device time of 8 steps of a trial batch with tile width ct, for each staging method
+// (ms[COL_STAGE_ASYNC], ms[COL_STAGE_BULK]).
+static int time_tile_width(int device, int L, int M, int ct, float ms[2]) {
     const long pts = (long)L * M;
     const int nruns = (int)std::max(4L, std::min(16L, (2L << 20) / pts));
     std::vector<pfc_run *> runs;
@@ -546,7 +572,7 @@ static int time_tile_width(int device, int L, int M, int ct, float *ms) {
         p.device = device;
         p.seed = 1000u + (uint32_t)i;
         pfc_run *r = nullptr;
-        rc = run_create(&p, ct, &r);
+        rc = run_create(&p, ct, COL_STAGE_BULK, &r);
         if (rc == PFC_OK) runs.push_back(r);
     }
     RunDesc *d = nullptr;
@@ -557,23 +583,26 @@ static int time_tile_width(int device, int L, int M, int ct, float *ms) {
         for (auto *r : runs) h.push_back(r->desc);
         cudaStream_t st = runs[0]->stream;
         const TwiddleSet &tw = runs[0]->ctx->tw;
-        auto step = [&]() {
+        auto step = [&](int stage) {
             cudaError_t x = launch_row_step(d, n, L, M, tw, st);
-            if (x == cudaSuccess) x = launch_col_step(d, n, L, M, ct, COL_STEP, tw, st);
+            if (x == cudaSuccess) x = launch_col_step(d, n, L, M, ct, stage, COL_STEP, tw, st);
             return x;
         };
         cudaError_t ce = cudaMalloc(&d, h.size() * sizeof(RunDesc));
         if (ce == cudaSuccess) ce = cudaMemcpyAsync(d, h.data(), h.size() * sizeof(RunDesc), cudaMemcpyHostToDevice, st);
         if (ce == cudaSuccess) ce = cudaEventCreate(&e0);
         if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
-        for (int i = 0; i < 3 && ce == cudaSuccess; ++i) ce = step();
-        if (ce == cudaSuccess) ce = cudaEventRecord(e0, st);
-        for (int i = 0; i < 8 && ce == cudaSuccess; ++i) ce = step();
-        if (ce == cudaSuccess) ce = cudaEventRecord(e1, st);
-        if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
-        if (ce == cudaSuccess) ce = cudaEventElapsedTime(ms, e0, e1);
+        for (int stage = COL_STAGE_ASYNC; stage <= COL_STAGE_BULK && ce == cudaSuccess; ++stage) {
+            for (int i = 0; i < 3 && ce == cudaSuccess; ++i) ce = step(stage);
+            if (ce == cudaSuccess) ce = cudaEventRecord(e0, st);
+            for (int i = 0; i < 8 && ce == cudaSuccess; ++i) ce = step(stage);
+            if (ce == cudaSuccess) ce = cudaEventRecord(e1, st);
+            if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+            if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms[stage], e0, e1);
+        }
         if (ce == cudaErrorMemoryAllocation) rc = set_error(PFC_E_NOMEM, "tile width trial: out of memory");
         else if (ce != cudaSuccess) rc = cuda_error(ce, "tile width trial");
+        if (rc == PFC_OK) rc = fault_status(runs[0]->ctx);
     }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
@@ -582,12 +611,13 @@ static int time_tile_width(int device, int L, int M, int ct, float *ms) {
     return rc;
 }
 
-static int tile_width_for(int device, int L, int M, int *width) {
+static int tile_width_for(int device, int L, int M, int *width, int *stage) {
     std::lock_guard<std::mutex> lk(g_tile_mu);
     const auto key = std::make_tuple(device, L, M);
     auto it = g_tile.find(key);
     if (it != g_tile.end()) {
         *width = it->second.width;
+        *stage = it->second.stage;
         return PFC_OK;
     }
     TileChoice c;
@@ -595,27 +625,31 @@ static int tile_width_for(int device, int L, int M, int *width) {
     int cand[4];
     const int nc = col_tile_candidates(L, cand);
     const char *env = std::getenv("PFC_AUTOTUNE");
-    if (nc > 1 && !(env && env[0] == '0')) {
+    if (!(env && env[0] == '0')) {
         float best = 0.f;
         for (int i = 0; i < nc; ++i) {
-            float ms = 0.f;
-            const int rc = time_tile_width(device, L, M, cand[i], &ms);
-            if (rc == PFC_E_NOMEM) {  // no room for trial runs: keep the default width
+            float ms[2] = {0.f, 0.f};
+            const int rc = time_tile_width(device, L, M, cand[i], ms);
+            if (rc == PFC_E_NOMEM) {  // no room for trial runs: keep the defaults
                 c = TileChoice{};
                 c.width = col_tile_width(L);
                 break;
             }
             if (rc != PFC_OK) return rc;
             c.cand[c.n] = cand[i];
-            c.ms[c.n++] = ms;
-            if (i == 0 || ms < best) {
-                best = ms;
-                c.width = cand[i];
-            }
+            c.ms[c.n][0] = ms[0];
+            c.ms[c.n++][1] = ms[1];
+            for (int s = COL_STAGE_ASYNC; s <= COL_STAGE_BULK; ++s)
+                if ((i == 0 && s == COL_STAGE_ASYNC) || ms[s] < best) {
+                    best = ms[s];
+                    c.width = cand[i];
+                    c.stage = s;
+                }
         }
     }
     g_tile[key] = c;
     *width = c.width;
+    *stage = c.stage;
     return PFC_OK;
 }
 
@@ -626,15 +660,95 @@ extern "C" int pfc_tile_width(int device, int L, int M, int *width, int *candida
     int rc = get_context(device, &ctx);
     if (rc != PFC_OK) return rc;
     PFC_CUDA_TRY(cudaSetDevice(device));
-    rc = tile_width_for(device, L, M, width);
+    int stage = 0;
+    rc = tile_width_for(device, L, M, width, &stage);
     if (rc != PFC_OK) return rc;
     std::lock_guard<std::mutex> lk(g_tile_mu);
     const TileChoice &c = g_tile[std::make_tuple(device, L, M)];
     if (ntrials) *ntrials = c.n;
     for (int i = 0; i < c.n; ++i) {
         if (candidates) candidates[i] = c.cand[i];
-        if (trial_ms) trial_ms[i] = c.ms[i];
+        if (trial_ms) trial_ms[i] = std::min(c.ms[i][0], c.ms[i][1]);
     }
+    return PFC_OK;
+}
+
+extern "C" int pfc_col_staging(int device, int L, int M, int *stage, float *ms_async, float *ms_bulk, int *ntrials) {
+    if (!stage) return set_error(PFC_E_INVALID, "null argument");
+    if (!is_supported_len(L) || !is_supported_len(M)) return set_error(PFC_E_INVALID, "unsupported grid");
+    Context *ctx = nullptr;
+    int rc = get_context(device, &ctx);
+    if (rc != PFC_OK) return rc;
+    PFC_CUDA_TRY(cudaSetDevice(device));
+    int width = 0;
+    rc = tile_width_for(device, L, M, &width, stage);
+    if (rc != PFC_OK) return rc;
+    std::lock_guard<std::mutex> lk(g_tile_mu);
+    const TileChoice &c = g_tile[std::make_tuple(device, L, M)];
+    if (ntrials) *ntrials = c.n;
+    for (int i = 0; i < c.n; ++i) {
+        if (ms_async) ms_async[i] = c.ms[i][COL_STAGE_ASYNC];
+        if (ms_bulk) ms_bulk[i] = c.ms[i][COL_STAGE_BULK];
+    }
+    return PFC_OK;
+}
+
+extern "C" int pfc_set_col_staging(int device, int L, int M, int stage) {
+    if (!is_supported_len(L) || !is_supported_len(M)) return set_error(PFC_E_INVALID, "unsupported grid");
+    if (stage != COL_STAGE_ASYNC && stage != COL_STAGE_BULK) return set_error(PFC_E_INVALID, "unknown staging");
+    std::lock_guard<std::mutex> lk(g_tile_mu);
+    auto it = g_tile.find(std::make_tuple(device, L, M));
+    if (it == g_tile.end()) {
+        TileChoice c;
+        c.width = col_tile_width(L);
+        it = g_tile.emplace(std::make_tuple(device, L, M), c).first;
+    }
+    it->second.stage = stage;  // a trial record, if any, is kept
+    return PFC_OK;
+}
+
+extern "C" int pfc_selftest_tile_stage(int device, int issue, int n, double limit_ms, int *timed_out, int *match,
+                                       double *ms) {
+    if (!timed_out || !match || !ms) return set_error(PFC_E_INVALID, "null argument");
+    if (n < 2 || n > 8192 || (n & 1) || !(limit_ms > 0.0) || limit_ms > 10000.0)
+        return set_error(PFC_E_INVALID, "n must be even in [2, 8192] and limit_ms in (0, 10000]");
+    Context *c = nullptr;
+    int rc = get_context(device, &c);
+    if (rc != PFC_OK) return rc;
+    PFC_CUDA_TRY(cudaSetDevice(device));
+    std::vector<float2> h(n), back(n, make_float2(0.f, 0.f));
+    for (int i = 0; i < n; ++i) h[i] = make_float2((float)i + 0.25f, -(float)(3 * i) - 0.5f);
+    float2 *d = nullptr;
+    int *f = nullptr, *fd = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaMalloc(&d, 2 * sizeof(float2) * n);
+    if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void **>(&f), sizeof(int), cudaHostAllocMapped);
+    if (e == cudaSuccess) {
+        *(volatile int *)f = 0;
+        e = cudaHostGetDevicePointer(reinterpret_cast<void **>(&fd), f, 0);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d, h.data(), sizeof(float2) * n, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d + n, 0, sizeof(float2) * n, c->stream);
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, c->stream);
+    if (e == cudaSuccess)
+        e = launch_stage_selftest(d, d + n, n, issue ? 1 : 0, (unsigned long long)(limit_ms * 1e6), fd, c->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(back.data(), d + n, sizeof(float2) * n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    float t = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+    if (e == cudaSuccess) {
+        *timed_out = *(volatile int *)f != 0 ? 1 : 0;
+        *match = std::memcmp(back.data(), h.data(), sizeof(float2) * n) == 0 ? 1 : 0;
+        *ms = t;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (f) cudaFreeHost(f);
+    if (d) cudaFree(d);
+    if (e != cudaSuccess) return cuda_error(e, "pfc_selftest_tile_stage");
     return PFC_OK;
 }
 
@@ -646,7 +760,9 @@ extern "C" int pfc_set_tile_width(int device, int L, int M, int width) {
     for (int i = 0; i < nc; ++i) ok = ok || cand[i] == width;
     if (!ok) return set_error(PFC_E_INVALID, "tile width not available for this grid");
     std::lock_guard<std::mutex> lk(g_tile_mu);
-    g_tile[std::make_tuple(device, L, M)].width = width;  // a trial record, if any, is kept
+    TileChoice &c = g_tile[std::make_tuple(device, L, M)];
+    c.width = width;  // a trial record, if any, is kept
+    c.stage = c.best_stage(width);
     return PFC_OK;
 }
 
@@ -749,8 +865,9 @@ static int fp32_from_real(pfc_run *r, bool means_from_device) {
     r->step_ctr_init = r->t - 1;
     PFC_CUDA_TRY(cudaMemcpyAsync(d.step_ctr, &r->step_ctr_init, sizeof(int), cudaMemcpyHostToDevice, r->stream));
     PFC_CUDA_TRY(launch_row_forward(r->d_desc, 1, r->L, r->M, r->ctx->tw, r->stream));
-    PFC_CUDA_TRY(launch_col_step(r->d_desc, 1, r->L, r->M, r->desc.CT, COL_PREPARE, r->ctx->tw, r->stream));
-    PFC_CUDA_TRY(cudaStreamSynchronize(r->stream));
+    PFC_CUDA_TRY(
+        launch_col_step(r->d_desc, 1, r->L, r->M, r->desc.CT, r->desc.stage, COL_PREPARE, r->ctx->tw, r->stream));
+    PFC_SYNC_CHECKED(r->ctx, r->stream);
     r->fields_valid = true;
     r->energy_valid = false;
     return PFC_OK;
@@ -777,9 +894,8 @@ static int fp32_advance(pfc_run *r, int nsteps, int analysis) {
     for (int i = 0; i < nsteps; ++i) {
         const bool last = i == nsteps - 1;
         PFC_CUDA_TRY(launch_row_step(r->d_desc, 1, r->L, r->M, r->ctx->tw, r->stream));
-        PFC_CUDA_TRY(launch_col_step(r->d_desc, 1, r->L, r->M, r->desc.CT,
-                                     (last && analysis) ? COL_STEP_CHECKPOINT : COL_STEP,
-                                     r->ctx->tw, r->stream));
+        PFC_CUDA_TRY(launch_col_step(r->d_desc, 1, r->L, r->M, r->desc.CT, r->desc.stage,
+                                     (last && analysis) ? COL_STEP_CHECKPOINT : COL_STEP, r->ctx->tw, r->stream));
     }
     r->t += nsteps;
     r->fields_valid = false;
@@ -818,7 +934,7 @@ extern "C" int pfc_run_advance_timed(pfc_run *r, int nsteps, float *ms) {
     cudaEventDestroy(e1);
     if (rc != PFC_OK) return rc;
     if (e != cudaSuccess) return cuda_error(e, "pfc_run_advance_timed");
-    return PFC_OK;
+    return fault_status(r->ctx);
 }
 
 extern "C" int pfc_run_steps(const pfc_run *r, int *steps) {
@@ -843,7 +959,7 @@ extern "C" int pfc_run_get_fields_f32(pfc_run *r, float *phi, float *con) {
     if (rc != PFC_OK) return rc;
     if (phi) PFC_CUDA_TRY(cudaMemcpyAsync(phi, r->desc.psi_real, r->P * sizeof(float), cudaMemcpyDeviceToHost, r->stream));
     if (con) PFC_CUDA_TRY(cudaMemcpyAsync(con, r->desc.con_real, r->P * sizeof(float), cudaMemcpyDeviceToHost, r->stream));
-    PFC_CUDA_TRY(cudaStreamSynchronize(r->stream));
+    PFC_SYNC_CHECKED(r->ctx, r->stream);
     return PFC_OK;
 }
 
@@ -948,7 +1064,7 @@ extern "C" int pfc_run_energy(pfc_run *r, double *e_over_p, double *mass_over_p)
     if (!r->energy_valid) return set_error(PFC_E_STATE, "energy is available after pfc_run_advance(..., analysis=1)");
     double s[2];
     PFC_CUDA_TRY(cudaMemcpyAsync(s, r->d_scratch, sizeof(s), cudaMemcpyDeviceToHost, r->stream));
-    PFC_CUDA_TRY(cudaStreamSynchronize(r->stream));
+    PFC_SYNC_CHECKED(r->ctx, r->stream);
     if (e_over_p) *e_over_p = s[0] / r->L / r->M / r->N;
     if (mass_over_p) *mass_over_p = s[1] / r->L / r->M / r->N;
     return PFC_OK;
@@ -966,7 +1082,7 @@ extern "C" int pfc_run_means(const pfc_run *r, double *phi_mean, double *con_mea
 // captured once into a CUDA graph per step count.
 // ---------------------------------------------------------------------------
 struct SizeClass {
-    int L, M, CT;
+    int L, M, CT, stage;
     std::vector<pfc_run *> runs;
     RunDesc *d_descs = nullptr;
 };
@@ -997,9 +1113,11 @@ extern "C" int pfc_batch_create(pfc_run *const *runs, int nruns, pfc_batch **out
     for (int i = 0; i < nruns; ++i) {
         SizeClass *sc = nullptr;
         for (auto &c : b->classes)
-            if (c.L == runs[i]->L && c.M == runs[i]->M && c.CT == runs[i]->desc.CT) sc = &c;
+            if (c.L == runs[i]->L && c.M == runs[i]->M && c.CT == runs[i]->desc.CT && c.stage == runs[i]->desc.stage)
+                sc = &c;
         if (!sc) {
-            b->classes.push_back(SizeClass{runs[i]->L, runs[i]->M, runs[i]->desc.CT, {}, nullptr});
+            b->classes.push_back(
+                SizeClass{runs[i]->L, runs[i]->M, runs[i]->desc.CT, runs[i]->desc.stage, {}, nullptr});
             sc = &b->classes.back();
         }
         sc->runs.push_back(runs[i]);
@@ -1034,7 +1152,8 @@ static int batch_enqueue(pfc_batch *b, int nsteps) {
             PFC_CUDA_TRY(launch_row_step(c.d_descs, (int)c.runs.size(), c.L, c.M, b->ctx->tw, b->stream));
         for (auto &c : b->classes)
             PFC_CUDA_TRY(
-                launch_col_step(c.d_descs, (int)c.runs.size(), c.L, c.M, c.CT, COL_STEP, b->ctx->tw, b->stream));
+                launch_col_step(c.d_descs, (int)c.runs.size(), c.L, c.M, c.CT, c.stage, COL_STEP, b->ctx->tw,
+                                b->stream));
     }
     return PFC_OK;
 }
@@ -1057,7 +1176,7 @@ extern "C" int pfc_batch_advance_timed(pfc_batch *b, int nsteps, float *ms) {
     cudaEventDestroy(e1);
     if (rc != PFC_OK) return rc;
     if (e != cudaSuccess) return cuda_error(e, "pfc_batch_advance_timed");
-    return PFC_OK;
+    return fault_status(b->ctx);
 }
 
 // Per-kernel device times: reps steps, each row-kernel and column-kernel launch
@@ -1075,10 +1194,11 @@ extern "C" int pfc_batch_kernel_times(pfc_batch *b, int reps, double *row_ms, do
         PFC_CUDA_TRY(cudaEventRecord(ev[3 * i + 1], b->stream));
         for (auto &c : b->classes)
             PFC_CUDA_TRY(
-                launch_col_step(c.d_descs, (int)c.runs.size(), c.L, c.M, c.CT, COL_STEP, b->ctx->tw, b->stream));
+                launch_col_step(c.d_descs, (int)c.runs.size(), c.L, c.M, c.CT, c.stage, COL_STEP, b->ctx->tw,
+                                b->stream));
         PFC_CUDA_TRY(cudaEventRecord(ev[3 * i + 2], b->stream));
     }
-    PFC_CUDA_TRY(cudaStreamSynchronize(b->stream));
+    PFC_SYNC_CHECKED(b->ctx, b->stream);
     double rs = 0.0, cs = 0.0;
     for (int i = 0; i < reps; ++i) {
         float a = 0.f, c = 0.f;
@@ -1111,7 +1231,7 @@ extern "C" int pfc_batch_advance(pfc_batch *b, int nsteps) {
             b->graph = nullptr;
         }
         // kernel attribute setup (max dynamic shared memory) happens outside the capture
-        for (auto &c : b->classes) PFC_CUDA_TRY(prepare_size(c.L, c.M, c.CT));
+        for (auto &c : b->classes) PFC_CUDA_TRY(prepare_size(c.L, c.M, c.CT, c.stage));
         int rc = PFC_OK;
         cudaGraph_t g = nullptr;
         PFC_CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));

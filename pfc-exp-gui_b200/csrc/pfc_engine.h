@@ -23,6 +23,8 @@ struct Context {
     std::mutex stage_mu;
     float *stage = nullptr;
     size_t stage_floats = 0;
+    // host view of tw.fault (mapped pinned memory); sticky once a kernel sets it
+    volatile int *fault = nullptr;
 };
 
 int set_error(int code, const std::string &msg);
@@ -33,6 +35,16 @@ int cuda_error(cudaError_t e, const char *what);
     do {                                                            \
         cudaError_t _e = (expr);                                    \
         if (_e != cudaSuccess) return pfc::cuda_error(_e, #expr);   \
+    } while (0)
+// PFC_OK, or PFC_E_CUDA when a kernel of the context has set its fault word (read
+// after the context's work has been synchronised)
+int fault_status(const Context *c);
+// synchronise a stream, then report a CUDA error or the context's fault word
+#define PFC_SYNC_CHECKED(ctx, stream)                                          \
+    do {                                                                       \
+        PFC_CUDA_TRY(cudaStreamSynchronize(stream));                           \
+        const int _rc = pfc::fault_status(ctx);                                \
+        if (_rc != PFC_OK) return _rc;                                         \
     } while (0)
 int get_context(int device, Context **out);
 void model_coefs(int model, ModelCoefs *k);
@@ -76,5 +88,5 @@ int fp64_get_fields(pfc_run *r, double *phi, double *con);
 int fp64_set_fields(pfc_run *r, const double *phi, const double *con);
 int fp64_energy(pfc_run *r, double *e_over_p, double *mass_over_p);
 // Kernel attribute setup for one grid size (must precede graph capture).
-cudaError_t prepare_size(int L, int M, int C);
+cudaError_t prepare_size(int L, int M, int C, int stage);
 }  // namespace pfc

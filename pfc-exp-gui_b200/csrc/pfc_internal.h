@@ -36,6 +36,7 @@ struct RunDesc {
     int L, M, N;      // grid (N = 1 for 2-D)
     int Hp;           // padded number of packed columns (T * CT >= M/2 + 1)
     int CT, lct, T;   // column-tile width (power of two), its log2, number of tiles
+    int stage;        // column-kernel tile staging (ColStage; a launch choice, results do not depend on it)
     int model;
     // row-space arrays, T tiles of [L][CT] float2 each: (l, km) at ((km/CT)*L + l)*CT + km%CT
     float2 *psi, *con, *ca, *cb, *inn, *inc, *gx, *gy;
@@ -65,17 +66,22 @@ struct RunDesc {
     int *step_ctr;
 };
 
-// Twiddle tables exp(-2 pi i j / n) for n = 2^1 .. 2^11, FP32 and FP64.
+// Twiddle tables exp(-2 pi i j / n) for n = 2^1 .. 2^11, FP32 and FP64, and the
+// context's fault word: a device-visible int in mapped pinned host memory that a
+// kernel sets to nonzero when one of its bounded waits gives up (the host reads it
+// after synchronising and reports PFC_E_CUDA).
 struct TwiddleSet {
     const float2 *f32[12];
     const double2 *f64[12];
+    int *fault;
 };
 
 // FP32 fused step (step_fp32.cu).  All runs of one call share (L, M).
 cudaError_t launch_row_step(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw, cudaStream_t s);
-// C: column tile width of the runs' layout (RunDesc::CT, the same for all nruns runs)
-cudaError_t launch_col_step(const RunDesc *d_runs, int nruns, int L, int M, int C, int mode, const TwiddleSet &tw,
-                            cudaStream_t s);
+// C: column tile width of the runs' layout (RunDesc::CT, the same for all nruns runs);
+// stage: how input tiles are staged (COL_STAGE_*; the results do not depend on it)
+cudaError_t launch_col_step(const RunDesc *d_runs, int nruns, int L, int M, int C, int stage, int mode,
+                            const TwiddleSet &tw, cudaStream_t s);
 cudaError_t launch_row_forward(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw, cudaStream_t s);
 cudaError_t launch_row_analysis(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw,
                                 cudaStream_t s);
@@ -90,6 +96,15 @@ cudaError_t launch_build_kcoef(const RunDesc *d_run, float2 *kden, float2 *kc2, 
 
 // column-kernel modes
 enum ColMode : int { COL_STEP = 0, COL_PREPARE = 1, COL_STEP_CHECKPOINT = 2 };
+// column-kernel tile staging: 16-byte cp.async copies, or one TMA bulk copy per tile
+// completing on an mbarrier (tile_io.cuh)
+enum ColStage : int { COL_STAGE_ASYNC = 0, COL_STAGE_BULK = 1 };
+
+// Self-test of the column kernel's tile staging (k_stage_selftest): n float2 (even,
+// <= 8192) staged from src by one bulk copy and written back to dst, or, without
+// issue, a wait that runs out after limit_ns and sets *fault.
+cudaError_t launch_stage_selftest(const float2 *src, float2 *dst, int n, int issue, unsigned long long limit_ns,
+                                  int *fault, cudaStream_t s);
 
 // Kernel attribute setup (before graph capture) of the row kernels of row length M.
 cudaError_t prepare_rows(int M);

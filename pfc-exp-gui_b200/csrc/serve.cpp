@@ -92,7 +92,7 @@ int steps_to_event(const Job &j) {
 }
 
 struct Cohort {
-    int model = 0, L = 0, M = 0, CT = 0;  // runs of one model, grid and column tile width
+    int model = 0, L = 0, M = 0, CT = 0, stage = 0;  // runs of one model, grid, column tile width and staging
     std::vector<Job *> jobs;
     RunDesc *d_descs = nullptr;
     double *d_ehist = nullptr;  // [n][SEG][2] (CVD)
@@ -211,7 +211,9 @@ int build_cohorts(pfc_engine *e) {
     for (Job *j : e->active) {
         Cohort *c = nullptr;
         for (auto &x : e->cohorts)
-            if (x.model == j->spec.kind && x.L == j->L && x.M == j->M && x.CT == j->run->desc.CT) c = &x;
+            if (x.model == j->spec.kind && x.L == j->L && x.M == j->M && x.CT == j->run->desc.CT &&
+                x.stage == j->run->desc.stage)
+                c = &x;
         if (!c) {
             e->cohorts.push_back(Cohort{});
             c = &e->cohorts.back();
@@ -219,6 +221,7 @@ int build_cohorts(pfc_engine *e) {
             c->L = j->L;
             c->M = j->M;
             c->CT = j->run->desc.CT;
+            c->stage = j->run->desc.stage;
         }
         c->jobs.push_back(j);
     }
@@ -237,7 +240,7 @@ int build_cohorts(pfc_engine *e) {
             h[i].ehist = c.d_ehist ? c.d_ehist + (size_t)i * SEG * 2 : nullptr;
         }
         PFC_CUDA_TRY(cudaMemcpyAsync(c.d_descs, h.data(), n * sizeof(RunDesc), cudaMemcpyHostToDevice, e->main));
-        PFC_CUDA_TRY(prepare_size(c.L, c.M, c.CT));
+        PFC_CUDA_TRY(prepare_size(c.L, c.M, c.CT, c.stage));
         cudaEvent_t ev;
         PFC_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         e->join_events.push_back(ev);
@@ -264,9 +267,9 @@ int cohort_step(pfc_engine *e, Cohort &c, int slot, cudaStream_t st) {
     const TwiddleSet &tw = e->ctx->tw;
     PFC_CUDA_TRY(launch_row_step(c.d_descs, n, c.L, c.M, tw, st));
     if (c.model == PFC_JOB_MISFIT) {
-        PFC_CUDA_TRY(launch_col_step(c.d_descs, n, c.L, c.M, c.CT, COL_STEP, tw, st));
+        PFC_CUDA_TRY(launch_col_step(c.d_descs, n, c.L, c.M, c.CT, c.stage, COL_STEP, tw, st));
     } else {
-        PFC_CUDA_TRY(launch_col_step(c.d_descs, n, c.L, c.M, c.CT, COL_STEP_CHECKPOINT, tw, st));
+        PFC_CUDA_TRY(launch_col_step(c.d_descs, n, c.L, c.M, c.CT, c.stage, COL_STEP_CHECKPOINT, tw, st));
         PFC_CUDA_TRY(launch_row_analysis(c.d_descs, n, c.L, c.M, tw, st));
         PFC_CUDA_TRY(launch_reduce_runs(c.d_descs, n, analysis_partials(c.L, c.M), slot, st));
     }
@@ -355,7 +358,7 @@ int copy_fields(pfc_engine *e, Job *j, std::shared_ptr<std::vector<float>> &phi,
     con = std::make_shared<std::vector<float>>(P);
     PFC_CUDA_TRY(cudaMemcpyAsync(phi->data(), j->run->desc.psi_real, P * sizeof(float), cudaMemcpyDeviceToHost, e->main));
     PFC_CUDA_TRY(cudaMemcpyAsync(con->data(), j->run->desc.con_real, P * sizeof(float), cudaMemcpyDeviceToHost, e->main));
-    PFC_CUDA_TRY(cudaStreamSynchronize(e->main));
+    PFC_SYNC_CHECKED(e->ctx, e->main);
     return PFC_OK;
 }
 
@@ -614,15 +617,15 @@ int quantum(pfc_engine *e) {
             PFC_CUDA_TRY(launch_row_step(c.d_descs, (int)c.jobs.size(), c.L, c.M, tw, e->main));
             for (Job *j : c.jobs) {
                 const bool ck = std::find(ckpt.begin(), ckpt.end(), j) != ckpt.end();
-                PFC_CUDA_TRY(
-                    launch_col_step(j->run->d_desc, 1, c.L, c.M, c.CT, ck ? COL_STEP_CHECKPOINT : COL_STEP, tw, e->main));
+                PFC_CUDA_TRY(launch_col_step(j->run->d_desc, 1, c.L, c.M, c.CT, c.stage,
+                                             ck ? COL_STEP_CHECKPOINT : COL_STEP, tw, e->main));
             }
         }
         const int rc = copy_energy_slots(e, (int)seg_len.size());
         if (rc != PFC_OK) return rc;
         seg_len.push_back(1);
     }
-    PFC_CUDA_TRY(cudaStreamSynchronize(e->main));
+    PFC_SYNC_CHECKED(e->ctx, e->main);
     unpack_energy_slots(e, seg_len);
     for (Job *j : e->active) {
         j->t += q;

@@ -466,19 +466,19 @@ static cudaError_t row_analysis_impl(const RunDesc *d_runs, int nruns, int L, co
     return cudaGetLastError();
 }
 
-template <int L, int C, int MODE>
+template <int L, int C, int MODE, int STAGE>
 static cudaError_t col_impl(const RunDesc *d_runs, int nruns, int M, const TwiddleSet &tw, cudaStream_t st) {
     constexpr int NT = ColCfg<L, C>::NT;
     constexpr size_t smem = 2 * smem_bytes<C * L>() + sizeof(float2) * C * L;  // s, P (padded) and Q
     static unsigned mask = 0;
-    cudaError_t e = set_smem(k_col_step<L, C, MODE>, smem, mask);
+    cudaError_t e = set_smem(k_col_step<L, C, MODE, STAGE>, smem, mask);
     if (nruns == 0) return e;
     if (e != cudaSuccess) return e;
     const int H = M / 2;
     const int items = ((H + 1 + C - 1) / C) * nruns;
     const int cap = ColCfg<L, C>::MINB * sm_count();
     const int grid = items < cap ? items : cap;
-    k_col_step<L, C, MODE><<<grid, NT, smem, st>>>(d_runs, nruns, tw.f32[log2i(L)]);
+    k_col_step<L, C, MODE, STAGE><<<grid, NT, smem, st>>>(d_runs, nruns, tw.f32[log2i(L)], tw.fault);
     return cudaGetLastError();
 }
 
@@ -495,44 +495,78 @@ cudaError_t launch_row_analysis(const RunDesc *d_runs, int nruns, int L, int M, 
     PFC_SIZE_SWITCH(M, row_analysis_impl, d_runs, nruns, L, tw, s)
 }
 
-template <int L, int C>
+template <int L, int C, int STAGE>
 static cudaError_t col_modes(const RunDesc *d_runs, int nruns, int M, int mode, const TwiddleSet &tw,
                              cudaStream_t s) {
     switch (mode) {
-        case COL_STEP: return col_impl<L, C, COL_STEP>(d_runs, nruns, M, tw, s);
-        case COL_PREPARE: return col_impl<L, C, COL_PREPARE>(d_runs, nruns, M, tw, s);
-        case COL_STEP_CHECKPOINT: return col_impl<L, C, COL_STEP_CHECKPOINT>(d_runs, nruns, M, tw, s);
+        case COL_STEP: return col_impl<L, C, COL_STEP, STAGE>(d_runs, nruns, M, tw, s);
+        case COL_PREPARE: return col_impl<L, C, COL_PREPARE, STAGE>(d_runs, nruns, M, tw, s);
+        case COL_STEP_CHECKPOINT: return col_impl<L, C, COL_STEP_CHECKPOINT, STAGE>(d_runs, nruns, M, tw, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+template <int L, int C>
+static cudaError_t col_stages(const RunDesc *d_runs, int nruns, int M, int stage, int mode, const TwiddleSet &tw,
+                              cudaStream_t s) {
+    switch (stage) {
+        case STAGE_ASYNC: return col_modes<L, C, STAGE_ASYNC>(d_runs, nruns, M, mode, tw, s);
+        case STAGE_BULK: return col_modes<L, C, STAGE_BULK>(d_runs, nruns, M, mode, tw, s);
         default: return cudaErrorInvalidValue;
     }
 }
 
 template <int L>
-static cudaError_t col_dispatch(const RunDesc *d_runs, int nruns, int M, int C, int mode, const TwiddleSet &tw,
-                                cudaStream_t s) {
+static cudaError_t col_dispatch(const RunDesc *d_runs, int nruns, int M, int C, int stage, int mode,
+                                const TwiddleSet &tw, cudaStream_t s) {
     switch (C) {
         case 1:
-            if constexpr (col_tile_ok(L, 1)) return col_modes<L, 1>(d_runs, nruns, M, mode, tw, s);
+            if constexpr (col_tile_ok(L, 1)) return col_stages<L, 1>(d_runs, nruns, M, stage, mode, tw, s);
             break;
         case 2:
-            if constexpr (col_tile_ok(L, 2)) return col_modes<L, 2>(d_runs, nruns, M, mode, tw, s);
+            if constexpr (col_tile_ok(L, 2)) return col_stages<L, 2>(d_runs, nruns, M, stage, mode, tw, s);
             break;
         case 4:
-            if constexpr (col_tile_ok(L, 4)) return col_modes<L, 4>(d_runs, nruns, M, mode, tw, s);
+            if constexpr (col_tile_ok(L, 4)) return col_stages<L, 4>(d_runs, nruns, M, stage, mode, tw, s);
             break;
         case 8:
-            if constexpr (col_tile_ok(L, 8)) return col_modes<L, 8>(d_runs, nruns, M, mode, tw, s);
+            if constexpr (col_tile_ok(L, 8)) return col_stages<L, 8>(d_runs, nruns, M, stage, mode, tw, s);
             break;
         case 16:
-            if constexpr (col_tile_ok(L, 16)) return col_modes<L, 16>(d_runs, nruns, M, mode, tw, s);
+            if constexpr (col_tile_ok(L, 16)) return col_stages<L, 16>(d_runs, nruns, M, stage, mode, tw, s);
             break;
         default: break;
     }
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_col_step(const RunDesc *d_runs, int nruns, int L, int M, int C, int mode, const TwiddleSet &tw,
-                            cudaStream_t s) {
-    PFC_SIZE_SWITCH(L, col_dispatch, d_runs, nruns, M, C, mode, tw, s)
+cudaError_t launch_col_step(const RunDesc *d_runs, int nruns, int L, int M, int C, int stage, int mode,
+                            const TwiddleSet &tw, cudaStream_t s) {
+    PFC_SIZE_SWITCH(L, col_dispatch, d_runs, nruns, M, C, stage, mode, tw, s)
+}
+
+// Self-test of the column kernel's tile staging (one CTA of 128 threads): with issue,
+// thread 0 stages n float2 of src into shared memory by one bulk copy, every thread
+// waits (bounded by limit_ns) and the tile is written back to dst; without issue no
+// copy is started, so the wait runs out, the CTA sets *fault and returns.
+__global__ void k_stage_selftest(const float2 *src, float2 *dst, int n, int issue, unsigned long long limit_ns,
+                                 int *fault) {
+    extern __shared__ __align__(16) float2 q[];
+    __shared__ __align__(8) unsigned long long bar_word;
+    const unsigned bar = smem_u32(&bar_word);
+    stage_init(bar);
+    if (issue) stage_issue(bar, src, q, (unsigned)(n * sizeof(float2)));
+    if (!tile_wait(bar, 0u, fault, limit_ns)) return;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = q[i];
+}
+
+cudaError_t launch_stage_selftest(const float2 *src, float2 *dst, int n, int issue, unsigned long long limit_ns,
+                                  int *fault, cudaStream_t s) {
+    if (n < 2 || n > 8192 || (n & 1)) return cudaErrorInvalidValue;  // whole 16-byte units, <= 64 KB
+    const size_t smem = sizeof(float2) * n;
+    cudaError_t e = cudaFuncSetAttribute(k_stage_selftest, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_stage_selftest<<<1, 128, smem, s>>>(src, dst, n, issue, limit_ns, fault);
+    return cudaGetLastError();
 }
 
 cudaError_t prepare_rows(int M) {
@@ -544,12 +578,12 @@ cudaError_t prepare_rows(int M) {
     return launch_row_analysis(nullptr, 0, 0, M, none, 0);
 }
 
-cudaError_t prepare_size(int L, int M, int C) {
+cudaError_t prepare_size(int L, int M, int C, int stage) {
     TwiddleSet none{};
     cudaError_t e;
     if ((e = prepare_rows(M)) != cudaSuccess) return e;
     for (int mode = 0; mode < 3; ++mode)
-        if ((e = launch_col_step(nullptr, 0, L, M, C, mode, none, 0)) != cudaSuccess) return e;
+        if ((e = launch_col_step(nullptr, 0, L, M, C, stage, mode, none, 0)) != cudaSuccess) return e;
     return cudaSuccess;
 }
 

@@ -26,6 +26,7 @@ FP64 = 1
 FP64_PURE = 2
 
 PFC_OK = 0
+PFC_E_INVALID, PFC_E_CUDA, PFC_E_NOMEM, PFC_E_IO, PFC_E_STATE = -1, -2, -3, -4, -5
 
 
 class PfcError(RuntimeError):
@@ -156,6 +157,9 @@ def lib():
         "pfc_run_bytes": ([P(RunParams), dp], C.c_int),
         "pfc_tile_width": ([C.c_int, C.c_int, C.c_int, P(C.c_int), P(C.c_int), fp, P(C.c_int)], C.c_int),
         "pfc_set_tile_width": ([C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
+        "pfc_col_staging": ([C.c_int, C.c_int, C.c_int, P(C.c_int), fp, fp, P(C.c_int)], C.c_int),
+        "pfc_set_col_staging": ([C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
+        "pfc_selftest_tile_stage": ([C.c_int, C.c_int, C.c_int, C.c_double, P(C.c_int), P(C.c_int), dp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -358,6 +362,26 @@ def tile_width(L: int, M: int, device: int = 0):
 def set_tile_width(L: int, M: int, width: int, device: int = 0):
     """Fix the column tile width of an L x M grid for the rest of the process."""
     _check(lib().pfc_set_tile_width(device, L, M, width), "pfc_set_tile_width")
+
+
+STAGE_ASYNC, STAGE_BULK = 0, 1
+
+
+def col_staging(L: int, M: int, device: int = 0):
+    """Tile staging method of the column kernel for an L x M grid (tuned on the device
+    on first use) and the trials: (stage, {candidate width: (ms async, ms bulk)})."""
+    st, n = C.c_int(), C.c_int()
+    a = (C.c_float * 4)()
+    b = (C.c_float * 4)()
+    _check(lib().pfc_col_staging(device, L, M, C.byref(st), a, b, C.byref(n)), "pfc_col_staging")
+    _, trials = tile_width(L, M, device)
+    cand = list(trials)
+    return st.value, {cand[i]: (a[i], b[i]) for i in range(n.value)}
+
+
+def set_col_staging(L: int, M: int, stage: int, device: int = 0):
+    """Fix the column kernel's tile staging (STAGE_ASYNC or STAGE_BULK) of an L x M grid."""
+    _check(lib().pfc_set_col_staging(device, L, M, stage), "pfc_set_col_staging")
 
 
 def run_bytes(params) -> float:

@@ -1,8 +1,10 @@
-"""GPU tests of the column tile-width autotuner.
+"""GPU tests of the column tile-width and staging autotuner.
 
 The width only regroups the columns that one column-kernel CTA transforms (and the
 row-space layout with them); every column goes through the same arithmetic, so runs
-with different widths must give bit-identical fields and energies.  The tuner's
+with different widths must give bit-identical fields and energies.  The staging
+method (16-byte cp.async copies or one TMA bulk copy per tile) only changes how the
+same bytes reach shared memory, so it must not change a bit either.  The tuner's
 choice is therefore free to differ between processes.
 """
 import numpy as np
@@ -46,8 +48,18 @@ def test_tuner_reports_its_trials():
         assert all(ms > 0 for ms in trials.values())
         assert trials[w] == min(trials.values())
     assert P.tile_width(1024, 1024)[0] == w
+    stage, st_trials = P.col_staging(1024, 1024)
+    print("1024^2 staging", stage, "trials (ms per 8 steps, async / bulk):", st_trials)
+    assert stage in (P.STAGE_ASYNC, P.STAGE_BULK)
+    if trials:
+        assert set(st_trials) == set(trials)
+        for c, (a, b) in st_trials.items():
+            assert a > 0 and b > 0 and trials[c] == min(a, b)
+        assert st_trials[w][stage] == trials[w]
     with pytest.raises(P.PfcError):
         P.set_tile_width(1024, 1024, 16)  # the tile would not fit
+    with pytest.raises(P.PfcError):
+        P.set_col_staging(1024, 1024, 2)  # no such method
 
 
 def test_batch_mixing_tile_widths_equals_single_runs():
@@ -76,3 +88,51 @@ def test_batch_mixing_tile_widths_equals_single_runs():
         batch.close()
     finally:
         P.set_tile_width(L, M, tuned)
+
+
+@pytest.mark.parametrize("model,L,M,width", [(P.MODEL_MISFIT, 1024, 1024, 2), (P.MODEL_MISFIT, 1024, 1024, 4),
+                                             (P.MODEL_CVD, 512, 128, None), (P.MODEL_MISFIT, 64, 2048, None)])
+def test_both_stagings_give_identical_results(model, L, M, width):
+    tuned, _ = P.tile_width(L, M)
+    stage0, _ = P.col_staging(L, M)
+    results = []
+    try:
+        if width:
+            P.set_tile_width(L, M, width)
+        for s in (P.STAGE_ASYNC, P.STAGE_BULK):
+            P.set_col_staging(L, M, s)
+            r = P.Run(P.default_params(model, L=L, M=M, seed=11))
+            r.advance(25, analysis=True)  # the last step writes the checkpoint outputs
+            phi, con = r.fields_f32()
+            results.append((phi, con, r.energy()))
+            r.close()
+    finally:
+        P.set_tile_width(L, M, tuned)
+        P.set_col_staging(L, M, stage0)
+    (pa, ca, ea), (pb, cb, eb) = results
+    assert np.array_equal(pa, pb)
+    assert np.array_equal(ca, cb)
+    assert ea == eb
+
+
+def test_batch_mixing_stagings_equals_single_runs():
+    L = M = 512
+    tuned, _ = P.tile_width(L, M)
+    stage0, _ = P.col_staging(L, M)
+    try:
+        runs, singles = [], []
+        for i, s in enumerate((P.STAGE_ASYNC, P.STAGE_BULK)):
+            P.set_col_staging(L, M, s)
+            runs.append(P.Run(P.default_params(P.MODEL_MISFIT, L=L, M=M, seed=300 + i)))
+            singles.append(P.Run(P.default_params(P.MODEL_MISFIT, L=L, M=M, seed=300 + i)))
+        batch = P.Batch(runs)
+        batch.advance(15)
+        for r in singles:
+            r.advance(15)
+        for a, b in zip(runs, singles):
+            fa, ca = a.fields_f32()
+            fb, cb = b.fields_f32()
+            assert np.array_equal(fa, fb) and np.array_equal(ca, cb)
+        batch.close()
+    finally:
+        P.set_col_staging(L, M, stage0)
