@@ -323,7 +323,7 @@ def sweep_bench(P, dev, nruns=64, steps=2000, master_seed=4242):
         for w in warm:
             eng.release(w)
         t0 = time.perf_counter()
-        ids = [eng.submit(P.JOB_MISFIT, p, steps=steps, mod=steps) for p in jobs]
+        ids = eng.submit_many(P.JOB_MISFIT, jobs, steps=steps, mod=steps)  # the sweep arrives at once
         done = drain_engine(P, eng, len(ids))
         wall = time.perf_counter() - t0
         ok = sum(1 for j in ids if j in done and done[j].type == P.EV_DONE)

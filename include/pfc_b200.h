@@ -283,6 +283,11 @@ int pfc_engine_create(const pfc_engine_opts *opts, pfc_engine **out);
 int pfc_engine_destroy(pfc_engine *e);
 /* Queue a job; *id receives its id (never 0).  The job's strings are copied. */
 int pfc_submit(pfc_engine *e, const pfc_job *job, uint64_t *id);
+/* Queue n jobs at once, in order (a whole sweep: the scheduler sees them together and
+ * admits as many as fit in one pass); ids[i] receives job i's id.  All or nothing: if
+ * any job is invalid, none is queued and the error names its index.  An Elastic job
+ * may name an earlier job of the same call as its source. */
+int pfc_submit_many(pfc_engine *e, const pfc_job *jobs, int n, uint64_t *ids);
 /* Copy up to max pending events into ev (oldest first) without waiting; *n
  * receives the number copied. */
 int pfc_poll(pfc_engine *e, pfc_event *ev, int max, int *n);

@@ -821,8 +821,8 @@ extern "C" int pfc_engine_destroy(pfc_engine *e) {
     return PFC_OK;
 }
 
-extern "C" int pfc_submit(pfc_engine *e, const pfc_job *job, uint64_t *id) {
-    if (!e || !job || !id) return set_error(PFC_E_INVALID, "null argument");
+// A job from its spec, checked; the caller queues it.
+static int make_job(pfc_engine *e, const pfc_job *job, std::unique_ptr<Job> &out) {
     auto j = std::make_unique<Job>();
     j->spec = *job;
     j->outdir = job->outdir ? job->outdir : "";
@@ -846,17 +846,48 @@ extern "C" int pfc_submit(pfc_engine *e, const pfc_job *job, uint64_t *id) {
     } else {
         return set_error(PFC_E_INVALID, "unknown job kind");
     }
-    std::lock_guard<std::mutex> lk(e->mu);
-    if (job->kind == PFC_JOB_ELASTIC && job->source_job) {
-        auto it = e->jobs.find(job->source_job);
-        if (it == e->jobs.end() || it->second->spec.kind == PFC_JOB_ELASTIC)
-            return set_error(PFC_E_INVALID, "source_job is not a Misfit or CVD job of this engine");
+    out = std::move(j);
+    return PFC_OK;
+}
+
+// An Elastic job's source must be a Misfit or CVD job of this engine (e->mu held);
+// `pending` are jobs queued in the same call, ahead of this one.
+static bool source_ok(pfc_engine *e, const pfc_job *job, const std::vector<std::unique_ptr<Job>> &pending,
+                      uint64_t first_id) {
+    if (job->kind != PFC_JOB_ELASTIC || !job->source_job) return true;
+    auto it = e->jobs.find(job->source_job);
+    if (it != e->jobs.end()) return it->second->spec.kind != PFC_JOB_ELASTIC;
+    const uint64_t k = job->source_job - first_id;
+    return job->source_job >= first_id && k < pending.size() && pending[k] && pending[k]->spec.kind != PFC_JOB_ELASTIC;
+}
+
+extern "C" int pfc_submit(pfc_engine *e, const pfc_job *job, uint64_t *id) {
+    if (!job) return set_error(PFC_E_INVALID, "null argument");
+    return pfc_submit_many(e, job, 1, id);
+}
+
+extern "C" int pfc_submit_many(pfc_engine *e, const pfc_job *jobs, int n, uint64_t *ids) {
+    if (!e || !jobs || !ids || n <= 0) return set_error(PFC_E_INVALID, "null argument or empty job list");
+    std::vector<std::unique_ptr<Job>> js(n);
+    for (int i = 0; i < n; ++i) {
+        const int rc = make_job(e, &jobs[i], js[i]);
+        if (rc != PFC_OK) return n > 1 ? set_error(rc, "job " + std::to_string(i) + ": " + pfc_last_error()) : rc;
     }
-    j->id = e->next_id++;
-    j->t_submit = e->now();
-    *id = j->id;
-    e->queue.push_back(j.get());
-    e->jobs[j->id] = std::move(j);
+    std::lock_guard<std::mutex> lk(e->mu);
+    const uint64_t first = e->next_id;
+    for (int i = 0; i < n; ++i)
+        if (!source_ok(e, &jobs[i], js, first))
+            return set_error(PFC_E_INVALID, (n > 1 ? "job " + std::to_string(i) + ": " : std::string()) +
+                                                "source_job is not a Misfit or CVD job of this engine");
+    const double t = e->now();
+    for (int i = 0; i < n; ++i) {
+        Job *j = js[i].get();
+        j->id = e->next_id++;
+        j->t_submit = t;
+        ids[i] = j->id;
+        e->queue.push_back(j);
+        e->jobs[j->id] = std::move(js[i]);
+    }
     e->wake = true;
     e->cv_sched.notify_all();
     return PFC_OK;

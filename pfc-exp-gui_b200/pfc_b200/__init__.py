@@ -149,6 +149,7 @@ def lib():
         "pfc_engine_create": ([P(EngineOpts), P(vp)], C.c_int),
         "pfc_engine_destroy": ([vp], C.c_int),
         "pfc_submit": ([vp, P(JobSpec), P(C.c_uint64)], C.c_int),
+        "pfc_submit_many": ([vp, P(JobSpec), C.c_int, P(C.c_uint64)], C.c_int),
         "pfc_poll": ([vp, P(Event), C.c_int, P(C.c_int)], C.c_int),
         "pfc_wait": ([vp, P(Event), C.c_int, P(C.c_int), C.c_int], C.c_int),
         "pfc_cancel": ([vp, C.c_uint64], C.c_int),
@@ -311,6 +312,16 @@ class Engine:
         _check(lib().pfc_submit(self.h, C.byref(j), C.byref(jid)), "pfc_submit")
         self.grids[jid.value] = (params.L, params.M, params.N)
         return jid.value
+
+    def submit_many(self, kind, params_list, steps=0, mod=0):
+        """Queue one job per parameter set in a single call (pfc_submit_many); returns their ids."""
+        n = len(params_list)
+        arr = (JobSpec * n)(*[JobSpec(kind, p, steps, mod, None, 0, None, 0.0) for p in params_list])
+        ids = (C.c_uint64 * n)()
+        _check(lib().pfc_submit_many(self.h, arr, n, ids), "pfc_submit_many")
+        for p, i in zip(params_list, ids):
+            self.grids[i] = (p.L, p.M, p.N)
+        return list(ids)
 
     def poll(self, max_events=256):
         ev = (Event * max_events)()

@@ -238,3 +238,27 @@ def test_engine_rejects_bad_jobs():
     with pytest.raises(P.PfcError):
         eng.submit(7, params(P.MODEL_MISFIT, 64, 64), steps=10, mod=5)
     eng.close()
+
+
+def test_engine_submit_many():
+    """pfc_submit_many queues a whole sweep in one call: all or nothing, ids in order, and
+    every job's result equals the same job submitted on its own."""
+    eng = P.Engine()
+    good = [params(P.MODEL_MISFIT, g, g, seed=40 + i, u0=0.05 + 0.01 * i) for i, g in enumerate((64, 128, 64, 256))]
+    bad = good[:2] + [params(P.MODEL_MISFIT, 64, 64, precision=P.FP64)] + good[2:]
+    with pytest.raises(P.PfcError, match="job 2"):
+        eng.submit_many(P.JOB_MISFIT, bad, steps=30, mod=15)
+    assert eng.poll() == []  # nothing was queued
+    ids = eng.submit_many(P.JOB_MISFIT, good, steps=30, mod=15)
+    assert ids == sorted(ids) and len(set(ids)) == len(good)
+    evs = drain(eng, ids)
+    assert all(evs[i][-1].type == P.EV_DONE for i in ids)
+    fields = [eng.fields(i) for i in ids]
+    eng.close()
+    one = P.Engine()
+    for p, f in zip(good, fields):
+        j = one.submit(P.JOB_MISFIT, p, steps=30, mod=15)
+        drain(one, [j])
+        for x, y in zip(f, one.fields(j)):
+            assert same_bits(x, y)
+    one.close()
