@@ -198,6 +198,30 @@ template <> struct ilog2<1> {
         }                                                                   \
     }
 
+// The same walk unrolled over a fixed bound IT of iterations per thread; the body sees
+// the iteration index `it`, so values can stay in registers from one walk to the next.
+// A run's Hp = round_up(M/2 + 1, CT) with CT <= 16, so T * CT * RPC <= (M/2 + 16) * RPC
+// and IT = ceil((M/2 + 16) * RPC / NT) covers every element.
+template <int M, int RPC, int NT> struct RowWalk {
+    static constexpr int IT = ((M / 2 + 16) * RPC + NT - 1) / NT;
+};
+#define ROW_TILE_LOOP_REG(RPC, H, NT, IT, ...)                             \
+    {                                                                       \
+        const int _ct = d.CT, _lct = d.lct;                                 \
+        const int _lblk = ilog2<(RPC)>::value + _lct;                       \
+        const int _total = d.T << _lblk;                                    \
+        _Pragma("unroll") for (int it = 0; it < (IT); ++it) {               \
+            const int w = threadIdx.x + it * (NT);                          \
+            if (w >= _total) continue;                                      \
+            const int t = w >> _lblk, rem = w & ((1 << _lblk) - 1);         \
+            const int r = rem >> _lct, k = (t << _lct) + (rem & (_ct - 1)); \
+            if (k > (H)) continue;                                          \
+            const int l = l0 + r;                                           \
+            (void)l;                                                        \
+            __VA_ARGS__                                                     \
+        }                                                                   \
+    }
+
 // ---------------------------------------------------------------------------
 // Row kernel: 4 row-space arrays in, 2 out.
 // ---------------------------------------------------------------------------
@@ -213,8 +237,12 @@ __global__ void __launch_bounds__(RowCfg<M>::NT, 2) k_row_step(const RunDesc *__
     const int l0 = blockIdx.x * RPC;
     // the noise stream's step index: advanced once per step, read by this step's column kernel
     if (d.noise_amp != 0.0f && blockIdx.x == 0 && threadIdx.x == 0) *d.step_ctr += 1;
+    // phi^ and con^ stay in registers until the block's maxima give the balance
+    // exponent; ca^ and cb^ go straight into their packed pair
+    constexpr int LIT = RowWalk<M, RPC, NT>::IT;
+    float2 Pr[LIT], Cr[LIT];
     float mp = 0.f, mc = 0.f;
-    ROW_TILE_LOOP(RPC, H, NT, {
+    ROW_TILE_LOOP_REG(RPC, H, NT, LIT, {
         float2 P = make_float2(0.f, 0.f), Cc = P, A = P, B = P;
         if (l < L) {
             const long o = rs_index(d, l, k);
@@ -223,7 +251,8 @@ __global__ void __launch_bounds__(RowCfg<M>::NT, 2) k_row_step(const RunDesc *__
             A = d.ca[o];
             B = d.cb[o];
         }
-        park_pair(s, NB, 2 * r, k, M, P, Cc);
+        Pr[it] = P;
+        Cr[it] = Cc;
         build_pair(s, NB, 2 * r + 1, k, M, A, B);
         mp = fmaxf(mp, absmax2(P));
         mc = fmaxf(mc, absmax2(Cc));
@@ -232,14 +261,15 @@ __global__ void __launch_bounds__(RowCfg<M>::NT, 2) k_row_step(const RunDesc *__
     block_max_put(wmax[1], mc);
     __syncthreads();
     // con rides as 2^e1 * con beside phi (balance_exp)
-    const int e1 = balance_exp(block_max_get<NW>(wmax[0]), block_max_get<NW>(wmax[1]));
-    ROW_TILE_LOOP(RPC, H, NT, { unpark_pair(s, NB, 2 * r, k, M, pow2f(e1)); })
+    const float g1 = pow2f(balance_exp(block_max_get<NW>(wmax[0]), block_max_get<NW>(wmax[1])));
+    ROW_TILE_LOOP_REG(RPC, H, NT, LIT,
+                      { build_pair(s, NB, 2 * r, k, M, Pr[it], make_float2(Cr[it].x * g1, Cr[it].y * g1)); })
     __syncthreads();
     fft_smem<M, NB, NT, false>(s, tw);
 
     constexpr int PTS = (RPC * M + NT - 1) / NT;
     const float invM = 1.0f / (float)M;
-    const float cs = invM * pow2f(-e1);
+    const float cs = invM / g1;  // 2^-e1 / M, exact
     const float inv_c0 = 1.0f / d.k.para_c0, inv_1mc0 = 1.0f / (1.0f - d.k.para_c0);
     float2 out[PTS];
     float mi = 0.f, mj = 0.f;
