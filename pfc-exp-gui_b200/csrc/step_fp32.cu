@@ -123,27 +123,6 @@ __device__ __forceinline__ void build_pair(float2 *s, int NB, int b, int k, int 
     }
 }
 
-// build_pair in two passes, for a Y whose scale is known only after all of the
-// block's values are seen: park_pair leaves X at Z[k] and Y at Z[M-k] (at k = 0 and
-// M/2 the only parts build_pair uses, (X.x, Y.x), at Z[k]); unpark_pair, run later
-// by the same thread for the same (b, k), writes build_pair(X, g * Y) over them.
-__device__ __forceinline__ void park_pair(float2 *s, int NB, int b, int k, int M, float2 X, float2 Y) {
-    if (k == 0 || k == M / 2) {
-        s[spad(k * NB + b)] = make_float2(X.x, Y.x);
-    } else {
-        s[spad(k * NB + b)] = X;
-        s[spad((M - k) * NB + b)] = Y;
-    }
-}
-__device__ __forceinline__ void unpark_pair(float2 *s, int NB, int b, int k, int M, float g) {
-    if (k == 0 || k == M / 2) {
-        s[spad(k * NB + b)].y *= g;
-    } else {
-        const float2 X = s[spad(k * NB + b)], Y = s[spad((M - k) * NB + b)];
-        build_pair(s, NB, b, k, M, X, make_float2(Y.x * g, Y.y * g));
-    }
-}
-
 // Balancing the two members of a packed transform.  The rounding error a transform
 // adds to either member of x + i y is set by the larger of the two, so a member that
 // is much smaller than its partner (con beside phi in Misfit runs: deviations about
@@ -380,8 +359,11 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_analysis(const RunDesc *_
     const RunDesc &d = runs[blockIdx.y];
     const int L = d.L;
     const int l0 = blockIdx.x * RPC;
+    // phi^ and con^ stay in registers until the block's maxima give the balance exponent
+    constexpr int LIT = RowWalk<M, RPC, NT>::IT;
+    float2 Pr[LIT], Cr[LIT];
     float mp = 0.f, mc = 0.f;
-    ROW_TILE_LOOP(RPC, H, NT, {
+    ROW_TILE_LOOP_REG(RPC, H, NT, LIT, {
         float2 z[6] = {};
         if (l < L) {
             const long o = rs_index(d, l, k);
@@ -392,7 +374,8 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_analysis(const RunDesc *_
             z[4] = d.gx[o];
             z[5] = d.gy[o];
         }
-        park_pair(s, NB, 3 * r, k, M, z[0], z[1]);
+        Pr[it] = z[0];
+        Cr[it] = z[1];
         build_pair(s, NB, 3 * r + 1, k, M, z[2], z[3]);
         build_pair(s, NB, 3 * r + 2, k, M, z[4], z[5]);
         mp = fmaxf(mp, absmax2(z[0]));
@@ -402,8 +385,9 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_analysis(const RunDesc *_
     block_max_put(wmax[1], mc);
     __syncthreads();
     // con rides as 2^e1 * con beside phi (balance_exp)
-    const int e1 = balance_exp(block_max_get<NW>(wmax[0]), block_max_get<NW>(wmax[1]));
-    ROW_TILE_LOOP(RPC, H, NT, { unpark_pair(s, NB, 3 * r, k, M, pow2f(e1)); })
+    const float g1 = pow2f(balance_exp(block_max_get<NW>(wmax[0]), block_max_get<NW>(wmax[1])));
+    ROW_TILE_LOOP_REG(RPC, H, NT, LIT,
+                      { build_pair(s, NB, 3 * r, k, M, Pr[it], make_float2(Cr[it].x * g1, Cr[it].y * g1)); })
     __syncthreads();
     fft_smem<M, NB, NT, false>(s, tw);
     const float invM = 1.0f / (float)M;
@@ -415,7 +399,7 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_analysis(const RunDesc *_
         if (l >= L) continue;
         const float2 z1 = s[spad(m * NB + 3 * r)], z2 = s[spad(m * NB + 3 * r + 1)], z3 = s[spad(m * NB + 3 * r + 2)];
         const float dpsi = z1.x * invM;
-        const float psi = dpsi + d.psi_mean_f, c = z1.y * (invM * pow2f(-e1)) + d.con_mean_f;
+        const float psi = dpsi + d.psi_mean_f, c = z1.y * (invM / g1) + d.con_mean_f;  // invM / g1 = 2^-e1 / M, exact
         const float a = z2.x * invM, b = z2.y * invM, gx = z3.x * invM, gy = z3.y * invM;
         d.psi_real[(size_t)l * M + m] = psi;
         d.con_real[(size_t)l * M + m] = c;
