@@ -38,20 +38,23 @@ extern "C" {
 #define PFC_MODEL_MISFIT 0
 #define PFC_MODEL_CVD 1
 
-#define PFC_PRECISION_FP32 0 /* fused FP32 path, FP64 k=0 mode and reductions */
+#define PFC_PRECISION_FP32 0 /* fused path in FP32 arithmetic, FP64 k=0 mode and reductions */
 #define PFC_PRECISION_FP64 1 /* plain FP64 path with the reference's float roundings */
 #define PFC_PRECISION_FP64_PURE 2 /* plain FP64 path, every intermediate in double */
+#define PFC_PRECISION_MIXED 3 /* fused path: the FP32 path's FP32 complex arrays in HBM, FP64
+                                 arithmetic and the pure-FP64 operator in the kernels (within
+                                 1e-5 of pure FP64 after 200 steps); the default */
 
 /* Parameters of one run.  Field meanings and defaults follow the reference CLI
  * (misfit_uniform_time_seed_fftw_early.cpp:17-35, 125-143; cvd.cpp:111-125, 33-53). */
 typedef struct pfc_run_params {
     int model;      /* PFC_MODEL_MISFIT or PFC_MODEL_CVD */
-    int L, M, N;    /* grid; L, M powers of two in [32, 2048]; N = 1 (2-D) on the FP32 path,
-                       a power of two <= 2048 on the FP64 paths (3-D CVD runs) */
+    int L, M, N;    /* grid; L, M powers of two in [32, 2048]; N = 1 (2-D) on the fused
+                       (FP32, mixed) paths, a power of two <= 2048 on the FP64 paths (3-D CVD runs) */
     float u0, con0, sig, dt, dx, axx;
     int grainx, grainy, grainz; /* Misfit initial grains */
     uint32_t seed;
-    int precision;  /* PFC_PRECISION_FP32, PFC_PRECISION_FP64 or PFC_PRECISION_FP64_PURE */
+    int precision;  /* PFC_PRECISION_MIXED, _FP32, _FP64 or _FP64_PURE */
     int device;     /* CUDA device ordinal */
 } pfc_run_params;
 
@@ -61,7 +64,7 @@ typedef struct pfc_batch pfc_batch;
 /* Last error message of the calling thread ("" if none). */
 const char *pfc_last_error(void);
 
-/* Fill *p with the reference defaults of `model` (grid 256 x 256 x 1, FP32). */
+/* Fill *p with the reference defaults of `model` (grid 256 x 256 x 1, mixed precision). */
 int pfc_default_params(int model, pfc_run_params *p);
 
 /* Allocate a run on the device and set its initial condition (INITIAL_dis for
@@ -77,31 +80,35 @@ int pfc_run_advance(pfc_run *r, int nsteps, int analysis);
  * *ms receives the device time.  (Measurement hook; no reference counterpart.) */
 int pfc_run_advance_timed(pfc_run *r, int nsteps, float *ms);
 
-/* Column tile width (packed columns per column-kernel tile, 1..16) that FP32 runs of
- * an L x M grid use on `device`.  The first FP32 run of a grid times each candidate
- * width with each tile staging method (a batch of Misfit runs, row and column sweeps,
- * CUDA events) and keeps the fastest pair for the process; neither changes the
- * results of a step, only its speed.  This call tunes the grid if it has not been
- * tuned, returns the width and, when the pointers are not NULL, the candidates (up to
- * 4) and their trial times (ms per 8 steps, the faster staging; *ntrials is 0 when no
- * trial ran).  PFC_AUTOTUNE=0 in the environment keeps the default widths with bulk
- * staging.  (Autotuner of the batched FFT sweeps; the reference uses FFTW and has no
+/* Column tile width (packed columns per column-kernel tile, 1..16) that fused-path
+ * runs (precision PFC_PRECISION_MIXED or PFC_PRECISION_FP32) of an L x M grid use on
+ * `device`.  The first run of a grid and precision times each candidate width with
+ * each tile staging method (a batch of Misfit runs, row and column sweeps, CUDA
+ * events) and keeps the fastest pair for the process; neither changes the results of
+ * a step, only its speed.  This call tunes the grid if it has not been tuned, returns
+ * the width and, when the pointers are not NULL, the candidates (up to 4) and their
+ * trial times (ms per 8 steps, the faster staging; *ntrials is 0 when no trial ran).
+ * PFC_AUTOTUNE=0 in the environment keeps the default widths with bulk staging.
+ * (Autotuner of the batched FFT sweeps; the reference uses FFTW and has no
  * counterpart.) */
-int pfc_tile_width(int device, int L, int M, int *width, int *candidates, float *trial_ms, int *ntrials);
-/* Fix the tile width of a grid for the rest of the process (one of the candidates;
- * the staging becomes the faster one of that width's trial, bulk without one); runs
- * created before keep their own. */
-int pfc_set_tile_width(int device, int L, int M, int width);
+int pfc_tile_width(int device, int L, int M, int precision, int *width, int *candidates, float *trial_ms,
+                   int *ntrials);
+/* Fix the tile width of a grid and precision for the rest of the process (one of the
+ * candidates; the staging becomes the faster one of that width's trial, bulk without
+ * one); runs created before keep their own. */
+int pfc_set_tile_width(int device, int L, int M, int precision, int width);
 
 #define PFC_STAGE_ASYNC 0 /* column kernel stages tiles by 16-byte cp.async copies */
 #define PFC_STAGE_BULK 1  /* ... by one TMA bulk copy per tile, completing on an mbarrier */
-/* Tile staging method (PFC_STAGE_*) that FP32 runs of an L x M grid use, tuning the
- * grid first if needed; when not NULL, ms_async / ms_bulk receive each candidate
- * width's trial time with either method (order of pfc_tile_width's candidates). */
-int pfc_col_staging(int device, int L, int M, int *stage, float *ms_async, float *ms_bulk, int *ntrials);
-/* Fix the staging method of a grid for the rest of the process; runs created before
- * keep their own. */
-int pfc_set_col_staging(int device, int L, int M, int stage);
+/* Tile staging method (PFC_STAGE_*) that fused-path runs of an L x M grid and
+ * precision use, tuning the grid first if needed; when not NULL, ms_async / ms_bulk
+ * receive each candidate width's trial time with either method (order of
+ * pfc_tile_width's candidates). */
+int pfc_col_staging(int device, int L, int M, int precision, int *stage, float *ms_async, float *ms_bulk,
+                    int *ntrials);
+/* Fix the staging method of a grid and precision for the rest of the process; runs
+ * created before keep their own. */
+int pfc_set_col_staging(int device, int L, int M, int precision, int stage);
 
 /* Self-test of the column kernel's tile staging on one device (not a reference
  * interface; the reference has no device code).  With issue = 1, n complex floats
@@ -131,8 +138,8 @@ int pfc_run_energy(pfc_run *r, double *e_over_p, double *mass_over_p);
 int pfc_run_means(const pfc_run *r, double *phi_mean, double *con_mean);
 
 /* Batched execution: runs of any of the supported grid sizes advanced together
- * (one launch per size class per sweep).  Runs must be FP32 and on one device;
- * the batch does not own them. */
+ * (one launch per size class and precision per sweep).  Runs must be on the fused
+ * paths (mixed or FP32) and on one device; the batch does not own them. */
 int pfc_batch_create(pfc_run *const *runs, int nruns, pfc_batch **out);
 int pfc_batch_destroy(pfc_batch *b);
 /* Advance every run of the batch by nsteps (captured once into a CUDA graph). */
@@ -168,8 +175,9 @@ int pfc_phimax_misfit(const float *phi, const float *con, int L, int M, float dx
  * that loads it, held until exit).  L*M must not exceed 4194304 (2048 x 2048);
  * larger fields are rejected with PFC_E_INVALID.  The function calls no cudaMalloc,
  * cudaFree or other allocating routine.  It runs on `stream` (a cudaStream_t;
- * NULL = the default stream) and returns after the atoms are written and *count
- * is set.
+ * NULL = the default stream), waits for that stream to finish, and returns after the
+ * atoms are written and *count is set.  *count is the number of atoms found, which
+ * may exceed cap; only the first cap records are written.
  *
  * The first call on a device looks up the scratch array's device address; make
  * that first call before any stream capture.  All calls on a device share the

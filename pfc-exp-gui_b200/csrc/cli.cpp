@@ -12,8 +12,9 @@
 // Files are byte-compatible with the reference writers (VTI/PVTI at
 // misfit_uniform_time_seed_fftw_early.cpp:1588-1810, text files with std::fixed and
 // precision(4)).  Additive options: --grid LxMxN (runtime grid; default 256x256x1)
-// and --precision fp32|fp64|fp64-pure (default fp32 on 2-D grids, fp64 on 3-D grids,
-// which the FP32 path does not take).  Output paths are prefixed with --outdir
+// and --precision mixed|fp32|fp64|fp64-pure (default mixed on 2-D grids: FP32 arrays,
+// FP64 arithmetic; fp64 on 3-D grids, which the fused paths do not take).  Output
+// paths are prefixed with --outdir
 // instead of changing the process working directory.
 #include <algorithm>
 #include <cerrno>
@@ -106,7 +107,8 @@ bool parse_grid(const char *v, int &L, int &M, int &N) {
 bool parse_precision(const char *v, int &out) {
     if (!v) return false;
     std::string s(v);
-    if (s == "fp32") out = PFC_PRECISION_FP32;
+    if (s == "mixed") out = PFC_PRECISION_MIXED;
+    else if (s == "fp32") out = PFC_PRECISION_FP32;
     else if (s == "fp64") out = PFC_PRECISION_FP64;
     else if (s == "fp64-pure") out = PFC_PRECISION_FP64_PURE;
     else return false;
@@ -148,7 +150,7 @@ struct SimOpts {
     unsigned int seed;
     int grainx, grainy, grainz;
     int L = 256, M = 256, N = 1;
-    int precision = -1;  // -1: FP32 on 2-D grids, FP64 on 3-D grids
+    int precision = -1;  // -1: mixed on 2-D grids, FP64 on 3-D grids
     int resume = -1;  // --resume <kd>: continue from the run's own checkpoint kd
     std::string outdir;
 };
@@ -201,7 +203,7 @@ void misfit_usage(const char *argv0) {
          << "  --axx <float>       Noise base intensity (default: 0)\n"
          << "  --outdir <path>     Output directory (default: current dir)\n"
          << "  --grid <LxMxN>      Grid (default: 256x256x1)\n"
-         << "  --precision <p>     fp32, fp64 or fp64-pure (default: fp32 on 2-D grids, fp64 on 3-D)\n"
+         << "  --precision <p>     mixed, fp32, fp64 or fp64-pure (default: mixed on 2-D grids, fp64 on 3-D)\n"
          << "  --resume <kd>       Continue from checkpoint kd in --outdir\n"
          << "  -h, --help          Show this help\n";
 }
@@ -397,7 +399,7 @@ int run_misfit_cli(int argc, char **argv) {
     p.grainy = o.grainy;
     p.grainz = o.grainz;
     p.seed = o.seed;
-    p.precision = o.precision >= 0 ? o.precision : (N == 1 ? PFC_PRECISION_FP32 : PFC_PRECISION_FP64);
+    p.precision = o.precision >= 0 ? o.precision : (N == 1 ? PFC_PRECISION_MIXED : PFC_PRECISION_FP64);
     RunGuard g;
     if (pfc_run_create(&p, &g.r) != PFC_OK) return gpu_fail("run setup");
     pfc_run *r = g.r;
@@ -466,7 +468,7 @@ void cvd_usage(const char *argv0) {
          << "  --seed <uint>       Random seed base (default: 20200604)\n"
          << "  --outdir <path>     Output directory (default: current dir)\n"
          << "  --grid <LxMxN>      Grid (default: 256x256x1)\n"
-         << "  --precision <p>     fp32, fp64 or fp64-pure (default: fp32 on 2-D grids, fp64 on 3-D)\n"
+         << "  --precision <p>     mixed, fp32, fp64 or fp64-pure (default: mixed on 2-D grids, fp64 on 3-D)\n"
          << "  --resume <kd>       Continue from checkpoint kd in --outdir\n"
          << "  -h, --help          Show this help\n";
 }
@@ -578,7 +580,7 @@ int run_cvd_cli(int argc, char **argv) {
     p.dt = o.dt;
     p.dx = o.dx;
     p.seed = o.seed;
-    p.precision = o.precision >= 0 ? o.precision : (N == 1 ? PFC_PRECISION_FP32 : PFC_PRECISION_FP64);
+    p.precision = o.precision >= 0 ? o.precision : (N == 1 ? PFC_PRECISION_MIXED : PFC_PRECISION_FP64);
     RunGuard g;
     if (pfc_run_create(&p, &g.r) != PFC_OK) return gpu_fail("run setup");
     pfc_run *r = g.r;

@@ -1,5 +1,13 @@
-// col_kernel.cuh -- the column kernel of the fused FP32 step (included by step_fp32.cu).
+// col_kernel.cuh -- the column kernel of the fused FP32 step, and its launchers.
 //
+// Instantiated one row length L per translation unit (col_inst.cu compiled with
+// PFC_COL_L = L); step_fp32.cu reaches it through launch_col_f32_L<L>.
+#pragma once
+
+#include "step_common.cuh"
+
+namespace pfc {
+
 // Work item: a tile of L rows x C packed columns of one run (a contiguous block of
 // the row-space layout).  CTAs are persistent and take items in turn.  For phi and
 // then con:
@@ -25,40 +33,7 @@
 // Tile staging (Stager, Prefetch, tile_out) and the
 // ScaleByTable / GradientOf multipliers come from tile_io.cuh.
 
-// Spectrum of the noise field at mode (l, km) of step t.  The reference draws real-space
-// white noise with a sequential polar Box-Muller generator (Gauss, MIS:951-981) and
-// transforms it (p5); the transform of white noise is itself white, so the modes are
-// drawn here directly, with the distribution the reference's masks leave
-// (MIS:1002-1003): re and im independent N(0, P/4), except at the four self-conjugate
-// modes (l in {0, L/2}, km in {0, M/2}) where re ~ N(0, P) and im = 0; along the
-// self-conjugate columns km = 0 and M/2, mode L - l is the conjugate of mode l.
-// Stream: the two normals of canonical mode c = (t*L + l)*(M/2 + 1) + km come from
-// Box-Muller of the splitmix64 outputs at positions 2c and 2c + 1 of the run's key.
-__device__ __forceinline__ unsigned long long sm64_out(unsigned long long z) {
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
-    return z ^ (z >> 31);
-}
-__device__ float2 noise_mode(unsigned long long key, int t, int l, int km, int L, int M) {
-    const int H = M / 2;
-    bool conj = false;
-    if ((km == 0 || km == H) && l > L / 2) {
-        l = L - l;
-        conj = true;
-    }
-    const unsigned long long c = ((unsigned long long)t * L + l) * (unsigned long long)(H + 1) + km;
-    const unsigned long long g = 0x9E3779B97F4A7C15ULL;
-    const unsigned long long w1 = sm64_out(key + (2 * c + 1) * g), w2 = sm64_out(key + (2 * c + 2) * g);
-    const float u1 = ((float)(w1 >> 40) + 0.5f) * (1.0f / 16777216.0f);  // (0, 1)
-    const float u2 = (float)(w2 >> 40) * (1.0f / 16777216.0f);           // [0, 1)
-    const float rad = sqrtf(-2.0f * logf(u1));
-    float sn, cs;
-    sincospif(2.0f * u2, &sn, &cs);
-    const float P = (float)L * (float)M;
-    if ((l == 0 || l == L / 2) && (km == 0 || km == H)) return make_float2(sqrtf(P) * rad * cs, 0.0f);
-    const float s = 0.5f * sqrtf(P);
-    return make_float2(s * rad * cs, conj ? -s * rad * sn : s * rad * sn);
-}
+// noise_mode (the spectrum of the noise field of step t) comes from step_common.cuh.
 
 template <int L, int C, int MODE, int STAGE>
 __global__ void __launch_bounds__(ColCfg<L, C>::NT, ColCfg<L, C>::MINB)
@@ -170,3 +145,71 @@ __global__ void __launch_bounds__(ColCfg<L, C>::NT, ColCfg<L, C>::MINB)
     }
     st.finish();  // every copy issued has been waited for: the last item issues none (next_psi = null)
 }
+
+template <int L, int C, int MODE, int STAGE>
+static cudaError_t col_impl(const RunDesc *d_runs, int nruns, int M, const TwiddleSet &tw, cudaStream_t st) {
+    constexpr int NT = ColCfg<L, C>::NT;
+    constexpr size_t smem = 2 * smem_bytes<C * L>() + sizeof(float2) * C * L;  // s, P (padded) and Q
+    static unsigned mask = 0;
+    cudaError_t e = set_smem(k_col_step<L, C, MODE, STAGE>, smem, mask);
+    if (nruns == 0) return e;
+    if (e != cudaSuccess) return e;
+    const int H = M / 2;
+    const int items = ((H + 1 + C - 1) / C) * nruns;
+    const int cap = ColCfg<L, C>::MINB * sm_count();
+    const int grid = items < cap ? items : cap;
+    k_col_step<L, C, MODE, STAGE><<<grid, NT, smem, st>>>(d_runs, nruns, tw.f32[log2i(L)], tw.fault);
+    return cudaGetLastError();
+}
+
+template <int L, int C, int STAGE>
+static cudaError_t col_modes(const RunDesc *d_runs, int nruns, int M, int mode, const TwiddleSet &tw,
+                             cudaStream_t s) {
+    switch (mode) {
+        case COL_STEP: return col_impl<L, C, COL_STEP, STAGE>(d_runs, nruns, M, tw, s);
+        case COL_PREPARE: return col_impl<L, C, COL_PREPARE, STAGE>(d_runs, nruns, M, tw, s);
+        case COL_STEP_CHECKPOINT: return col_impl<L, C, COL_STEP_CHECKPOINT, STAGE>(d_runs, nruns, M, tw, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+template <int L, int C>
+static cudaError_t col_stages(const RunDesc *d_runs, int nruns, int M, int stage, int mode, const TwiddleSet &tw,
+                              cudaStream_t s) {
+    switch (stage) {
+        case STAGE_ASYNC: return col_modes<L, C, STAGE_ASYNC>(d_runs, nruns, M, mode, tw, s);
+        case STAGE_BULK: return col_modes<L, C, STAGE_BULK>(d_runs, nruns, M, mode, tw, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int L>
+static cudaError_t col_dispatch(const RunDesc *d_runs, int nruns, int M, int C, int stage, int mode,
+                                const TwiddleSet &tw, cudaStream_t s) {
+    switch (C) {
+        case 1:
+            if constexpr (col_tile_ok(L, 1)) return col_stages<L, 1>(d_runs, nruns, M, stage, mode, tw, s);
+            break;
+        case 2:
+            if constexpr (col_tile_ok(L, 2)) return col_stages<L, 2>(d_runs, nruns, M, stage, mode, tw, s);
+            break;
+        case 4:
+            if constexpr (col_tile_ok(L, 4)) return col_stages<L, 4>(d_runs, nruns, M, stage, mode, tw, s);
+            break;
+        case 8:
+            if constexpr (col_tile_ok(L, 8)) return col_stages<L, 8>(d_runs, nruns, M, stage, mode, tw, s);
+            break;
+        case 16:
+            if constexpr (col_tile_ok(L, 16)) return col_stages<L, 16>(d_runs, nruns, M, stage, mode, tw, s);
+            break;
+        default: break;
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <int L>
+cudaError_t launch_col_f32_L(const RunDesc *d_runs, int nruns, int M, int C, int stage, int mode,
+                             const TwiddleSet &tw, cudaStream_t s) {
+    return col_dispatch<L>(d_runs, nruns, M, C, stage, mode, tw, s);
+}
+
+}  // namespace pfc

@@ -53,9 +53,13 @@ static constexpr double PI_REF = 3.1415926;  // pfc_common.h:152
 static std::mutex g_ctx_mu;
 static std::map<int, Context *> g_ctx;
 
+// The word is cleared once it has been reported: the call that synchronised the work
+// whose wait gave up returns the error, and later work on the device starts clean.
 int fault_status(const Context *c) {
-    if (c && c->fault && *c->fault != 0)
+    if (c && c->fault && *c->fault != 0) {
+        *c->fault = 0;
         return set_error(PFC_E_CUDA, "column kernel: a tile copy did not arrive within its bounded wait");
+    }
     return PFC_OK;
 }
 
@@ -201,15 +205,15 @@ static C2Params c2_params(float sig, float g1, float g2, float k1, float k2, flo
 // and dx use one table, so a batch of such runs reads it from L2.
 // ---------------------------------------------------------------------------
 struct KcoefKey {
-    int device, model, L, M, CT;
+    int device, model, prec, L, M, N, CT;
     uint32_t sig, dt, dx;
     bool operator<(const KcoefKey &o) const {
-        return std::tie(device, model, L, M, CT, sig, dt, dx) <
-               std::tie(o.device, o.model, o.L, o.M, o.CT, o.sig, o.dt, o.dx);
+        return std::tie(device, model, prec, L, M, N, CT, sig, dt, dx) <
+               std::tie(o.device, o.model, o.prec, o.L, o.M, o.N, o.CT, o.sig, o.dt, o.dx);
     }
 };
 struct KcoefEntry {
-    float2 *ptr = nullptr;
+    void *ptr = nullptr;
     int refs = 0;
 };
 static std::mutex g_kcoef_mu;
@@ -222,21 +226,60 @@ static uint32_t fbits(float f) {
 }
 
 static KcoefKey kcoef_key(const pfc_run *r) {
-    return KcoefKey{r->p.device, r->p.model, r->L, r->M, r->desc.CT, fbits(r->p.sig), fbits(r->p.dt), fbits(r->p.dx)};
+    return KcoefKey{r->p.device, r->p.model, r->p.precision, r->L, r->M, r->N, r->desc.CT,
+                    fbits(r->p.sig), fbits(r->p.dt), fbits(r->p.dx)};
+}
+
+// Bytes per k point of the shared table: (kden, kc2) float2 pairs on the FP32 path,
+// (kmix, kc2d) = double4 + double2 on the mixed path.
+static size_t kcoef_point_bytes(int prec) {
+    return prec == PFC_PRECISION_MIXED ? sizeof(double4) + sizeof(double2) : 2 * sizeof(float2);
+}
+
+// Pure-FP64 C2 parameters (the oracle's pure mode of MIS:700-750): crossover, peak
+// heights exp(-(sig/sigM)^2), peak positions and Gaussian widths 2 g^2, all in double.
+static C2ParamsD c2_params_pure(float sig, float g1, float g2, float k1, float k2, float s1, float s2) {
+    const double daa1 = std::pow((double)sig / s1, 2), daa2 = std::pow((double)sig / s2, 2);
+    const double dbb1 = 1. / (2. * g1 * g1), dbb2 = 1. / (2. * g2 * g2);
+    const double dD = dbb1 * k1 - dbb2 * k2;
+    const double dE = daa1 - daa2 + dbb1 * k1 * k1 - dbb2 * k2 * k2;
+    double dkc = (dD + std::sqrt(dD * dD - (dbb1 - dbb2) * dE)) / (dbb1 - dbb2);
+    if (g1 == g2) dkc = (daa2 - daa1 + dbb1 * ((double)k2 * k2 - (double)k1 * k1)) / (2 * dbb1 * ((double)k2 - k1));
+    const double q1 = (double)sig / s1, q2 = (double)sig / s2;
+    C2ParamsD p;
+    p.kc = dkc;
+    p.e1 = std::exp(-q1 * q1);
+    p.e2 = std::exp(-q2 * q2);
+    p.k1 = k1;
+    p.k2 = k2;
+    p.gg1 = 2.0 * g1 * g1;
+    p.gg2 = 2.0 * g2 * g2;
+    return p;
 }
 
 // Table for run r (its descriptor must already be on the device); built on first use.
 static int acquire_kcoef(pfc_run *r) {
     std::lock_guard<std::mutex> lk(g_kcoef_mu);
     KcoefEntry &e = g_kcoef[kcoef_key(r)];
+    const size_t npts = (size_t)r->desc.T * r->L * r->desc.CT;
+    const bool mixed = r->p.precision == PFC_PRECISION_MIXED;
     if (!e.ptr) {
-        const size_t bytes = 2 * (size_t)r->desc.T * r->L * r->desc.CT * sizeof(float2);
+        const size_t bytes = npts * kcoef_point_bytes(r->p.precision);
         cudaError_t ce = cudaMalloc(&e.ptr, bytes);
         if (ce != cudaSuccess) {
             e.ptr = nullptr;
             return set_error(PFC_E_NOMEM, std::string("cudaMalloc coefficient table: ") + cudaGetErrorString(ce));
         }
-        ce = launch_build_kcoef(r->d_desc, e.ptr, e.ptr + (size_t)r->desc.T * r->L * r->desc.CT, r->stream);
+        if (mixed) {
+            const ModelCoefs &k = r->k;
+            const C2ParamsD ca = c2_params_pure(r->p.sig, k.gaa1, k.gaa2, k.ka1, k.ka2, k.sigMa1, k.sigMa2);
+            const C2ParamsD cb = c2_params_pure(r->p.sig, k.gab1, k.gab2, k.kb1, k.kb2, k.sigMb1, k.sigMb2);
+            ce = launch_build_kmix(r->d_desc, (double)k.dynamic_mn * (double)r->p.dt,
+                                   (double)k.dynamic_mc * (double)r->p.dt, (double)k.para_alpha, ca, cb,
+                                   (double4 *)e.ptr, (double2 *)((double4 *)e.ptr + npts), r->stream);
+        } else {
+            ce = launch_build_kcoef(r->d_desc, (float2 *)e.ptr, (float2 *)e.ptr + npts, r->stream);
+        }
         if (ce == cudaSuccess) ce = cudaStreamSynchronize(r->stream);
         if (ce != cudaSuccess) {
             cudaFree(e.ptr);
@@ -245,13 +288,20 @@ static int acquire_kcoef(pfc_run *r) {
         }
     }
     e.refs++;
-    r->desc.kden = e.ptr;
-    r->desc.kc2 = e.ptr + (size_t)r->desc.T * r->L * r->desc.CT;
+    if (mixed) {
+        r->desc.kmix = (const double4 *)e.ptr;
+        r->desc.kc2d = (const double2 *)((const double4 *)e.ptr + npts);
+    } else {
+        r->desc.kden = (const float2 *)e.ptr;
+        r->desc.kc2 = (const float2 *)e.ptr + npts;
+    }
+    r->kcoef_held = true;
     return PFC_OK;
 }
 
 static void release_kcoef(pfc_run *r) {
-    if (!r->desc.kden) return;
+    if (!r->kcoef_held) return;
+    r->kcoef_held = false;
     std::lock_guard<std::mutex> lk(g_kcoef_mu);
     auto it = g_kcoef.find(kcoef_key(r));
     if (it == g_kcoef.end()) return;
@@ -261,6 +311,8 @@ static void release_kcoef(pfc_run *r) {
     }
     r->desc.kden = nullptr;
     r->desc.kc2 = nullptr;
+    r->desc.kmix = nullptr;
+    r->desc.kc2d = nullptr;
 }
 
 // k-vectors exactly as MIS:455-462 (float storage, double arithmetic).
@@ -293,15 +345,30 @@ static unsigned long long noise_key(uint32_t seed) {
     return z ^ (z >> 31);
 }
 
+bool fused_path(int prec) { return prec == PFC_PRECISION_FP32 || prec == PFC_PRECISION_MIXED; }
+
 // Bytes of a run's own device allocation with column tile width ct: 8 row-space
-// arrays (FP32 path) + 2 real fields + k tables + partials + result slots + descriptor.
-static size_t run_state_bytes(int L, int M, int N, bool fp32, int ct) {
+// arrays (fused paths) + 2 real fields + k tables (float; and double on the mixed
+// path) + partials + result slots + descriptor.
+static size_t run_state_bytes(int L, int M, int N, int prec, int ct) {
+    const bool fused = fused_path(prec);
     const int Hp = round_up(M / 2 + 1, ct);
     const size_t rs = (size_t)L * Hp * sizeof(float2);
     const size_t real = (size_t)L * M * N * sizeof(float);
     const size_t ktab = (size_t)(L + M + N + 1) * sizeof(float);  // k-vectors + the step counter
-    const size_t parts = (size_t)(2 * analysis_partials(L, M) + 4096) * sizeof(double);
-    return (fp32 ? 8 * rs : 0) + 2 * real + round_up((int)ktab, 256) + parts + sizeof(RunDesc) + 1024;
+    const size_t kdtab = prec == PFC_PRECISION_MIXED ? (size_t)(L + M) * sizeof(double) : 0;
+    const int parts_n = fused ? analysis_partials(L, M, prec) : analysis_partials(L, M, PFC_PRECISION_FP32);
+    const size_t parts = (size_t)(2 * parts_n + 4096) * sizeof(double);
+    return (fused ? 8 * rs : 0) + 2 * real + round_up((int)ktab, 256) + round_up((int)kdtab, 256) + parts +
+           sizeof(RunDesc) + 1024;
+}
+
+// Column tile widths of a precision's fused kernels (default and autotuner candidates).
+static int tile_default(int L, int prec) {
+    return prec == PFC_PRECISION_MIXED ? mixed_col_tile_width(L) : col_tile_width(L);
+}
+static int tile_candidates(int L, int prec, int *out) {
+    return prec == PFC_PRECISION_MIXED ? mixed_col_tile_candidates(L, out) : col_tile_candidates(L, out);
 }
 
 }  // namespace pfc
@@ -314,14 +381,14 @@ extern "C" int pfc_run_bytes(const pfc_run_params *p, double *bytes) {
     if (!p || !bytes) return set_error(PFC_E_INVALID, "null argument");
     if (!is_supported_len(p->L) || !is_supported_len(p->M) || p->N < 1)
         return set_error(PFC_E_INVALID, "unsupported grid");
-    const bool fp32 = p->precision == PFC_PRECISION_FP32;
+    const bool fused = fused_path(p->precision);
     // the widest tile the autotuner may choose (the most padding)
     int cand[4];
-    const int nc = col_tile_candidates(p->L, cand);
-    const int ct = nc ? cand[nc - 1] : col_tile_width(p->L);
-    double b = (double)run_state_bytes(p->L, p->M, p->N, fp32, ct);
+    const int nc = tile_candidates(p->L, p->precision, cand);
+    const int ct = nc ? cand[nc - 1] : tile_default(p->L, p->precision);
+    double b = (double)run_state_bytes(p->L, p->M, p->N, p->precision, ct);
     const double P = (double)p->L * p->M * p->N;
-    if (fp32) b += 2.0 * (double)p->L * round_up(p->M / 2 + 1, ct) * sizeof(float2);
+    if (fused) b += (double)p->L * round_up(p->M / 2 + 1, ct) * kcoef_point_bytes(p->precision);
     else b += P * (22.0 * 16.0 + 6.0 * 8.0);
     *bytes = b;
     return PFC_OK;
@@ -355,7 +422,7 @@ extern "C" int pfc_default_params(int model, pfc_run_params *p) {
     p->dx = 0.125f;
     p->con0 = 0.2f;
     p->axx = 0.0f;
-    p->precision = PFC_PRECISION_FP32;
+    p->precision = PFC_PRECISION_MIXED;
     p->device = 0;
     if (model == PFC_MODEL_CVD) {
         p->u0 = 0.01f;
@@ -381,7 +448,7 @@ static void free_run(pfc_run *r) {
     delete r;
 }
 
-static int tile_width_for(int device, int L, int M, int *width, int *stage);
+static int tile_width_for(int device, int L, int M, int prec, int *width, int *stage);
 
 // Create a run; ct_force > 0 fixes the column tile width of an FP32 run (the
 // autotuner's trial runs), 0 takes the grid's tuned width.
@@ -392,29 +459,32 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
     if (!is_supported_len(p->L) || !is_supported_len(p->M))
         return set_error(PFC_E_INVALID, "L and M must be powers of two in [32, 2048]");
     if (p->N < 1 || p->N > 2048 || (p->N & (p->N - 1)) != 0) return set_error(PFC_E_INVALID, "N must be a power of two <= 2048");
-    if (p->N != 1 && p->precision == PFC_PRECISION_FP32)
-        return set_error(PFC_E_INVALID, "the FP32 path supports 2-D grids (N = 1); use an FP64 precision for 3-D");
+    if (p->precision != PFC_PRECISION_FP32 && p->precision != PFC_PRECISION_FP64 &&
+        p->precision != PFC_PRECISION_FP64_PURE && p->precision != PFC_PRECISION_MIXED)
+        return set_error(PFC_E_INVALID, "unknown precision");
+    const bool fused = fused_path(p->precision);
+    if (p->N != 1 && fused)
+        return set_error(PFC_E_INVALID,
+                         "the fused (mixed, FP32) paths take 2-D grids (N = 1); use an FP64 precision for 3-D");
     if (p->N != 1 && p->model == PFC_MODEL_MISFIT) return set_error(PFC_E_INVALID, "Misfit runs are 2-D (N = 1)");
     if (!(p->dt > 0.0f) || !(p->dx > 0.0f)) return set_error(PFC_E_INVALID, "dt and dx must be > 0");
-    if (p->precision != PFC_PRECISION_FP32 && p->precision != PFC_PRECISION_FP64 && p->precision != PFC_PRECISION_FP64_PURE)
-        return set_error(PFC_E_INVALID, "unknown precision");
     if (p->model == PFC_MODEL_MISFIT &&
         (p->grainx <= 0 || p->grainy <= 0 || p->grainz <= 0 || p->grainx > p->L || p->grainy > p->M || p->grainz > p->N))
         return set_error(PFC_E_INVALID, "grain counts must be in [1, grid extent]");
     if (!(p->axx >= 0.0f)) return set_error(PFC_E_INVALID, "axx must be >= 0");
-    if (p->axx > 0.0f && p->model == PFC_MODEL_MISFIT && p->precision != PFC_PRECISION_FP32)
-        return set_error(PFC_E_INVALID, "stochastic noise (axx > 0) runs on the FP32 path only");
+    if (p->axx > 0.0f && p->model == PFC_MODEL_MISFIT && !fused)
+        return set_error(PFC_E_INVALID, "stochastic noise (axx > 0) runs on the fused (mixed, FP32) paths only");
     Context *ctx = nullptr;
     int rc = get_context(p->device, &ctx);
     if (rc != PFC_OK) return rc;
     PFC_CUDA_TRY(cudaSetDevice(p->device));
-    int ct = col_tile_width(p->L), stage = COL_STAGE_BULK;
-    if (p->precision == PFC_PRECISION_FP32) {
+    int ct = tile_default(p->L, p->precision), stage = COL_STAGE_BULK;
+    if (fused) {
         if (ct_force > 0) {
             ct = ct_force;
             stage = stage_force;
         } else {
-            rc = tile_width_for(p->device, p->L, p->M, &ct, &stage);
+            rc = tile_width_for(p->device, p->L, p->M, p->precision, &ct, &stage);
             if (rc != PFC_OK) return rc;
         }
     }
@@ -441,12 +511,13 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
     // device memory: 8 row-space arrays + 2 real fields + k tables + partials + result
     const size_t rs = (size_t)r->L * r->Hp * sizeof(float2);
     const size_t real = (size_t)r->P * sizeof(float);
-    const int nparts = analysis_partials(r->L, r->M);
+    const int nparts = fused ? analysis_partials(r->L, r->M, p->precision)
+                             : analysis_partials(r->L, r->M, PFC_PRECISION_FP32);
     r->nparts = nparts;
     const size_t ktab = (size_t)(r->L + r->M + r->N + 1) * sizeof(float);
+    const size_t kdtab = p->precision == PFC_PRECISION_MIXED ? (size_t)(r->L + r->M) * sizeof(double) : 0;
     const size_t parts = (size_t)(2 * nparts + 4096) * sizeof(double);
-    const bool fp32 = p->precision == PFC_PRECISION_FP32;
-    const size_t bytes = run_state_bytes(r->L, r->M, r->N, fp32, ct);
+    const size_t bytes = run_state_bytes(r->L, r->M, r->N, p->precision, ct);
     cudaError_t e = cudaMalloc(&r->dev_mem, bytes);
     if (e != cudaSuccess) {
         free_run(r);
@@ -456,7 +527,7 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
     char *m = (char *)r->dev_mem;
     RunDesc &d = r->desc;
     std::memset(&d, 0, sizeof(d));
-    if (fp32) {
+    if (fused) {
         float2 **arrs[8] = {&d.psi, &d.con, &d.ca, &d.cb, &d.inn, &d.inc, &d.gx, &d.gy};
         for (int i = 0; i < 8; ++i) {
             *arrs[i] = (float2 *)m;
@@ -473,6 +544,20 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
     d.krefm = kt + r->L;
     r->d_krefn = kt + r->L + r->M;
     d.step_ctr = (int *)(kt + r->L + r->M + r->N);
+    if (kdtab) {
+        // pure-FP64 k-vectors (the oracle's pure mode of MIS:455-462)
+        double *kd = (double *)m;
+        m += round_up((int)kdtab, 256);
+        std::vector<double> h(r->L + r->M);
+        for (int l = 0; l < r->L; ++l)
+            h[l] = (double)(l <= r->L / 2 ? l : l - r->L) * 2.0 * PI_REF / ((double)r->L * p->dx);
+        for (int mm = 0; mm < r->M; ++mm)
+            h[r->L + mm] = (double)(mm <= r->M / 2 ? mm : mm - r->M) * 2.0 * PI_REF / ((double)r->M * p->dx);
+        r->kd_host = h;
+        cudaMemcpyAsync(kd, r->kd_host.data(), kdtab, cudaMemcpyHostToDevice, r->stream);
+        d.kdl = kd;
+        d.kdm = kd + r->L;
+    }
     d.partials = (double *)m;
     r->d_scratch = (double *)m + 2 * nparts;
     m += parts;
@@ -497,7 +582,8 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
     // noise (MIS:490-491, 983-1014): amplitude dt * b0 in float, as the reference's product
     d.noise_amp = (p->model == PFC_MODEL_MISFIT && r->b0 != 0.0f) ? p->dt * r->b0 : 0.0f;
     d.noise_key = noise_key(p->seed);
-    if (fp32) {
+    d.noise_amp_d = (p->model == PFC_MODEL_MISFIT && r->b0 != 0.0f) ? (double)p->dt * (double)r->b0 : 0.0;
+    if (fused) {
         cudaError_t ce = cudaMemcpyAsync(r->d_desc, &d, sizeof(RunDesc), cudaMemcpyHostToDevice, r->stream);
         if (ce != cudaSuccess) {
             free_run(r);
@@ -510,7 +596,7 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
         }
     }
 
-    if (!fp32) {
+    if (!fused) {
         rc = fp64_create(r);
         if (rc != PFC_OK) {
             free_run(r);
@@ -529,12 +615,13 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
 extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) { return run_create(p, 0, 0, out); }
 
 // ---------------------------------------------------------------------------
-// Autotuner: the column tile width of FP32 runs of an L x M grid, and how the column
-// kernel stages its input tiles.  A run's row-space layout and its column kernel's tile
-// both follow the width; every column's transform is the same arithmetic whatever the
-// width or the staging, so the choice changes speed, not results.  On the first FP32
-// run of a grid on a device, each candidate width (col_tile_candidates: the default, a
-// quarter, half and twice it, where the tile fits) runs a batch of Misfit runs of at
+// Autotuner: the column tile width of fused-path runs (FP32 or mixed precision) of an
+// L x M grid, and how the column kernel stages its input tiles.  A run's row-space
+// layout and its column kernel's tile both follow the width; every column's transform
+// is the same arithmetic whatever the width or the staging, so the choice changes
+// speed, not results.  On the first run of a grid and precision on a device, each
+// candidate width (the default, a quarter, half and twice it, where the tile fits:
+// col_tile_candidates, mixed_col_tile_candidates) runs a batch of Misfit runs of at
 // least 2 M points in all (4 to 16 runs) with each staging method: 3 warm-up steps,
 // then 8 steps of the row and column sweeps timed with CUDA events.  The fastest pair
 // is kept for the rest of the process.  PFC_AUTOTUNE=0 in the environment keeps the
@@ -555,11 +642,11 @@ struct TileChoice {
     }
 };
 static std::mutex g_tile_mu;
-static std::map<std::tuple<int, int, int>, TileChoice> g_tile;
+static std::map<std::tuple<int, int, int, int>, TileChoice> g_tile;  // (device, L, M, precision)
 
 // Device time of 8 steps of a trial batch with tile width ct, for each staging method
 // (ms[COL_STAGE_ASYNC], ms[COL_STAGE_BULK]).
-static int time_tile_width(int device, int L, int M, int ct, float ms[2]) {
+static int time_tile_width(int device, int L, int M, int prec, int ct, float ms[2]) {
     const long pts = (long)L * M;
     const int nruns = (int)std::max(4L, std::min(16L, (2L << 20) / pts));
     std::vector<pfc_run *> runs;
@@ -570,6 +657,7 @@ static int time_tile_width(int device, int L, int M, int ct, float ms[2]) {
         p.L = L;
         p.M = M;
         p.device = device;
+        p.precision = prec;
         p.seed = 1000u + (uint32_t)i;
         pfc_run *r = nullptr;
         rc = run_create(&p, ct, COL_STAGE_BULK, &r);
@@ -584,8 +672,8 @@ static int time_tile_width(int device, int L, int M, int ct, float ms[2]) {
         cudaStream_t st = runs[0]->stream;
         const TwiddleSet &tw = runs[0]->ctx->tw;
         auto step = [&](int stage) {
-            cudaError_t x = launch_row_step(d, n, L, M, tw, st);
-            if (x == cudaSuccess) x = launch_col_step(d, n, L, M, ct, stage, COL_STEP, tw, st);
+            cudaError_t x = launch_row_step(d, n, L, M, prec, tw, st);
+            if (x == cudaSuccess) x = launch_col_step(d, n, L, M, ct, stage, COL_STEP, prec, tw, st);
             return x;
         };
         cudaError_t ce = cudaMalloc(&d, h.size() * sizeof(RunDesc));
@@ -611,9 +699,9 @@ static int time_tile_width(int device, int L, int M, int ct, float ms[2]) {
     return rc;
 }
 
-static int tile_width_for(int device, int L, int M, int *width, int *stage) {
+static int tile_width_for(int device, int L, int M, int prec, int *width, int *stage) {
     std::lock_guard<std::mutex> lk(g_tile_mu);
-    const auto key = std::make_tuple(device, L, M);
+    const auto key = std::make_tuple(device, L, M, prec);
     auto it = g_tile.find(key);
     if (it != g_tile.end()) {
         *width = it->second.width;
@@ -621,18 +709,18 @@ static int tile_width_for(int device, int L, int M, int *width, int *stage) {
         return PFC_OK;
     }
     TileChoice c;
-    c.width = col_tile_width(L);
+    c.width = tile_default(L, prec);
     int cand[4];
-    const int nc = col_tile_candidates(L, cand);
+    const int nc = tile_candidates(L, prec, cand);
     const char *env = std::getenv("PFC_AUTOTUNE");
     if (!(env && env[0] == '0')) {
         float best = 0.f;
         for (int i = 0; i < nc; ++i) {
             float ms[2] = {0.f, 0.f};
-            const int rc = time_tile_width(device, L, M, cand[i], ms);
+            const int rc = time_tile_width(device, L, M, prec, cand[i], ms);
             if (rc == PFC_E_NOMEM) {  // no room for trial runs: keep the defaults
                 c = TileChoice{};
-                c.width = col_tile_width(L);
+                c.width = tile_default(L, prec);
                 break;
             }
             if (rc != PFC_OK) return rc;
@@ -653,18 +741,26 @@ static int tile_width_for(int device, int L, int M, int *width, int *stage) {
     return PFC_OK;
 }
 
-extern "C" int pfc_tile_width(int device, int L, int M, int *width, int *candidates, float *trial_ms, int *ntrials) {
-    if (!width) return set_error(PFC_E_INVALID, "null argument");
+static int check_tile_args(int L, int M, int prec) {
     if (!is_supported_len(L) || !is_supported_len(M)) return set_error(PFC_E_INVALID, "unsupported grid");
+    if (!fused_path(prec)) return set_error(PFC_E_INVALID, "tile widths belong to the fused (mixed, FP32) paths");
+    return PFC_OK;
+}
+
+extern "C" int pfc_tile_width(int device, int L, int M, int precision, int *width, int *candidates, float *trial_ms,
+                              int *ntrials) {
+    if (!width) return set_error(PFC_E_INVALID, "null argument");
+    int rc = check_tile_args(L, M, precision);
+    if (rc != PFC_OK) return rc;
     Context *ctx = nullptr;
-    int rc = get_context(device, &ctx);
+    rc = get_context(device, &ctx);
     if (rc != PFC_OK) return rc;
     PFC_CUDA_TRY(cudaSetDevice(device));
     int stage = 0;
-    rc = tile_width_for(device, L, M, width, &stage);
+    rc = tile_width_for(device, L, M, precision, width, &stage);
     if (rc != PFC_OK) return rc;
     std::lock_guard<std::mutex> lk(g_tile_mu);
-    const TileChoice &c = g_tile[std::make_tuple(device, L, M)];
+    const TileChoice &c = g_tile[std::make_tuple(device, L, M, precision)];
     if (ntrials) *ntrials = c.n;
     for (int i = 0; i < c.n; ++i) {
         if (candidates) candidates[i] = c.cand[i];
@@ -673,18 +769,20 @@ extern "C" int pfc_tile_width(int device, int L, int M, int *width, int *candida
     return PFC_OK;
 }
 
-extern "C" int pfc_col_staging(int device, int L, int M, int *stage, float *ms_async, float *ms_bulk, int *ntrials) {
+extern "C" int pfc_col_staging(int device, int L, int M, int precision, int *stage, float *ms_async, float *ms_bulk,
+                               int *ntrials) {
     if (!stage) return set_error(PFC_E_INVALID, "null argument");
-    if (!is_supported_len(L) || !is_supported_len(M)) return set_error(PFC_E_INVALID, "unsupported grid");
+    int rc = check_tile_args(L, M, precision);
+    if (rc != PFC_OK) return rc;
     Context *ctx = nullptr;
-    int rc = get_context(device, &ctx);
+    rc = get_context(device, &ctx);
     if (rc != PFC_OK) return rc;
     PFC_CUDA_TRY(cudaSetDevice(device));
     int width = 0;
-    rc = tile_width_for(device, L, M, &width, stage);
+    rc = tile_width_for(device, L, M, precision, &width, stage);
     if (rc != PFC_OK) return rc;
     std::lock_guard<std::mutex> lk(g_tile_mu);
-    const TileChoice &c = g_tile[std::make_tuple(device, L, M)];
+    const TileChoice &c = g_tile[std::make_tuple(device, L, M, precision)];
     if (ntrials) *ntrials = c.n;
     for (int i = 0; i < c.n; ++i) {
         if (ms_async) ms_async[i] = c.ms[i][COL_STAGE_ASYNC];
@@ -693,15 +791,17 @@ extern "C" int pfc_col_staging(int device, int L, int M, int *stage, float *ms_a
     return PFC_OK;
 }
 
-extern "C" int pfc_set_col_staging(int device, int L, int M, int stage) {
-    if (!is_supported_len(L) || !is_supported_len(M)) return set_error(PFC_E_INVALID, "unsupported grid");
+extern "C" int pfc_set_col_staging(int device, int L, int M, int precision, int stage) {
+    int rc = check_tile_args(L, M, precision);
+    if (rc != PFC_OK) return rc;
     if (stage != COL_STAGE_ASYNC && stage != COL_STAGE_BULK) return set_error(PFC_E_INVALID, "unknown staging");
     std::lock_guard<std::mutex> lk(g_tile_mu);
-    auto it = g_tile.find(std::make_tuple(device, L, M));
+    const auto key = std::make_tuple(device, L, M, precision);
+    auto it = g_tile.find(key);
     if (it == g_tile.end()) {
         TileChoice c;
-        c.width = col_tile_width(L);
-        it = g_tile.emplace(std::make_tuple(device, L, M), c).first;
+        c.width = tile_default(L, precision);
+        it = g_tile.emplace(key, c).first;
     }
     it->second.stage = stage;  // a trial record, if any, is kept
     return PFC_OK;
@@ -752,15 +852,16 @@ extern "C" int pfc_selftest_tile_stage(int device, int issue, int n, double limi
     return PFC_OK;
 }
 
-extern "C" int pfc_set_tile_width(int device, int L, int M, int width) {
-    if (!is_supported_len(L) || !is_supported_len(M)) return set_error(PFC_E_INVALID, "unsupported grid");
+extern "C" int pfc_set_tile_width(int device, int L, int M, int precision, int width) {
+    int rc = check_tile_args(L, M, precision);
+    if (rc != PFC_OK) return rc;
     int cand[4];
-    const int nc = col_tile_candidates(L, cand);
+    const int nc = tile_candidates(L, precision, cand);
     bool ok = false;
     for (int i = 0; i < nc; ++i) ok = ok || cand[i] == width;
     if (!ok) return set_error(PFC_E_INVALID, "tile width not available for this grid");
     std::lock_guard<std::mutex> lk(g_tile_mu);
-    TileChoice &c = g_tile[std::make_tuple(device, L, M)];
+    TileChoice &c = g_tile[std::make_tuple(device, L, M, precision)];
     c.width = width;  // a trial record, if any, is kept
     c.stage = c.best_stage(width);
     return PFC_OK;
@@ -864,9 +965,10 @@ static int fp32_from_real(pfc_run *r, bool means_from_device) {
     // the row kernel of step t advances the counter to t before the column kernel reads it
     r->step_ctr_init = r->t - 1;
     PFC_CUDA_TRY(cudaMemcpyAsync(d.step_ctr, &r->step_ctr_init, sizeof(int), cudaMemcpyHostToDevice, r->stream));
-    PFC_CUDA_TRY(launch_row_forward(r->d_desc, 1, r->L, r->M, r->ctx->tw, r->stream));
-    PFC_CUDA_TRY(
-        launch_col_step(r->d_desc, 1, r->L, r->M, r->desc.CT, r->desc.stage, COL_PREPARE, r->ctx->tw, r->stream));
+    const int prec = r->p.precision;
+    PFC_CUDA_TRY(launch_row_forward(r->d_desc, 1, r->L, r->M, prec, r->ctx->tw, r->stream));
+    PFC_CUDA_TRY(launch_col_step(r->d_desc, 1, r->L, r->M, r->desc.CT, r->desc.stage, COL_PREPARE, prec, r->ctx->tw,
+                                 r->stream));
     PFC_SYNC_CHECKED(r->ctx, r->stream);
     r->fields_valid = true;
     r->energy_valid = false;
@@ -878,7 +980,7 @@ int pfc_run_init_state(pfc_run *r) {
     int rc = init_real_fields(r);
     if (rc != PFC_OK) return rc;
     r->t = 0;
-    if (r->p.precision != PFC_PRECISION_FP32) return fp64_init_from_real(r, true);
+    if (!fused_path(r->p.precision)) return fp64_init_from_real(r, true);
     return fp32_from_real(r, true);
 }
 
@@ -890,18 +992,20 @@ extern "C" int pfc_run_destroy(pfc_run *r) {
     return PFC_OK;
 }
 
-static int fp32_advance(pfc_run *r, int nsteps, int analysis) {
+static int fused_advance(pfc_run *r, int nsteps, int analysis) {
+    const int prec = r->p.precision;
     for (int i = 0; i < nsteps; ++i) {
         const bool last = i == nsteps - 1;
-        PFC_CUDA_TRY(launch_row_step(r->d_desc, 1, r->L, r->M, r->ctx->tw, r->stream));
+        PFC_CUDA_TRY(launch_row_step(r->d_desc, 1, r->L, r->M, prec, r->ctx->tw, r->stream));
         PFC_CUDA_TRY(launch_col_step(r->d_desc, 1, r->L, r->M, r->desc.CT, r->desc.stage,
-                                     (last && analysis) ? COL_STEP_CHECKPOINT : COL_STEP, r->ctx->tw, r->stream));
+                                     (last && analysis) ? COL_STEP_CHECKPOINT : COL_STEP, prec, r->ctx->tw,
+                                     r->stream));
     }
     r->t += nsteps;
     r->fields_valid = false;
     r->energy_valid = false;
     if (analysis) {
-        PFC_CUDA_TRY(launch_row_analysis(r->d_desc, 1, r->L, r->M, r->ctx->tw, r->stream));
+        PFC_CUDA_TRY(launch_row_analysis(r->d_desc, 1, r->L, r->M, prec, r->ctx->tw, r->stream));
         PFC_CUDA_TRY(launch_reduce_fixed(r->desc.partials, r->nparts, 2, 2, r->d_scratch, r->stream));
         r->fields_valid = true;
         r->energy_valid = true;
@@ -913,8 +1017,8 @@ extern "C" int pfc_run_advance(pfc_run *r, int nsteps, int analysis) {
     if (!r || nsteps < 0) return set_error(PFC_E_INVALID, "bad run or step count");
     if (nsteps == 0) return PFC_OK;
     PFC_CUDA_TRY(cudaSetDevice(r->p.device));
-    if (r->p.precision != PFC_PRECISION_FP32) return fp64_advance(r, nsteps);
-    return fp32_advance(r, nsteps, analysis);
+    if (!fused_path(r->p.precision)) return fp64_advance(r, nsteps);
+    return fused_advance(r, nsteps, analysis);
 }
 
 extern "C" int pfc_run_advance_timed(pfc_run *r, int nsteps, float *ms) {
@@ -945,9 +1049,9 @@ extern "C" int pfc_run_steps(const pfc_run *r, int *steps) {
 
 // Make d.psi_real / d.con_real hold the current state.
 static int materialize(pfc_run *r) {
-    if (r->p.precision != PFC_PRECISION_FP32) return fp64_materialize(r);
+    if (!fused_path(r->p.precision)) return fp64_materialize(r);
     if (r->fields_valid) return PFC_OK;
-    PFC_CUDA_TRY(launch_row_analysis(r->d_desc, 1, r->L, r->M, r->ctx->tw, r->stream));
+    PFC_CUDA_TRY(launch_row_analysis(r->d_desc, 1, r->L, r->M, r->p.precision, r->ctx->tw, r->stream));
     r->fields_valid = true;
     return PFC_OK;
 }
@@ -965,7 +1069,7 @@ extern "C" int pfc_run_get_fields_f32(pfc_run *r, float *phi, float *con) {
 
 extern "C" int pfc_run_get_fields(pfc_run *r, double *phi, double *con) {
     if (!r) return set_error(PFC_E_INVALID, "null run");
-    if (r->p.precision != PFC_PRECISION_FP32) return fp64_get_fields(r, phi, con);
+    if (!fused_path(r->p.precision)) return fp64_get_fields(r, phi, con);
     std::vector<float> a(phi ? r->P : 0), b(con ? r->P : 0);
     int rc = pfc_run_get_fields_f32(r, phi ? a.data() : nullptr, con ? b.data() : nullptr);
     if (rc != PFC_OK) return rc;
@@ -1035,7 +1139,7 @@ static void convert_fields(const double *phi, const double *con, long P, float *
 extern "C" int pfc_run_set_fields(pfc_run *r, const double *phi, const double *con) {
     if (!r || !phi || !con) return set_error(PFC_E_INVALID, "null argument");
     PFC_CUDA_TRY(cudaSetDevice(r->p.device));
-    if (r->p.precision != PFC_PRECISION_FP32) return fp64_set_fields(r, phi, con);
+    if (!fused_path(r->p.precision)) return fp64_set_fields(r, phi, con);
     // converted into the context's pinned staging buffer and uploaded from there; the
     // buffer is held until fp32_from_real has synchronised the stream
     Context *ctx = r->ctx;
@@ -1060,7 +1164,7 @@ extern "C" int pfc_run_set_fields(pfc_run *r, const double *phi, const double *c
 extern "C" int pfc_run_energy(pfc_run *r, double *e_over_p, double *mass_over_p) {
     if (!r) return set_error(PFC_E_INVALID, "null run");
     PFC_CUDA_TRY(cudaSetDevice(r->p.device));
-    if (r->p.precision != PFC_PRECISION_FP32) return fp64_energy(r, e_over_p, mass_over_p);
+    if (!fused_path(r->p.precision)) return fp64_energy(r, e_over_p, mass_over_p);
     if (!r->energy_valid) return set_error(PFC_E_STATE, "energy is available after pfc_run_advance(..., analysis=1)");
     double s[2];
     PFC_CUDA_TRY(cudaMemcpyAsync(s, r->d_scratch, sizeof(s), cudaMemcpyDeviceToHost, r->stream));
@@ -1082,7 +1186,7 @@ extern "C" int pfc_run_means(const pfc_run *r, double *phi_mean, double *con_mea
 // captured once into a CUDA graph per step count.
 // ---------------------------------------------------------------------------
 struct SizeClass {
-    int L, M, CT, stage;
+    int L, M, CT, stage, prec;
     std::vector<pfc_run *> runs;
     RunDesc *d_descs = nullptr;
 };
@@ -1102,7 +1206,8 @@ extern "C" int pfc_batch_create(pfc_run *const *runs, int nruns, pfc_batch **out
     const int dev = runs[0]->p.device;
     for (int i = 0; i < nruns; ++i) {
         if (!runs[i]) return set_error(PFC_E_INVALID, "null run in batch");
-        if (runs[i]->p.precision != PFC_PRECISION_FP32) return set_error(PFC_E_INVALID, "batches hold FP32 runs only");
+        if (!fused_path(runs[i]->p.precision))
+            return set_error(PFC_E_INVALID, "batches hold fused-path (mixed, FP32) runs only");
         if (runs[i]->p.device != dev) return set_error(PFC_E_INVALID, "batch runs must share one device");
     }
     PFC_CUDA_TRY(cudaSetDevice(dev));
@@ -1113,11 +1218,12 @@ extern "C" int pfc_batch_create(pfc_run *const *runs, int nruns, pfc_batch **out
     for (int i = 0; i < nruns; ++i) {
         SizeClass *sc = nullptr;
         for (auto &c : b->classes)
-            if (c.L == runs[i]->L && c.M == runs[i]->M && c.CT == runs[i]->desc.CT && c.stage == runs[i]->desc.stage)
+            if (c.L == runs[i]->L && c.M == runs[i]->M && c.CT == runs[i]->desc.CT && c.stage == runs[i]->desc.stage &&
+                c.prec == runs[i]->p.precision)
                 sc = &c;
         if (!sc) {
-            b->classes.push_back(
-                SizeClass{runs[i]->L, runs[i]->M, runs[i]->desc.CT, runs[i]->desc.stage, {}, nullptr});
+            b->classes.push_back(SizeClass{runs[i]->L, runs[i]->M, runs[i]->desc.CT, runs[i]->desc.stage,
+                                           runs[i]->p.precision, {}, nullptr});
             sc = &b->classes.back();
         }
         sc->runs.push_back(runs[i]);
@@ -1149,11 +1255,11 @@ extern "C" int pfc_batch_destroy(pfc_batch *b) {
 static int batch_enqueue(pfc_batch *b, int nsteps) {
     for (int i = 0; i < nsteps; ++i) {
         for (auto &c : b->classes)
-            PFC_CUDA_TRY(launch_row_step(c.d_descs, (int)c.runs.size(), c.L, c.M, b->ctx->tw, b->stream));
+            PFC_CUDA_TRY(launch_row_step(c.d_descs, (int)c.runs.size(), c.L, c.M, c.prec, b->ctx->tw, b->stream));
         for (auto &c : b->classes)
             PFC_CUDA_TRY(
-                launch_col_step(c.d_descs, (int)c.runs.size(), c.L, c.M, c.CT, c.stage, COL_STEP, b->ctx->tw,
-                                b->stream));
+                launch_col_step(c.d_descs, (int)c.runs.size(), c.L, c.M, c.CT, c.stage, COL_STEP, c.prec,
+                                b->ctx->tw, b->stream));
     }
     return PFC_OK;
 }
@@ -1190,12 +1296,12 @@ extern "C" int pfc_batch_kernel_times(pfc_batch *b, int reps, double *row_ms, do
     for (int i = 0; i < reps; ++i) {
         PFC_CUDA_TRY(cudaEventRecord(ev[3 * i], b->stream));
         for (auto &c : b->classes)
-            PFC_CUDA_TRY(launch_row_step(c.d_descs, (int)c.runs.size(), c.L, c.M, b->ctx->tw, b->stream));
+            PFC_CUDA_TRY(launch_row_step(c.d_descs, (int)c.runs.size(), c.L, c.M, c.prec, b->ctx->tw, b->stream));
         PFC_CUDA_TRY(cudaEventRecord(ev[3 * i + 1], b->stream));
         for (auto &c : b->classes)
             PFC_CUDA_TRY(
-                launch_col_step(c.d_descs, (int)c.runs.size(), c.L, c.M, c.CT, c.stage, COL_STEP, b->ctx->tw,
-                                b->stream));
+                launch_col_step(c.d_descs, (int)c.runs.size(), c.L, c.M, c.CT, c.stage, COL_STEP, c.prec,
+                                b->ctx->tw, b->stream));
         PFC_CUDA_TRY(cudaEventRecord(ev[3 * i + 2], b->stream));
     }
     PFC_SYNC_CHECKED(b->ctx, b->stream);
@@ -1231,7 +1337,7 @@ extern "C" int pfc_batch_advance(pfc_batch *b, int nsteps) {
             b->graph = nullptr;
         }
         // kernel attribute setup (max dynamic shared memory) happens outside the capture
-        for (auto &c : b->classes) PFC_CUDA_TRY(prepare_size(c.L, c.M, c.CT, c.stage));
+        for (auto &c : b->classes) PFC_CUDA_TRY(prepare_size(c.L, c.M, c.CT, c.stage, c.prec));
         int rc = PFC_OK;
         cudaGraph_t g = nullptr;
         PFC_CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));

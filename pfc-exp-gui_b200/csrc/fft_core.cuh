@@ -52,6 +52,13 @@ __device__ __forceinline__ double2 cmulc(double2 a, double2 b) {
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
 
+// widen a stored value to the arithmetic type of a transform (float2 -> double2 for the
+// mixed-precision path; the identity otherwise)
+template <typename C> __device__ __forceinline__ C to_c(float2 v);
+template <> __device__ __forceinline__ float2 to_c<float2>(float2 v) { return v; }
+template <> __device__ __forceinline__ double2 to_c<double2>(float2 v) { return make_double2(v.x, v.y); }
+template <typename C> __device__ __forceinline__ C to_c(double2 v) { return v; }
+
 // multiply by -i (forward) or +i (inverse)
 template <bool FWD, typename C> __device__ __forceinline__ C mul_mi(C a) {
     return FWD ? mk(a.y, -a.x) : mk(-a.y, a.x);
@@ -254,8 +261,11 @@ struct Identity {
 // item w = tid + q*NT, b = w % NB, j = w / NB) and nothing is stored.
 // A stage whose input and output are the same shared array synchronises between
 // its loads and its stores.
-template <int N, int NB, int NT, int R, int NS, bool FWD, int IN, int OUT, typename C, typename XF = Identity>
-__device__ __forceinline__ void stage(const C *__restrict__ in, typename nodeduce<C>::type *out, const C *__restrict__ tw,
+// A stage that reads global memory (or an unpadded staging buffer) may read a narrower
+// stored type CI than its arithmetic type C (float2 into double2 arithmetic).
+template <int N, int NB, int NT, int R, int NS, bool FWD, int IN, int OUT, typename C, typename XF = Identity,
+          typename CI = C>
+__device__ __forceinline__ void stage(const CI *__restrict__ in, typename nodeduce<C>::type *out, const C *__restrict__ tw,
                                       C (&v)[StageShape<N, NB, NT, R>::PER_T][R], XF xf = XF()) {
     typedef StageShape<N, NB, NT, R> S;
     constexpr int DIN = (N / R) * NB;  // element offset between a butterfly's inputs
@@ -273,7 +283,7 @@ __device__ __forceinline__ void stage(const C *__restrict__ in, typename nodeduc
             for (int r = 0; r < R; ++r) {
                 C x;
                 if constexpr (IN != SP_SMEM)
-                    x = in[w + r * DIN];
+                    x = to_c<C>(in[w + r * DIN]);
                 else if constexpr (DIN % 16 == 0)  // spad(w + r*DIN) = spad(w) + r*DIN*17/16
                     x = in[pw + r * (DIN + DIN / 16)];
                 else
@@ -349,8 +359,9 @@ struct NoHook {
 // stage af() runs.  Callers must __syncthreads() before a transform that reads
 // shared data they wrote; a transform whose last stage writes shared memory
 // synchronises before returning.
-template <int N, int NB, int NT, bool FWD, int IN, int OUT, typename C, typename XF = Identity, typename AF = NoHook>
-__device__ __forceinline__ void fft(const typename nodeduce<C>::type *src, C *s, typename nodeduce<C>::type *dst,
+template <int N, int NB, int NT, bool FWD, int IN, int OUT, typename C, typename XF = Identity, typename AF = NoHook,
+          typename CI = C>
+__device__ __forceinline__ void fft(const CI *src, C *s, typename nodeduce<C>::type *dst,
                                     const C *__restrict__ tw,
                                     C (&last)[RegOut<N, NB, NT>::PER_T][RegOut<N, NB, NT>::R], XF xf = XF(),
                                     AF af = AF()) {

@@ -1,0 +1,237 @@
+// mcol_kernel.cuh -- the column kernel of the mixed-precision fused step (FP32 tiles in
+// HBM, FP64 arithmetic), and its launchers.
+//
+// Instantiated one row length L per translation unit (col_inst.cu compiled with
+// PFC_COL_L = L); step_mixed.cu reaches it through launch_col_mixed_L<L>.
+#pragma once
+
+#include "step_common.cuh"
+
+namespace pfc {
+
+// Column tile of the mixed path: L rows x C packed columns, 512 <= C*L <= 4096 complex
+// values (two padded double2 buffers and an FP32 staging buffer: 43 KB to 172 KB).
+constexpr bool mcol_tile_ok(int L, int C) { return C >= 1 && C <= COL_TILE_MAX && C * L >= 512 && C * L <= 4096; }
+template <int L, int C> struct MColCfg {
+    static constexpr int NT = (C * L / 16) < 32 ? 32 : (C * L / 16);
+    static constexpr int SMEM = 2 * (int)sizeof(double2) * padded_len<C * L>::value + (int)sizeof(float2) * C * L;
+    static constexpr int FIT = (228 * 1024) / (SMEM + 1024);  // CTAs per SM the shared memory leaves room for
+    static constexpr int MINB = FIT > 8 ? 8 : (FIT < 1 ? 1 : FIT);
+};
+
+__device__ __forceinline__ double2 wide(float2 v) { return make_double2(v.x, v.y); }
+__device__ __forceinline__ float2 narrow(double2 v) { return make_float2((float)v.x, (float)v.y); }
+
+// ---------------------------------------------------------------------------
+// Column kernel.
+// ---------------------------------------------------------------------------
+// multiplier of an inverse transform's first stage: P * C2A (which = 0) or C2B (which = 1)
+struct ScaleByTableD {
+    const double2 *tab;
+    int C, which;
+    __device__ __forceinline__ double2 operator()(int e, int b, double2 v) const {
+        const double2 t = tab[e * C + b];
+        const double g = which == 0 ? t.x : t.y;
+        return make_double2(v.x * g, v.y * g);
+    }
+};
+// -i k P along l (which = 0) or m (which = 1), double k-vectors
+struct GradientOfD {
+    const double *kdl, *kdm;
+    int km0, H, which;
+    __device__ __forceinline__ double2 operator()(int e, int b, double2 v) const {
+        const int km = km0 + b;
+        const double kv = which == 0 ? kdl[e] : kdm[km <= H ? km : 0];
+        return make_double2(kv * v.y, -kv * v.x);
+    }
+};
+// padded shared double2 tile -> FP32 tile in HBM (16-byte stores)
+template <int L, int C, int NT> __device__ __forceinline__ void tile_out_d(const double2 *sm, float2 *__restrict__ g) {
+    float4 *g4 = reinterpret_cast<float4 *>(g);
+    for (int i = threadIdx.x; i < L * C / 2; i += NT) {
+        const double2 a = sm[spad(2 * i)], b = sm[spad(2 * i + 1)];
+        g4[i] = make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
+    }
+}
+
+// Work item = (tile, run), tile-major: item i is tile i / nruns of run i % nruns.  CTA j
+// takes items [j*per, (j+1)*per).  Per item, as the FP32 column kernel: for phi and then
+// con, the field's tile is transformed forward into the parked buffer P, the nonlinear
+// term's tile forward into s, the update runs in P, and each output is an inverse
+// transform whose first stage reads P through a multiplier.  Inputs are staged (FP32)
+// into Q by cp.async or one TMA bulk copy per tile (bounded waits; a CTA whose copy
+// does not arrive sets the context's fault word and returns), each issued as soon as
+// the previous transform's first stage has read Q.
+template <int L, int C, int MODE, int STAGE>
+__global__ void __launch_bounds__(MColCfg<L, C>::NT, MColCfg<L, C>::MINB)
+    k_mcol_step(const RunDesc *__restrict__ runs, int nruns, int per, const double2 *__restrict__ tw, int *fault) {
+    constexpr int NT = MColCfg<L, C>::NT;
+    constexpr int SPAD = padded_len<C * L>::value;
+    typedef RegOut<L, C, NT> RO;
+    extern __shared__ __align__(16) double2 smd[];
+    __shared__ __align__(8) unsigned long long stage_bar;
+    double2 *s = smd;                                         // FFT scratch
+    double2 *Pk = smd + SPAD;                                 // parked spectrum
+    float2 *Q = reinterpret_cast<float2 *>(smd + 2 * SPAD);  // FP32 staging buffer (16-byte aligned)
+    const int T = runs[0].T;                                  // all runs of a launch share L, M and CT
+    const int items = nruns * T;
+    const int first = blockIdx.x * per;
+    const int end = first + per < items ? first + per : items;
+    if (first >= end) return;
+    double2 b[RO::PER_T][RO::R];
+    typedef Stager<L, C, NT, STAGE> ST;
+    const ST st{smem_u32(&stage_bar), Q};
+    st.init();
+    auto run_of = [&](int it) { return it % nruns; };
+    auto tile_of = [&](int it) { return (long)(it / nruns) * L * C; };
+    st.issue(runs[run_of(first)].psi + tile_of(first));
+    for (int item = first; item < end; ++item) {
+        const RunDesc &d = runs[run_of(item)];
+        const int H = d.M / 2;
+        const long tile = tile_of(item);
+        const int km0 = (item / nruns) * C;
+        const float2 *next_psi = item + 1 < end ? runs[run_of(item + 1)].psi + tile_of(item + 1) : nullptr;
+        // barrier phase of this item's first wait: an item of the step modes waits four
+        // times (phases 0, 1, 0, 1), a COL_PREPARE item once (the iteration's parity)
+        const unsigned p0 = MODE == COL_PREPARE ? (unsigned)(item - first) & 1u : 0u;
+
+        // ---- phi ----
+        if (!st.wait(p0, fault)) return;
+        if (MODE == COL_PREPARE) {
+            fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, Pk, tw, b, Identity(), Prefetch<ST>{st, next_psi});
+        } else {
+            fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, Pk, tw, b, Identity(), Prefetch<ST>{st, d.inn + tile});
+            if (!st.wait(1u, fault)) return;
+            fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, s, tw, b, Identity(), Prefetch<ST>{st, d.con + tile});
+        }
+        const int nstep = (MODE != COL_PREPARE && d.noise_amp != 0.0f) ? *d.step_ctr : -1;
+        for (int e = threadIdx.x; e < L * C; e += NT) {
+            const int pi = spad(e);
+            double2 v = Pk[pi];
+            if (MODE != COL_PREPARE) {
+                // (psi^ - Mn dt k^2 N^ [+ dt b0 xi^ |k| lowpass]) / (1 + Mn dt k^2) / L as
+                // fn/L * psi^ - (an fn/L) * N^; the table is 0 at k = 0 and past M/2
+                const double4 f = d.kmix[tile + e];
+                const double2 nh = s[pi];
+                double rx = v.x * f.x - f.y * nh.x, ry = v.y * f.x - f.y * nh.y;
+                const int l = e / C, km = km0 + e % C;
+                if (nstep >= 0 && km <= H) {
+                    // MAINEQUATIONC2_NOI's noise term (MIS:1002-1003), lowpass at |k| = 2 pi
+                    const float2 xi = noise_mode(d.noise_key, nstep, l, km, L, d.M);
+                    const double kl = d.kdl[l], kmv = d.kdm[km];
+                    const double sk = sqrt(kl * kl + kmv * kmv);
+                    const double wn = d.noise_amp_d * sk * (0.5 - 0.5 * tanh((sk - 2.0 * 3.1415926) / 0.1)) * f.x;
+                    rx += wn * (double)xi.x;
+                    ry += wn * (double)xi.y;
+                }
+                v = make_double2(rx, ry);
+            } else {
+                const int l = e / C, km = km0 + e % C;
+                v = (l == 0 && km == 0) ? make_double2(0.0, 0.0) : cscale(v, 1.0 / (double)L);
+            }
+            Pk[pi] = v;
+        }
+        __syncthreads();
+        if (MODE != COL_PREPARE) {
+            fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b);
+            tile_out_d<L, C, NT>(s, d.psi + tile);
+        }
+        fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, ScaleByTableD{d.kc2d + tile, C, 0});
+        tile_out_d<L, C, NT>(s, d.ca + tile);
+        fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, ScaleByTableD{d.kc2d + tile, C, 1});
+        tile_out_d<L, C, NT>(s, d.cb + tile);
+        if (MODE == COL_PREPARE) continue;
+
+        // ---- con ----
+        if (!st.wait(0u, fault)) return;
+        fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, Pk, tw, b, Identity(), Prefetch<ST>{st, d.inc + tile});
+        if (!st.wait(1u, fault)) return;
+        fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, s, tw, b, Identity(), Prefetch<ST>{st, next_psi});
+        for (int e = threadIdx.x; e < L * C; e += NT) {
+            const int pi = spad(e);
+            // (c^ - Mc dt k^2 I^) / (1 + Mc dt alpha k^4) / L as fc/L * c^ - (ac fc/L) * I^
+            const double4 f = d.kmix[tile + e];
+            const double2 ih = s[pi];
+            const double2 v = Pk[pi];
+            Pk[pi] = make_double2(v.x * f.z - f.w * ih.x, v.y * f.z - f.w * ih.y);
+        }
+        __syncthreads();
+        fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b);
+        tile_out_d<L, C, NT>(s, d.con + tile);
+        if (MODE == COL_STEP_CHECKPOINT) {
+            fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, GradientOfD{d.kdl, d.kdm, km0, H, 0});
+            tile_out_d<L, C, NT>(s, d.gx + tile);
+            fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, GradientOfD{d.kdl, d.kdm, km0, H, 1});
+            tile_out_d<L, C, NT>(s, d.gy + tile);
+        }
+    }
+    st.finish();  // every copy issued has been waited for: the last item issues none
+}
+
+template <int L, int C, int MODE, int STAGE>
+static cudaError_t mcol_impl(const RunDesc *d_runs, int nruns, int M, const TwiddleSet &tw, cudaStream_t st) {
+    constexpr int NT = MColCfg<L, C>::NT;
+    constexpr size_t smem = MColCfg<L, C>::SMEM;
+    static unsigned mask = 0;
+    cudaError_t e = set_smem(k_mcol_step<L, C, MODE, STAGE>, smem, mask);
+    if (nruns == 0 || e != cudaSuccess) return e;
+    const int H = M / 2;
+    const int items = ((H + 1 + C - 1) / C) * nruns;
+    const int cap = MColCfg<L, C>::MINB * sm_count();
+    const int g0 = items < cap ? items : cap;
+    const int per = (items + g0 - 1) / g0;
+    const int grid = (items + per - 1) / per;
+    k_mcol_step<L, C, MODE, STAGE><<<grid, NT, smem, st>>>(d_runs, nruns, per, tw.f64[log2i(L)], tw.fault);
+    return cudaGetLastError();
+}
+
+template <int L, int C, int STAGE>
+static cudaError_t mcol_modes(const RunDesc *d_runs, int nruns, int M, int mode, const TwiddleSet &tw,
+                              cudaStream_t s) {
+    switch (mode) {
+        case COL_STEP: return mcol_impl<L, C, COL_STEP, STAGE>(d_runs, nruns, M, tw, s);
+        case COL_PREPARE: return mcol_impl<L, C, COL_PREPARE, STAGE>(d_runs, nruns, M, tw, s);
+        case COL_STEP_CHECKPOINT: return mcol_impl<L, C, COL_STEP_CHECKPOINT, STAGE>(d_runs, nruns, M, tw, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+template <int L, int C>
+static cudaError_t mcol_stages(const RunDesc *d_runs, int nruns, int M, int stage, int mode, const TwiddleSet &tw,
+                               cudaStream_t s) {
+    switch (stage) {
+        case STAGE_ASYNC: return mcol_modes<L, C, STAGE_ASYNC>(d_runs, nruns, M, mode, tw, s);
+        case STAGE_BULK: return mcol_modes<L, C, STAGE_BULK>(d_runs, nruns, M, mode, tw, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+template <int L>
+static cudaError_t mcol_dispatch(const RunDesc *d_runs, int nruns, int M, int C, int stage, int mode,
+                                 const TwiddleSet &tw, cudaStream_t s) {
+    switch (C) {
+        case 1:
+            if constexpr (mcol_tile_ok(L, 1)) return mcol_stages<L, 1>(d_runs, nruns, M, stage, mode, tw, s);
+            break;
+        case 2:
+            if constexpr (mcol_tile_ok(L, 2)) return mcol_stages<L, 2>(d_runs, nruns, M, stage, mode, tw, s);
+            break;
+        case 4:
+            if constexpr (mcol_tile_ok(L, 4)) return mcol_stages<L, 4>(d_runs, nruns, M, stage, mode, tw, s);
+            break;
+        case 8:
+            if constexpr (mcol_tile_ok(L, 8)) return mcol_stages<L, 8>(d_runs, nruns, M, stage, mode, tw, s);
+            break;
+        case 16:
+            if constexpr (mcol_tile_ok(L, 16)) return mcol_stages<L, 16>(d_runs, nruns, M, stage, mode, tw, s);
+            break;
+        default: break;
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <int L>
+cudaError_t launch_col_mixed_L(const RunDesc *d_runs, int nruns, int M, int C, int stage, int mode,
+                               const TwiddleSet &tw, cudaStream_t s) {
+    return mcol_dispatch<L>(d_runs, nruns, M, C, stage, mode, tw, s);
+}
+
+}  // namespace pfc

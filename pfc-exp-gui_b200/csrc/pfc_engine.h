@@ -23,7 +23,8 @@ struct Context {
     std::mutex stage_mu;
     float *stage = nullptr;
     size_t stage_floats = 0;
-    // host view of tw.fault (mapped pinned memory); sticky once a kernel sets it
+    // host view of tw.fault (mapped pinned memory): set by a kernel whose bounded wait
+    // gave up, cleared by fault_status when it reports the error
     volatile int *fault = nullptr;
 };
 
@@ -37,7 +38,7 @@ int cuda_error(cudaError_t e, const char *what);
         if (_e != cudaSuccess) return pfc::cuda_error(_e, #expr);   \
     } while (0)
 // PFC_OK, or PFC_E_CUDA when a kernel of the context has set its fault word (read
-// after the context's work has been synchronised)
+// after the context's work has been synchronised; the word is then cleared)
 int fault_status(const Context *c);
 // synchronise a stream, then report a CUDA error or the context's fault word
 #define PFC_SYNC_CHECKED(ctx, stream)                                          \
@@ -51,6 +52,8 @@ void model_coefs(int model, ModelCoefs *k);
 void kref_table(int n, float dx, std::vector<float> &k);
 float c2_kc(float sig, float g1, float g2, float k1, float k2, float s1, float s2);
 bool is_supported_len(int n);
+// PFC_PRECISION_FP32 or PFC_PRECISION_MIXED: the fused two-sweep kernels
+bool fused_path(int prec);
 }  // namespace pfc
 
 struct pfc_run {
@@ -75,6 +78,8 @@ struct pfc_run {
     bool fields_valid = false;
     bool energy_valid = false;
     pfc::Fp64State *f64 = nullptr;
+    bool kcoef_held = false;        // holds a reference on the shared coefficient table
+    std::vector<double> kd_host;    // mixed path: the double k-vectors (lengths L and M)
 };
 
 namespace pfc {
@@ -87,6 +92,6 @@ int fp64_materialize(pfc_run *r);
 int fp64_get_fields(pfc_run *r, double *phi, double *con);
 int fp64_set_fields(pfc_run *r, const double *phi, const double *con);
 int fp64_energy(pfc_run *r, double *e_over_p, double *mass_over_p);
-// Kernel attribute setup for one grid size (must precede graph capture).
-cudaError_t prepare_size(int L, int M, int C, int stage);
+// Kernel attribute setup for one grid size and precision (must precede graph capture).
+cudaError_t prepare_size(int L, int M, int C, int stage, int prec);
 }  // namespace pfc

@@ -54,6 +54,14 @@ struct RunDesc {
     float dt;
     ModelCoefs k;
     C2Params c2a, c2b;
+    // mixed-precision runs (FP32 storage, FP64 arithmetic) only, pure-FP64 operator:
+    //   kmix = (fn/L, an*fn/L, fc/L, ac*fc/L) with an = Mn dt k^2, ac = Mc dt k^2,
+    //          fn = 1/(1 + an), fc = 1/(1 + Mc dt alpha k^4); kc2d = (C2A(k), C2B(k));
+    //   kdl, kdm: the k-vectors in double (lengths L and M)
+    const double4 *kmix;
+    const double2 *kc2d;
+    const double *kdl, *kdm;
+    double noise_amp_d;  // dt * b0 in double (0 = off)
     // per-CTA partial sums written by the analysis row kernel: [2 * L] doubles
     double *partials;
     // batched runs only: slots of (energy sum, mass sum) that launch_reduce_runs fills
@@ -76,15 +84,42 @@ struct TwiddleSet {
     int *fault;
 };
 
-// FP32 fused step (step_fp32.cu).  All runs of one call share (L, M).
-cudaError_t launch_row_step(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw, cudaStream_t s);
+// Fused step (two sweeps per step).  All runs of one call share (L, M) and the
+// precision prec: PFC_PRECISION_FP32 (step_fp32.cu, FP32 arithmetic) or
+// PFC_PRECISION_MIXED (step_mixed.cu, FP64 arithmetic on the same FP32 arrays).
+cudaError_t launch_row_step(const RunDesc *d_runs, int nruns, int L, int M, int prec, const TwiddleSet &tw,
+                            cudaStream_t s);
 // C: column tile width of the runs' layout (RunDesc::CT, the same for all nruns runs);
 // stage: how input tiles are staged (COL_STAGE_*; the results do not depend on it)
-cudaError_t launch_col_step(const RunDesc *d_runs, int nruns, int L, int M, int C, int stage, int mode,
+cudaError_t launch_col_step(const RunDesc *d_runs, int nruns, int L, int M, int C, int stage, int mode, int prec,
                             const TwiddleSet &tw, cudaStream_t s);
-cudaError_t launch_row_forward(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw, cudaStream_t s);
-cudaError_t launch_row_analysis(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw,
+cudaError_t launch_row_forward(const RunDesc *d_runs, int nruns, int L, int M, int prec, const TwiddleSet &tw,
+                               cudaStream_t s);
+cudaError_t launch_row_analysis(const RunDesc *d_runs, int nruns, int L, int M, int prec, const TwiddleSet &tw,
                                 cudaStream_t s);
+// The column kernels of one row length L (instantiated per L in col_inst.cu).
+template <int L>
+cudaError_t launch_col_f32_L(const RunDesc *d_runs, int nruns, int M, int C, int stage, int mode,
+                             const TwiddleSet &tw, cudaStream_t s);
+template <int L>
+cudaError_t launch_col_mixed_L(const RunDesc *d_runs, int nruns, int M, int C, int stage, int mode,
+                               const TwiddleSet &tw, cudaStream_t s);
+// The FP32 and mixed-precision kernels behind them.
+cudaError_t launch_row_step_f32(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw, cudaStream_t s);
+cudaError_t launch_col_step_f32(const RunDesc *d_runs, int nruns, int L, int M, int C, int stage, int mode,
+                                const TwiddleSet &tw, cudaStream_t s);
+cudaError_t launch_row_forward_f32(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw,
+                                   cudaStream_t s);
+cudaError_t launch_row_analysis_f32(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw,
+                                    cudaStream_t s);
+cudaError_t launch_row_step_mixed(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw,
+                                  cudaStream_t s);
+cudaError_t launch_col_step_mixed(const RunDesc *d_runs, int nruns, int L, int M, int C, int stage, int mode,
+                                  const TwiddleSet &tw, cudaStream_t s);
+cudaError_t launch_row_forward_mixed(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw,
+                                     cudaStream_t s);
+cudaError_t launch_row_analysis_mixed(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw,
+                                      cudaStream_t s);
 
 // For each of nruns runs: (sum, in CTA order, of the analysis row kernel's nparts
 // partial pairs) -> runs[i].ehist[2*slot], [2*slot+1]; the same additions in the same
@@ -93,6 +128,14 @@ cudaError_t launch_reduce_runs(const RunDesc *d_runs, int nruns, int nparts, int
 
 // Build the per k-point coefficient table of one run (layout and values as RunDesc::kcoef).
 cudaError_t launch_build_kcoef(const RunDesc *d_run, float2 *kden, float2 *kc2, cudaStream_t s);
+// Pure-FP64 correlation kernel C2(|k|) (misfit_uniform_time_seed_fftw_early.cpp:700-750 with
+// every intermediate in double): e1 * exp(-(|k| - k1)^2 / gg1) for |k| <= kc, else with 2.
+struct C2ParamsD {
+    double kc, e1, e2, k1, k2, gg1, gg2;
+};
+// The mixed-precision table of one run (RunDesc::kmix, kc2d), from its double k-vectors.
+cudaError_t launch_build_kmix(const RunDesc *d_run, double mn_dt, double mc_dt, double alpha, C2ParamsD a,
+                              C2ParamsD b, double4 *kmix, double2 *kc2d, cudaStream_t s);
 
 // column-kernel modes
 enum ColMode : int { COL_STEP = 0, COL_PREPARE = 1, COL_STEP_CHECKPOINT = 2 };
@@ -107,13 +150,21 @@ cudaError_t launch_stage_selftest(const float2 *src, float2 *dst, int n, int iss
                                   int *fault, cudaStream_t s);
 
 // Kernel attribute setup (before graph capture) of the row kernels of row length M.
-cudaError_t prepare_rows(int M);
+cudaError_t prepare_rows(int M, int prec);
+cudaError_t prepare_rows_f32(int M);
+cudaError_t prepare_rows_mixed(int M);
 
-// Number of partial-sum slots the analysis kernel writes per run (2 doubles each).
-int analysis_partials(int L, int M);
+// Number of partial-sum slots the analysis kernel of precision prec writes per run (2
+// doubles each).
+int analysis_partials(int L, int M, int prec);
+int analysis_partials_f32(int L, int M);
+int analysis_partials_mixed(int L, int M);
 // Default column-tile width of the row-space layout for a grid with L rows, and the
 // widths the autotuner may choose from (out[] holds up to 4; returns their number).
 int col_tile_width(int L);
 int col_tile_candidates(int L, int *out);
+// The same for the mixed-precision column kernel (double2 tiles, half as long).
+int mixed_col_tile_width(int L);
+int mixed_col_tile_candidates(int L, int *out);
 
 }  // namespace pfc

@@ -92,7 +92,7 @@ int steps_to_event(const Job &j) {
 }
 
 struct Cohort {
-    int model = 0, L = 0, M = 0, CT = 0, stage = 0;  // runs of one model, grid, column tile width and staging
+    int model = 0, L = 0, M = 0, CT = 0, stage = 0, prec = 0;  // runs of one model, grid, tile width, staging, precision
     std::vector<Job *> jobs;
     RunDesc *d_descs = nullptr;
     double *d_ehist = nullptr;  // [n][SEG][2] (CVD)
@@ -212,7 +212,7 @@ int build_cohorts(pfc_engine *e) {
         Cohort *c = nullptr;
         for (auto &x : e->cohorts)
             if (x.model == j->spec.kind && x.L == j->L && x.M == j->M && x.CT == j->run->desc.CT &&
-                x.stage == j->run->desc.stage)
+                x.stage == j->run->desc.stage && x.prec == j->run->p.precision)
                 c = &x;
         if (!c) {
             e->cohorts.push_back(Cohort{});
@@ -222,6 +222,7 @@ int build_cohorts(pfc_engine *e) {
             c->M = j->M;
             c->CT = j->run->desc.CT;
             c->stage = j->run->desc.stage;
+            c->prec = j->run->p.precision;
         }
         c->jobs.push_back(j);
     }
@@ -240,7 +241,7 @@ int build_cohorts(pfc_engine *e) {
             h[i].ehist = c.d_ehist ? c.d_ehist + (size_t)i * SEG * 2 : nullptr;
         }
         PFC_CUDA_TRY(cudaMemcpyAsync(c.d_descs, h.data(), n * sizeof(RunDesc), cudaMemcpyHostToDevice, e->main));
-        PFC_CUDA_TRY(prepare_size(c.L, c.M, c.CT, c.stage));
+        PFC_CUDA_TRY(prepare_size(c.L, c.M, c.CT, c.stage, c.prec));
         cudaEvent_t ev;
         PFC_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         e->join_events.push_back(ev);
@@ -265,13 +266,13 @@ int build_cohorts(pfc_engine *e) {
 int cohort_step(pfc_engine *e, Cohort &c, int slot, cudaStream_t st) {
     const int n = (int)c.jobs.size();
     const TwiddleSet &tw = e->ctx->tw;
-    PFC_CUDA_TRY(launch_row_step(c.d_descs, n, c.L, c.M, tw, st));
+    PFC_CUDA_TRY(launch_row_step(c.d_descs, n, c.L, c.M, c.prec, tw, st));
     if (c.model == PFC_JOB_MISFIT) {
-        PFC_CUDA_TRY(launch_col_step(c.d_descs, n, c.L, c.M, c.CT, c.stage, COL_STEP, tw, st));
+        PFC_CUDA_TRY(launch_col_step(c.d_descs, n, c.L, c.M, c.CT, c.stage, COL_STEP, c.prec, tw, st));
     } else {
-        PFC_CUDA_TRY(launch_col_step(c.d_descs, n, c.L, c.M, c.CT, c.stage, COL_STEP_CHECKPOINT, tw, st));
-        PFC_CUDA_TRY(launch_row_analysis(c.d_descs, n, c.L, c.M, tw, st));
-        PFC_CUDA_TRY(launch_reduce_runs(c.d_descs, n, analysis_partials(c.L, c.M), slot, st));
+        PFC_CUDA_TRY(launch_col_step(c.d_descs, n, c.L, c.M, c.CT, c.stage, COL_STEP_CHECKPOINT, c.prec, tw, st));
+        PFC_CUDA_TRY(launch_row_analysis(c.d_descs, n, c.L, c.M, c.prec, tw, st));
+        PFC_CUDA_TRY(launch_reduce_runs(c.d_descs, n, analysis_partials(c.L, c.M, c.prec), slot, st));
     }
     return PFC_OK;
 }
@@ -371,7 +372,7 @@ void timestamp_line(const std::string &outdir, int step) {
 // sequence of the CLI's pfc_run_advance(..., 1) + Phimax + checkpoint files).
 int misfit_checkpoint(pfc_engine *e, Job *j) {
     pfc_run *r = j->run;
-    PFC_CUDA_TRY(launch_row_analysis(r->d_desc, 1, r->L, r->M, e->ctx->tw, e->main));
+    PFC_CUDA_TRY(launch_row_analysis(r->d_desc, 1, r->L, r->M, r->p.precision, e->ctx->tw, e->main));
     PFC_CUDA_TRY(launch_reduce_fixed(r->desc.partials, r->nparts, 2, 2, r->d_scratch, e->main));
     r->fields_valid = true;
     r->energy_valid = true;
@@ -614,11 +615,11 @@ int quantum(pfc_engine *e) {
                 if (rc != PFC_OK) return rc;
                 continue;
             }
-            PFC_CUDA_TRY(launch_row_step(c.d_descs, (int)c.jobs.size(), c.L, c.M, tw, e->main));
+            PFC_CUDA_TRY(launch_row_step(c.d_descs, (int)c.jobs.size(), c.L, c.M, c.prec, tw, e->main));
             for (Job *j : c.jobs) {
                 const bool ck = std::find(ckpt.begin(), ckpt.end(), j) != ckpt.end();
                 PFC_CUDA_TRY(launch_col_step(j->run->d_desc, 1, c.L, c.M, c.CT, c.stage,
-                                             ck ? COL_STEP_CHECKPOINT : COL_STEP, tw, e->main));
+                                             ck ? COL_STEP_CHECKPOINT : COL_STEP, c.prec, tw, e->main));
             }
         }
         const int rc = copy_energy_slots(e, (int)seg_len.size());
@@ -832,7 +833,8 @@ static int make_job(pfc_engine *e, const pfc_job *job, std::unique_ptr<Job> &out
     if (job->kind == PFC_JOB_MISFIT || job->kind == PFC_JOB_CVD) {
         pfc_run_params p = job->params;
         p.model = job->kind;
-        if (p.precision != PFC_PRECISION_FP32) return set_error(PFC_E_INVALID, "engine runs use the FP32 path");
+        if (!fused_path(p.precision))
+            return set_error(PFC_E_INVALID, "engine runs use the fused paths (mixed or FP32 precision)");
         if (p.N != 1) return set_error(PFC_E_INVALID, "engine runs are 2-D (N = 1)");
         if (job->steps <= 0 || job->mod <= 0) return set_error(PFC_E_INVALID, "steps and mod must be > 0");
         double b = 0.0;

@@ -10,10 +10,11 @@
 namespace pfc {
 
 constexpr int COL_TILE = 4096;  // complex elements per column-kernel tile (32 KB in FP32)
+constexpr int COL_TILE_MAX = 16;  // widest column tile (packed columns); the row walks' bound
 
-// Column-kernel tile: L rows x C packed columns, C a power of two in [1, 16] with
-// 512 <= C*L <= 8192 complex elements (three such buffers per CTA: 13 KB to 204 KB).
-constexpr bool col_tile_ok(int L, int C) { return C >= 1 && C <= 16 && C * L >= 512 && C * L <= 8192; }
+// Column-kernel tile: L rows x C packed columns, C a power of two in [1, COL_TILE_MAX]
+// with 512 <= C*L <= 8192 complex elements (three such buffers per CTA: 13 KB to 204 KB).
+constexpr bool col_tile_ok(int L, int C) { return C >= 1 && C <= COL_TILE_MAX && C * L >= 512 && C * L <= 8192; }
 template <int L, int C> struct ColCfg {
     static constexpr int NT = (C * L / 16) < 32 ? 32 : (C * L / 16);
     // CTAs per SM that the shared memory leaves room for (two at C*L = 4096)
@@ -30,6 +31,70 @@ __device__ __forceinline__ float c2_ref(const C2Params &p, float ks) {
     }
     const double d = (double)__fsub_rn(s, p.k2);
     return (float)(exp(-(double)p.q2 * (double)p.q2) * exp(-(d * d) / (double)p.gg2));
+}
+
+// Row-space element (l, km) of a run: column-tile-major, ((km/CT)*L + l)*CT + km%CT.
+__device__ __forceinline__ long rs_index(const RunDesc &d, int l, int km) {
+    return ((long)(km >> d.lct) * d.L + l) * d.CT + (km & (d.CT - 1));
+}
+
+// Loop over the row-space elements (l0 + r, km), r < RPC, km <= M/2, in an order
+// that walks each column tile's contiguous RPC*CT block: w -> (tile t, row r, col c).
+// RPC and CT are powers of two, so the block split is a shift and a mask.
+template <int n> struct ilog2 {
+    static constexpr int value = n <= 1 ? 0 : 1 + ilog2<n / 2>::value;
+};
+template <> struct ilog2<1> {
+    static constexpr int value = 0;
+};
+#define ROW_TILE_LOOP(RPC, H, NT, ...)                                     \
+    {                                                                       \
+        const int _ct = d.CT, _lct = d.lct;                                 \
+        const int _lblk = ilog2<(RPC)>::value + _lct;                       \
+        const int _total = d.T << _lblk;                                    \
+        for (int w = threadIdx.x; w < _total; w += (NT)) {                  \
+            const int t = w >> _lblk, rem = w & ((1 << _lblk) - 1);         \
+            const int r = rem >> _lct, k = (t << _lct) + (rem & (_ct - 1)); \
+            if (k > (H)) continue;                                          \
+            const int l = l0 + r;                                           \
+            (void)l;                                                        \
+            __VA_ARGS__                                                     \
+        }                                                                   \
+    }
+
+// Spectrum of the noise field at mode (l, km) of step t.  The reference draws real-space
+// white noise with a sequential polar Box-Muller generator (Gauss, MIS:951-981) and
+// transforms it (p5); the transform of white noise is itself white, so the modes are
+// drawn here directly, with the distribution the reference's masks leave
+// (MIS:1002-1003): re and im independent N(0, P/4), except at the four self-conjugate
+// modes (l in {0, L/2}, km in {0, M/2}) where re ~ N(0, P) and im = 0; along the
+// self-conjugate columns km = 0 and M/2, mode L - l is the conjugate of mode l.
+// Stream: the two normals of canonical mode c = (t*L + l)*(M/2 + 1) + km come from
+// Box-Muller of the splitmix64 outputs at positions 2c and 2c + 1 of the run's key.
+static __device__ __forceinline__ unsigned long long sm64_out(unsigned long long z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+static __device__ float2 noise_mode(unsigned long long key, int t, int l, int km, int L, int M) {
+    const int H = M / 2;
+    bool conj = false;
+    if ((km == 0 || km == H) && l > L / 2) {
+        l = L - l;
+        conj = true;
+    }
+    const unsigned long long c = ((unsigned long long)t * L + l) * (unsigned long long)(H + 1) + km;
+    const unsigned long long g = 0x9E3779B97F4A7C15ULL;
+    const unsigned long long w1 = sm64_out(key + (2 * c + 1) * g), w2 = sm64_out(key + (2 * c + 2) * g);
+    const float u1 = ((float)(w1 >> 40) + 0.5f) * (1.0f / 16777216.0f);  // (0, 1)
+    const float u2 = (float)(w2 >> 40) * (1.0f / 16777216.0f);           // [0, 1)
+    const float rad = sqrtf(-2.0f * logf(u1));
+    float sn, cs;
+    sincospif(2.0f * u2, &sn, &cs);
+    const float P = (float)L * (float)M;
+    if ((l == 0 || l == L / 2) && (km == 0 || km == H)) return make_float2(sqrtf(P) * rad * cs, 0.0f);
+    const float s = 0.5f * sqrtf(P);
+    return make_float2(s * rad * cs, conj ? -s * rad * sn : s * rad * sn);
 }
 
 static inline int log2i(int n) {

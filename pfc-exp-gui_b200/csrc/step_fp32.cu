@@ -48,10 +48,6 @@ int col_tile_candidates(int L, int *out) {
     return n;
 }
 
-__device__ __forceinline__ long rs_index(const RunDesc &d, int l, int km) {
-    return ((long)(km >> d.lct) * d.L + l) * d.CT + (km & (d.CT - 1));
-}
-
 // Per k-point coefficients of one run (RunDesc::kcoef), built once in FP64 and rounded.
 // ks and the k^4 product use the reference's float operation order (ks, MAINEQUATIONC2_NOI,
 // MIS:1002-1010); the intrinsics keep them from being contracted into FMAs.
@@ -153,36 +149,13 @@ template <int NW> __device__ __forceinline__ unsigned block_max_get(const unsign
 }
 __device__ __forceinline__ float absmax2(float2 v) { return fmaxf(fabsf(v.x), fabsf(v.y)); }
 
-// Loop over the row-space elements (l0 + r, km), r < RPC, km <= M/2, in an order
-// that walks each column tile's contiguous RPC*CT block: w -> (tile t, row r, col c).
-// RPC and CT are powers of two, so the block split is a shift and a mask.
-template <int n> struct ilog2 {
-    static constexpr int value = n <= 1 ? 0 : 1 + ilog2<n / 2>::value;
-};
-template <> struct ilog2<1> {
-    static constexpr int value = 0;
-};
-#define ROW_TILE_LOOP(RPC, H, NT, ...)                                     \
-    {                                                                       \
-        const int _ct = d.CT, _lct = d.lct;                                 \
-        const int _lblk = ilog2<(RPC)>::value + _lct;                       \
-        const int _total = d.T << _lblk;                                    \
-        for (int w = threadIdx.x; w < _total; w += (NT)) {                  \
-            const int t = w >> _lblk, rem = w & ((1 << _lblk) - 1);         \
-            const int r = rem >> _lct, k = (t << _lct) + (rem & (_ct - 1)); \
-            if (k > (H)) continue;                                          \
-            const int l = l0 + r;                                           \
-            (void)l;                                                        \
-            __VA_ARGS__                                                     \
-        }                                                                   \
-    }
-
-// The same walk unrolled over a fixed bound IT of iterations per thread; the body sees
-// the iteration index `it`, so values can stay in registers from one walk to the next.
-// A run's Hp = round_up(M/2 + 1, CT) with CT <= 16, so T * CT * RPC <= (M/2 + 16) * RPC
-// and IT = ceil((M/2 + 16) * RPC / NT) covers every element.
+// The row-space walk (ROW_TILE_LOOP, step_common.cuh) unrolled over a fixed bound IT of
+// iterations per thread; the body sees the iteration index `it`, so values can stay in
+// registers from one walk to the next.  A run's Hp = round_up(M/2 + 1, CT) with
+// CT <= COL_TILE_MAX, so T * CT * RPC <= (M/2 + COL_TILE_MAX) * RPC and
+// IT = ceil((M/2 + COL_TILE_MAX) * RPC / NT) covers every element.
 template <int M, int RPC, int NT> struct RowWalk {
-    static constexpr int IT = ((M / 2 + 16) * RPC + NT - 1) / NT;
+    static constexpr int IT = ((M / 2 + COL_TILE_MAX) * RPC + NT - 1) / NT;
 };
 #define ROW_TILE_LOOP_REG(RPC, H, NT, IT, ...)                             \
     {                                                                       \
@@ -336,10 +309,7 @@ __global__ void __launch_bounds__(RowCfg<M>::NT) k_row_forward(const RunDesc *__
     })
 }
 
-// ---------------------------------------------------------------------------
-// Column kernel.
-// ---------------------------------------------------------------------------
-#include "col_kernel.cuh"
+// The column kernel (col_kernel.cuh) is instantiated per row length L in col_inst.cu.
 
 // ---------------------------------------------------------------------------
 // Analysis row kernel (checkpoints): real fields, energy density and mass.
@@ -480,82 +450,23 @@ static cudaError_t row_analysis_impl(const RunDesc *d_runs, int nruns, int L, co
     return cudaGetLastError();
 }
 
-template <int L, int C, int MODE, int STAGE>
-static cudaError_t col_impl(const RunDesc *d_runs, int nruns, int M, const TwiddleSet &tw, cudaStream_t st) {
-    constexpr int NT = ColCfg<L, C>::NT;
-    constexpr size_t smem = 2 * smem_bytes<C * L>() + sizeof(float2) * C * L;  // s, P (padded) and Q
-    static unsigned mask = 0;
-    cudaError_t e = set_smem(k_col_step<L, C, MODE, STAGE>, smem, mask);
-    if (nruns == 0) return e;
-    if (e != cudaSuccess) return e;
-    const int H = M / 2;
-    const int items = ((H + 1 + C - 1) / C) * nruns;
-    const int cap = ColCfg<L, C>::MINB * sm_count();
-    const int grid = items < cap ? items : cap;
-    k_col_step<L, C, MODE, STAGE><<<grid, NT, smem, st>>>(d_runs, nruns, tw.f32[log2i(L)], tw.fault);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_row_step(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw, cudaStream_t s) {
+cudaError_t launch_row_step_f32(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw, cudaStream_t s) {
     PFC_SIZE_SWITCH(M, row_step_impl, d_runs, nruns, L, tw, s)
 }
 
-cudaError_t launch_row_forward(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw, cudaStream_t s) {
+cudaError_t launch_row_forward_f32(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw,
+                                   cudaStream_t s) {
     PFC_SIZE_SWITCH(M, row_forward_impl, d_runs, nruns, L, tw, s)
 }
 
-cudaError_t launch_row_analysis(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw,
-                                cudaStream_t s) {
+cudaError_t launch_row_analysis_f32(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw,
+                                    cudaStream_t s) {
     PFC_SIZE_SWITCH(M, row_analysis_impl, d_runs, nruns, L, tw, s)
 }
 
-template <int L, int C, int STAGE>
-static cudaError_t col_modes(const RunDesc *d_runs, int nruns, int M, int mode, const TwiddleSet &tw,
-                             cudaStream_t s) {
-    switch (mode) {
-        case COL_STEP: return col_impl<L, C, COL_STEP, STAGE>(d_runs, nruns, M, tw, s);
-        case COL_PREPARE: return col_impl<L, C, COL_PREPARE, STAGE>(d_runs, nruns, M, tw, s);
-        case COL_STEP_CHECKPOINT: return col_impl<L, C, COL_STEP_CHECKPOINT, STAGE>(d_runs, nruns, M, tw, s);
-        default: return cudaErrorInvalidValue;
-    }
-}
-template <int L, int C>
-static cudaError_t col_stages(const RunDesc *d_runs, int nruns, int M, int stage, int mode, const TwiddleSet &tw,
-                              cudaStream_t s) {
-    switch (stage) {
-        case STAGE_ASYNC: return col_modes<L, C, STAGE_ASYNC>(d_runs, nruns, M, mode, tw, s);
-        case STAGE_BULK: return col_modes<L, C, STAGE_BULK>(d_runs, nruns, M, mode, tw, s);
-        default: return cudaErrorInvalidValue;
-    }
-}
-
-template <int L>
-static cudaError_t col_dispatch(const RunDesc *d_runs, int nruns, int M, int C, int stage, int mode,
+cudaError_t launch_col_step_f32(const RunDesc *d_runs, int nruns, int L, int M, int C, int stage, int mode,
                                 const TwiddleSet &tw, cudaStream_t s) {
-    switch (C) {
-        case 1:
-            if constexpr (col_tile_ok(L, 1)) return col_stages<L, 1>(d_runs, nruns, M, stage, mode, tw, s);
-            break;
-        case 2:
-            if constexpr (col_tile_ok(L, 2)) return col_stages<L, 2>(d_runs, nruns, M, stage, mode, tw, s);
-            break;
-        case 4:
-            if constexpr (col_tile_ok(L, 4)) return col_stages<L, 4>(d_runs, nruns, M, stage, mode, tw, s);
-            break;
-        case 8:
-            if constexpr (col_tile_ok(L, 8)) return col_stages<L, 8>(d_runs, nruns, M, stage, mode, tw, s);
-            break;
-        case 16:
-            if constexpr (col_tile_ok(L, 16)) return col_stages<L, 16>(d_runs, nruns, M, stage, mode, tw, s);
-            break;
-        default: break;
-    }
-    return cudaErrorInvalidValue;
-}
-
-cudaError_t launch_col_step(const RunDesc *d_runs, int nruns, int L, int M, int C, int stage, int mode,
-                            const TwiddleSet &tw, cudaStream_t s) {
-    PFC_SIZE_SWITCH(L, col_dispatch, d_runs, nruns, M, C, stage, mode, tw, s)
+    PFC_SIZE_SWITCH(L, launch_col_f32_L, d_runs, nruns, M, C, stage, mode, tw, s)
 }
 
 // Self-test of the column kernel's tile staging (one CTA of 128 threads): with issue,
@@ -583,25 +494,16 @@ cudaError_t launch_stage_selftest(const float2 *src, float2 *dst, int n, int iss
     return cudaGetLastError();
 }
 
-cudaError_t prepare_rows(int M) {
+cudaError_t prepare_rows_f32(int M) {
     // nruns == 0: only the shared-memory attributes are set, nothing is launched
     TwiddleSet none{};
     cudaError_t e;
-    if ((e = launch_row_step(nullptr, 0, 0, M, none, 0)) != cudaSuccess) return e;
-    if ((e = launch_row_forward(nullptr, 0, 0, M, none, 0)) != cudaSuccess) return e;
-    return launch_row_analysis(nullptr, 0, 0, M, none, 0);
+    if ((e = launch_row_step_f32(nullptr, 0, 0, M, none, 0)) != cudaSuccess) return e;
+    if ((e = launch_row_forward_f32(nullptr, 0, 0, M, none, 0)) != cudaSuccess) return e;
+    return launch_row_analysis_f32(nullptr, 0, 0, M, none, 0);
 }
 
-cudaError_t prepare_size(int L, int M, int C, int stage) {
-    TwiddleSet none{};
-    cudaError_t e;
-    if ((e = prepare_rows(M)) != cudaSuccess) return e;
-    for (int mode = 0; mode < 3; ++mode)
-        if ((e = launch_col_step(nullptr, 0, L, M, C, stage, mode, none, 0)) != cudaSuccess) return e;
-    return cudaSuccess;
-}
-
-int analysis_partials(int L, int M) {
+int analysis_partials_f32(int L, int M) {
     int rpc = (ROW_TILE / 2) / M;
     if (rpc < 1) rpc = 1;
     return (L + rpc - 1) / rpc;

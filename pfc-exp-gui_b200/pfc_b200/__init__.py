@@ -24,6 +24,7 @@ MODEL_CVD = 1
 FP32 = 0
 FP64 = 1
 FP64_PURE = 2
+MIXED = 3  # FP32 arrays in HBM, FP64 arithmetic (the default precision)
 
 PFC_OK = 0
 PFC_E_INVALID, PFC_E_CUDA, PFC_E_NOMEM, PFC_E_IO, PFC_E_STATE = -1, -2, -3, -4, -5
@@ -156,10 +157,10 @@ def lib():
         "pfc_job_fields": ([vp, C.c_uint64, fp, fp], C.c_int),
         "pfc_release": ([vp, C.c_uint64], C.c_int),
         "pfc_run_bytes": ([P(RunParams), dp], C.c_int),
-        "pfc_tile_width": ([C.c_int, C.c_int, C.c_int, P(C.c_int), P(C.c_int), fp, P(C.c_int)], C.c_int),
-        "pfc_set_tile_width": ([C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
-        "pfc_col_staging": ([C.c_int, C.c_int, C.c_int, P(C.c_int), fp, fp, P(C.c_int)], C.c_int),
-        "pfc_set_col_staging": ([C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
+        "pfc_tile_width": ([C.c_int, C.c_int, C.c_int, C.c_int, P(C.c_int), P(C.c_int), fp, P(C.c_int)], C.c_int),
+        "pfc_set_tile_width": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
+        "pfc_col_staging": ([C.c_int, C.c_int, C.c_int, C.c_int, P(C.c_int), fp, fp, P(C.c_int)], C.c_int),
+        "pfc_set_col_staging": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
         "pfc_selftest_tile_stage": ([C.c_int, C.c_int, C.c_int, C.c_double, P(C.c_int), P(C.c_int), dp], C.c_int),
     }
     for name, (args, res) in sig.items():
@@ -360,39 +361,41 @@ class Engine:
             pass
 
 
-def tile_width(L: int, M: int, device: int = 0):
-    """Column tile width FP32 runs of an L x M grid use (tuned on the device on first
-    use) and the autotuner's trials: (width, {candidate: ms per 8 steps})."""
+def tile_width(L: int, M: int, device: int = 0, precision: int = MIXED):
+    """Column tile width fused-path runs (MIXED or FP32) of an L x M grid use (tuned on
+    the device on first use) and the autotuner's trials: (width, {candidate: ms per 8
+    steps})."""
     w, n = C.c_int(), C.c_int()
     cand = (C.c_int * 4)()
     ms = (C.c_float * 4)()
-    _check(lib().pfc_tile_width(device, L, M, C.byref(w), cand, ms, C.byref(n)), "pfc_tile_width")
+    _check(lib().pfc_tile_width(device, L, M, precision, C.byref(w), cand, ms, C.byref(n)), "pfc_tile_width")
     return w.value, {cand[i]: ms[i] for i in range(n.value)}
 
 
-def set_tile_width(L: int, M: int, width: int, device: int = 0):
-    """Fix the column tile width of an L x M grid for the rest of the process."""
-    _check(lib().pfc_set_tile_width(device, L, M, width), "pfc_set_tile_width")
+def set_tile_width(L: int, M: int, width: int, device: int = 0, precision: int = MIXED):
+    """Fix the column tile width of an L x M grid and precision for the rest of the process."""
+    _check(lib().pfc_set_tile_width(device, L, M, precision, width), "pfc_set_tile_width")
 
 
 STAGE_ASYNC, STAGE_BULK = 0, 1
 
 
-def col_staging(L: int, M: int, device: int = 0):
-    """Tile staging method of the column kernel for an L x M grid (tuned on the device
-    on first use) and the trials: (stage, {candidate width: (ms async, ms bulk)})."""
+def col_staging(L: int, M: int, device: int = 0, precision: int = MIXED):
+    """Tile staging method of the column kernel for an L x M grid and precision (tuned
+    on the device on first use) and the trials: (stage, {candidate width: (ms async,
+    ms bulk)})."""
     st, n = C.c_int(), C.c_int()
     a = (C.c_float * 4)()
     b = (C.c_float * 4)()
-    _check(lib().pfc_col_staging(device, L, M, C.byref(st), a, b, C.byref(n)), "pfc_col_staging")
-    _, trials = tile_width(L, M, device)
+    _check(lib().pfc_col_staging(device, L, M, precision, C.byref(st), a, b, C.byref(n)), "pfc_col_staging")
+    _, trials = tile_width(L, M, device, precision)
     cand = list(trials)
     return st.value, {cand[i]: (a[i], b[i]) for i in range(n.value)}
 
 
-def set_col_staging(L: int, M: int, stage: int, device: int = 0):
+def set_col_staging(L: int, M: int, stage: int, device: int = 0, precision: int = MIXED):
     """Fix the column kernel's tile staging (STAGE_ASYNC or STAGE_BULK) of an L x M grid."""
-    _check(lib().pfc_set_col_staging(device, L, M, stage), "pfc_set_col_staging")
+    _check(lib().pfc_set_col_staging(device, L, M, precision, stage), "pfc_set_col_staging")
 
 
 def run_bytes(params) -> float:
