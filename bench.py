@@ -1,11 +1,14 @@
-"""Benchmark: PFC Misfit time steps per second at 1024^2, FP32 fused path, batched.
+"""Benchmark: PFC Misfit time steps per second at 1024^2, batched fused step.
 
 Workload (one GPU): B Misfit runs of 1024 x 1024 x 1 (the single-run GPU
-configuration: FP32 complex FFT path with the FP64 k = 0 mode), seeds 1000+i,
-u0/con0 = reference defaults, advanced together.  One "step" advances every run
-of the batch by one time step; `value` is run-steps per second over all GPUs.
-The batch's resident state (B x ~26 MB of row-space arrays) is larger than the
-126 MB L2, so timed steps stream from HBM.
+configuration), seeds 1000+i, u0/con0 = reference defaults, advanced together on the
+default mixed-precision path: FP32 complex arrays in HBM, FP64 arithmetic in the
+kernels, FP64 k = 0 modes; within 1e-5 of pure FP64 after 200 steps.  One "step"
+advances every run of the batch by one time step; `value` is run-steps per second over
+all GPUs.  The batch's resident state (B x ~26 MB of row-space arrays) is larger than
+the 126 MB L2, so timed steps stream from HBM.  The FP32-arithmetic path, the plain
+FP64 path, the 3-D CVD grid, Elastic Analysis at the 1024^2 checkpoint size, the C4
+sweep and the C5 serving mix are reported beside it.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl ours|reference]
 
@@ -29,7 +32,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "pfc-exp-gui_b200"))
 
 GRID = 1024
-METRIC = "PFC Misfit steps/s at 1024^2 (FP32 fused step, batched; run-steps/s)"
+METRIC = "PFC Misfit steps/s at 1024^2 (batched fused step, FP32 storage / FP64 arithmetic; run-steps/s)"
 UNIT = "steps/s"
 
 
@@ -47,6 +50,7 @@ def parse(argv=None):
     ap.add_argument("--no-serve", action="store_true", help="skip the serving (Poisson arrivals) measurement")
     ap.add_argument("--serve-requests", type=int, default=48)
     ap.add_argument("--no-cvd3d", action="store_true", help="skip the 3-D CVD (256x256x64) step measurement")
+    ap.add_argument("--no-elastic", action="store_true", help="skip the Elastic Analysis measurement")
     ap.add_argument("--tile-width", type=int, default=0,
                     help="fix the column tile width instead of the autotuner's choice (reproducible profiles)")
     ap.add_argument("--staging", choices=["auto", "async", "bulk"], default="auto",
@@ -197,15 +201,14 @@ def time_reference_process(exe, steps, outdir):
 
 
 def cpu_steps_per_s(grid, nproc, extra_steps):
-    """Per-step throughput of `nproc` concurrent single-threaded reference processes.
+    """Per-step throughput of `nproc` concurrent single-threaded reference processes
+    (seeds 1000+i, the GPU arm's runs).
 
     Each process runs once with 1 step and once with 1+extra_steps steps (same init
     and the same single checkpoint), so the difference is exactly extra_steps steps."""
     import tempfile
     exe = ref_binary(grid)
-    kind = "reference"
-    if exe is None:
-        kind = "port"
+    kind = "reference" if exe is not None else "port"
     with tempfile.TemporaryDirectory() as tmp:
         def phase(steps):
             if exe is not None:
@@ -213,17 +216,20 @@ def cpu_steps_per_s(grid, nproc, extra_steps):
                 t0 = time.perf_counter()
                 for i in range(nproc):
                     procs.append(subprocess.Popen([exe, "--model", "misfit", "--steps", str(steps), "--mod",
-                                                   str(steps), "--outdir", os.path.join(tmp, f"r{i}_{steps}")],
+                                                   str(steps), "--seed", str(1000 + i),
+                                                   "--outdir", os.path.join(tmp, f"r{i}_{steps}")],
                                                   stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL))
                 for p in procs:
                     p.wait()
                 return time.perf_counter() - t0
             # oracle port (bit-identical restatement of the reference step), one process per core
-            code = ("import sys; sys.path.insert(0, %r); import oracle as O; "
-                    "r = O.Run(O.default_params(0, L=%d, M=%d)); r.step(%d)") % (os.path.join(ROOT, "oracle"), grid,
-                                                                                 grid, steps)
             t0 = time.perf_counter()
-            procs = [subprocess.Popen([sys.executable, "-c", code]) for _ in range(nproc)]
+            procs = []
+            for i in range(nproc):
+                code = ("import sys; sys.path.insert(0, %r); import oracle as O; "
+                        "r = O.Run(O.default_params(0, L=%d, M=%d, seed=%d)); r.step(%d)") % (
+                            os.path.join(ROOT, "oracle"), grid, grid, 1000 + i, steps)
+                procs.append(subprocess.Popen([sys.executable, "-c", code]))
             for p in procs:
                 p.wait()
             return time.perf_counter() - t0
@@ -233,27 +239,36 @@ def cpu_steps_per_s(grid, nproc, extra_steps):
     return nproc * extra_steps / dt, kind
 
 
-def cpu_baseline(grid):
-    v, kind = cpu_steps_per_s(grid, 1, 2)
+def workload(grid, runs):
+    return f"Misfit {grid}x{grid}x1, {runs} runs (seeds 1000+i, u0 0.05, con0 0.2), run-steps/s"
+
+
+def cpu_baseline(grid, steps=2):
+    v, kind = cpu_steps_per_s(grid, 1, steps)
     what = "reference pfc-exp-cli built from its sources" if kind == "reference" else "oracle port of the reference step"
     return {"value": round(v, 4), "unit": UNIT, "cores": 1, "kind": kind,
-            "sample": f"2 Misfit {grid}^2 FP64 steps of one run ({what}; FFTW unavailable, "
-                      "project FFTW-API shim FFT), 1 core; time(1+2 steps) - time(1 step)"}
+            "sample": f"{steps} Misfit {grid}^2 FP64 steps of one run ({what}; FFTW unavailable, "
+                      f"project FFTW-API shim FFT), 1 core; time(1+{steps} steps) - time(1 step)"}
 
 
 def run_reference(args):
+    """The reference program's own CPU step on this host's cores: one single-threaded
+    process per run, as many runs as the GPU arm's batch (fewer if the host has fewer
+    cores), each timed over exactly args.steps steps (capped at 50 so that the arm ends
+    within minutes)."""
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
-    nproc = os.cpu_count() or 1
-    v, kind = cpu_steps_per_s(args.grid, nproc, 2)
-    sample = (f"each step: {nproc} concurrent single-threaded processes x 2 Misfit {args.grid}^2 FP64 steps "
+    nproc = max(1, min(args.batch, os.cpu_count() or 1))
+    steps = max(1, min(args.steps, 50))
+    v, kind = cpu_steps_per_s(args.grid, nproc, steps)
+    sample = (f"{nproc} concurrent single-threaded processes (one per run, seeds 1000+i), each timed over "
+              f"{steps} Misfit {args.grid}^2 FP64 steps as time(1+{steps} steps) - time(1 step) "
               f"({'reference pfc-exp-cli built from its sources' if kind == 'reference' else 'oracle port'}; "
               "FFTW unavailable, project FFTW-API shim FFT)")
     line = {"metric": METRIC, "value": round(v, 4), "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000.0 / v, 3) if v else None,
+            "steps": steps, "warmup": 0, "ms_per_step": round(1000.0 / v, 3) if v else None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"Misfit {args.grid}x{args.grid}x1, reference CPU step (seed 20200604, "
-                                   "u0 0.05, con0 0.2)", "grid": [args.grid, args.grid, 1]},
+            "config": {"workload": workload(args.grid, nproc), "grid": [args.grid, args.grid, 1], "runs": nproc},
             "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": nproc, "kind": kind, "sample": sample},
             "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -420,23 +435,73 @@ def serve_bench(P, dev, n_req=48, lam=4.0, seed=777, budget=150e9):
             "what": "engine with continuous batching; latency = submission to DONE (results and events ready)"}
 
 
+def step_roofline(P, batch, G, B, reps=20):
+    """Event-timed row and column kernel launches of a batch, each against the HBM peak
+    with its algorithmic bytes (row: 4 row-space arrays read, 2 written; column: 4 + 4;
+    8 bytes per complex half-spectrum element)."""
+    row_ms, col_ms = batch.kernel_times(reps)
+    H1 = G // 2 + 1
+    by = {"row": B * G * H1 * 8 * 6, "col": B * G * H1 * 8 * 8}
+    peak, _ = measured_peak()
+    out = {}
+    for name, ms_k in (("row", row_ms), ("col", col_ms)):
+        ach = by[name] / (ms_k / 1000.0) / 1e9
+        out[name] = {"launch_ms": round(ms_k, 5), "algorithmic_bytes_per_launch": by[name],
+                     "achieved": round(ach, 1), "frac": round(ach / peak, 4)}
+    return out
+
+
+def elastic_bench(P, dev, G=1024, steps=500):
+    """Elastic Analysis on a 1024^2 Misfit checkpoint (C2 checkpoint size): peak finder,
+    elastic3D and cryst_order through the C ABI, host arrays in and out."""
+    import numpy as np
+    r = P.Run(P.default_params(P.MODEL_MISFIT, L=G, M=G, seed=1000, device=dev))
+    r.advance(steps, analysis=True)
+    phi, _ = r.fields_f32()
+    r.close()
+    f = phi.reshape(G, G, 1).astype(np.float64)
+    P.phimax_elastic(f)  # first use loads the kernels
+    t = {}
+    t0 = time.perf_counter()
+    atoms = P.phimax_elastic(f)
+    t["peak_s"] = time.perf_counter() - t0
+    x, y, z = atoms[:, 0].copy(), atoms[:, 1].copy(), atoms[:, 2].copy()
+    P.elastic3d(x, y, z, G, G, 1)
+    t0 = time.perf_counter()
+    P.elastic3d(x, y, z, G, G, 1)
+    t["elastic3d_s"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    P.cryst_order(x, y, z, G, G, 1)
+    t["cryst_order_s"] = time.perf_counter() - t0
+    total = sum(t.values())
+    n = len(atoms)
+    return {"workload": f"Misfit {G}^2 state after {steps} steps (seed 1000), Float32 fields", "atoms": n,
+            **{k: round(v, 5) for k, v in t.items()}, "analyses_per_s": round(1.0 / total, 2),
+            "elastic3d_pair_tests_per_s": round(n * (n - 1) / t["elastic3d_s"], 1),
+            "what": "wall time of pfc_phimax_elastic + pfc_elastic3d + pfc_cryst_order on host arrays "
+                    "(each call copies its inputs in and its results out)"}
+
+
 def run_ours(args):
     dist = Dist(args.gpus)
     import numpy as np
     import pfc_b200 as P
     dev = dist.local
     G, B = args.grid, args.batch
+    prec = P.MIXED
     if args.tile_width:
-        P.set_tile_width(G, G, args.tile_width, device=dev)
+        P.set_tile_width(G, G, args.tile_width, device=dev, precision=prec)
     if args.staging != "auto":
-        P.set_col_staging(G, G, P.STAGE_ASYNC if args.staging == "async" else P.STAGE_BULK, device=dev)
+        P.set_col_staging(G, G, P.STAGE_ASYNC if args.staging == "async" else P.STAGE_BULK, device=dev,
+                          precision=prec)
     runs = []
     for i in range(B):
-        p = P.default_params(P.MODEL_MISFIT, L=G, M=G, N=1, seed=1000 + i + 100000 * dist.rank, device=dev)
+        p = P.default_params(P.MODEL_MISFIT, L=G, M=G, N=1, seed=1000 + i + 100000 * dist.rank, device=dev,
+                             precision=prec)
         runs.append(P.Run(p))
     batch = P.Batch(runs)
-    tile_w, tile_trials = P.tile_width(G, G, device=dev)  # chosen by the autotuner at the first run
-    stage, stage_trials = P.col_staging(G, G, device=dev)
+    tile_w, tile_trials = P.tile_width(G, G, device=dev, precision=prec)  # chosen by the autotuner at the first run
+    stage, stage_trials = P.col_staging(G, G, device=dev, precision=prec)
     batch.advance(max(3, args.warmup))
     dist.barrier()
     clocks = Clocks(dev)
@@ -448,66 +513,90 @@ def run_ours(args):
     value = total_run_steps / (ms_max / 1000.0)
 
     # per-kernel roofline (dominant kernel), timed with events on the library stream
-    row_ms, col_ms = batch.kernel_times(20)
-    H1 = G // 2 + 1
-    bytes_row = B * G * H1 * 8 * 6   # 4 row-space arrays read, 2 written
-    bytes_col = B * G * H1 * 8 * 8   # 4 read, 4 written
-    if col_ms >= row_ms:
-        dom, dom_ms, dom_bytes = "k_col_step", col_ms, bytes_col
-    else:
-        dom, dom_ms, dom_bytes = "k_row_step", row_ms, bytes_row
+    kern = step_roofline(P, batch, G, B)
+    dom = "col" if kern["col"]["launch_ms"] >= kern["row"]["launch_ms"] else "row"
+    names = {"row": "k_mrow_step", "col": "k_mcol_step"}
     peak, peak_kind = measured_peak()
-    achieved = dom_bytes / (dom_ms / 1000.0) / 1e9
-    traffic = profiled_traffic(G, B, "col" if dom == "k_col_step" else "row")
-    # both step kernels, each against the same peak (the dominant one is the block above)
-    per_kernel = {}
-    for name, ms_k, by, key in (("k_row_step", row_ms, bytes_row, "row"), ("k_col_step", col_ms, bytes_col, "col")):
-        ach = by / (ms_k / 1000.0) / 1e9
-        per_kernel[name] = {"achieved": round(ach, 1), "frac": round(ach / peak, 4), "launch_ms": round(ms_k, 5),
-                            "algorithmic_bytes_per_launch": by, "traffic": profiled_traffic(G, B, key)}
 
-    # end to end through the public API: host initial fields in, B runs x K steps, host fields out
-    phi0, con0 = runs[0].fields()
-    host_phi = [np.ascontiguousarray(phi0) for _ in range(B)]
-    host_con = [np.ascontiguousarray(con0) for _ in range(B)]
+    # end to end through the public API: FP32 host fields from pinned memory in, B runs x K
+    # steps, FP32 host fields out into pinned memory
+    phi0, con0 = runs[0].fields_f32()
+    try:
+        import torch
+        pin = torch.cuda.is_available()
+    except Exception:  # noqa: BLE001
+        pin = False
+
+    def host_buf():
+        if pin:
+            return torch.empty(G * G, dtype=torch.float32, pin_memory=True).numpy()
+        return np.empty(G * G, np.float32)
+    ins = []
+    for _ in range(B):
+        a, c = host_buf(), host_buf()
+        a[:] = phi0.ravel()
+        c[:] = con0.ravel()
+        ins.append((a, c))
+    outs = [(host_buf(), host_buf()) for _ in range(B)]
     dist.barrier()
     t0 = time.perf_counter()
-    for r, a, c in zip(runs, host_phi, host_con):
-        r.set_fields(a, c)
+    for r, (a, c) in zip(runs, ins):
+        r.set_fields_f32(a, c)
     batch.advance(args.steps)
-    outs = [r.fields_f32() for r in runs]
+    for r, o in zip(runs, outs):
+        r.fields_f32(out=o)
     e2e_s = time.perf_counter() - t0
     e2e_s = dist.max(e2e_s)
     e2e_value = total_run_steps / e2e_s
-    P_pts = G * G
-    h2d = B * P_pts * 16 / args.steps
-    d2h = B * P_pts * 8 / args.steps
-    del outs
+    h2d = B * G * G * 8 / args.steps
+    d2h = B * G * G * 8 / args.steps
 
     line = {
         "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": round(ms_max / args.steps, 5), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 k=0 mode, FP64 denominators)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (reference INITIAL_dis seeded polycrystal, seeds 1000+i)",
-        "config": {"workload": f"Misfit {G}x{G}x1 FP32 fused step, {B} runs per GPU advanced together "
-                               "(graph-captured row/column sweeps)",
-                   "grid": [G, G, 1], "runs_per_gpu": B, "parallelism": f"replicas x{dist.world}",
+        "config": {"workload": workload(G, B), "grid": [G, G, 1], "runs": B,
+                   "path": "fused two-sweep step, mixed precision: FP32 complex arrays in HBM, FP64 arithmetic "
+                           "(pure-FP64 operator), FP64 k=0 modes; graph-captured row/column sweeps",
+                   "parallelism": f"replicas x{dist.world}",
                    "l2": "inputs larger than L2 (resident state ~26 MB/run x batch)",
                    "column_tile_width": tile_w,
                    "column_staging": "async" if stage == P.STAGE_ASYNC else "bulk",
                    "autotuner_trials_ms_per_8_steps": {str(k): {"async": round(a, 4), "bulk": round(b, 4)}
                                                        for k, (a, b) in stage_trials.items()}},
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                     "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes,
-                     "launch_ms": round(dom_ms, 5), "row_ms": round(row_ms, 5), "col_ms": round(col_ms, 5),
-                     "per_kernel": per_kernel},
+        "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": kern[dom]["achieved"], "peak": peak,
+                     "unit": "GB/s", "frac": kern[dom]["frac"], "peak_source": peak_kind,
+                     "traffic": profiled_traffic(G, B, dom),
+                     "algorithmic_bytes_per_launch": kern[dom]["algorithmic_bytes_per_launch"],
+                     "launch_ms": kern[dom]["launch_ms"],
+                     "per_kernel": {names[k]: dict(v, traffic=profiled_traffic(G, B, k)) for k, v in kern.items()}},
         "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h),
-                "what": "pfc_run_set_fields (host FP64 fields) + pfc_batch_advance(K) + pfc_run_get_fields_f32"},
+                "d2h_bytes_per_step": int(d2h), "steps": args.steps, "pinned_host_buffers": pin,
+                "what": "pfc_run_set_fields_f32 (FP32 host fields) + pfc_batch_advance(K) + pfc_run_get_fields_f32, "
+                        "wall clock"},
         "gpu_launches": 2 * args.steps,
         "clocks": clk,
     }
+    batch.close()
+    for r in runs:
+        r.close()
+    # the FP32-arithmetic fused path on the same batch (faster, but 7e-5 from pure FP64 after
+    # 200 steps at 1024^2, outside the 1e-5 bound)
+    runs32 = [P.Run(P.default_params(P.MODEL_MISFIT, L=G, M=G, seed=1000 + i, device=dev, precision=P.FP32))
+              for i in range(B)]
+    b32 = P.Batch(runs32)
+    b32.advance(5)
+    ms32 = b32.advance_timed(min(args.steps, 200))
+    k32 = step_roofline(P, b32, G, B)
+    line["fp32_path"] = {"run_steps_per_s": round(B * min(args.steps, 200) / (ms32 / 1000.0), 2),
+                         "ms_per_step": round(ms32 / min(args.steps, 200), 5),
+                         "column_tile_width": P.tile_width(G, G, device=dev, precision=P.FP32)[0],
+                         "per_kernel": {"k_row_step": k32["row"], "k_col_step": k32["col"]},
+                         "what": "the same batch on the FP32-arithmetic path (opt-in --precision fp32)"}
+    b32.close()
+    for r in runs32:
+        r.close()
     # the plain FP64 GPU path (one run, the reference's step structure) on the same grid
     if not args.no_fp64_plain:
         r64 = P.Run(P.default_params(P.MODEL_MISFIT, L=G, M=G, N=1, seed=1000, device=dev, precision=P.FP64))
@@ -516,11 +605,19 @@ def run_ours(args):
         ms64 = r64.advance_timed(n64)
         r64.close()
         fp64_sps = n64 / (ms64 / 1000.0)
-        line["fp64_plain"] = {"steps_per_s": round(fp64_sps, 2),
+        # 13 complex-double 3-D DFTs per step, each 3 axis passes reading and writing 16 B per
+        # point, plus the pointwise kernels' 14 reads and writes of complex doubles per point
+        fp64_bytes = G * G * (13 * 3 * 2 * 16 + 14 * 16)
+        ach64 = fp64_bytes / (ms64 / n64 / 1000.0) / 1e9
+        line["fp64_plain"] = {"steps_per_s": round(fp64_sps, 2), "ms_per_step": round(ms64 / n64, 4),
                               "what": "one Misfit run, plain FP64 path (13 complex-double 3-D DFTs + pointwise "
                                       "kernels per step, reference roundings), CUDA events",
-                              "batched_fp32_over_fp64_plain": round(value / dist.world / fp64_sps, 2)}
-    # the 3-D CVD workload (256 x 256 x 64): 3-D runs take the plain FP64 path
+                              "roofline": {"bound": "hbm", "achieved": round(ach64, 1),
+                                           "frac": round(ach64 / peak, 4),
+                                           "algorithmic_bytes_per_step": fp64_bytes},
+                              "batched_over_fp64_plain": round(value / dist.world / fp64_sps, 2),
+                              "fp32_path_over_fp64_plain": round(line["fp32_path"]["run_steps_per_s"] / fp64_sps, 2)}
+    # the 3-D CVD workload (256 x 256 x 64)
     if not args.no_cvd3d:
         r3 = P.Run(P.default_params(P.MODEL_CVD, L=256, M=256, N=64, device=dev, precision=P.FP64))
         r3.advance(2)
@@ -537,14 +634,13 @@ def run_ours(args):
                          "cli_step_with_energy_ms": round(cli_ms, 3),
                          "what": "pfc_run_advance_timed (CUDA events) of 10 steps; cli_step_with_energy_ms is wall "
                                  "time of advance(1) + pfc_run_energy"}
+    if not args.no_elastic:
+        line["elastic"] = elastic_bench(P, dev, G)
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(G)
         except Exception as e:  # noqa: BLE001
             line["cpu_baseline"] = {"value": None, "error": str(e)}
-    batch.close()
-    for r in runs:
-        r.close()
     # sweep and serving workloads, each rank on its own GPU (rank 0 reports its own)
     if not args.no_sweep:
         line["sweep"] = sweep_bench(P, dev)

@@ -34,6 +34,7 @@ extern "C" {
 #define PFC_E_NOMEM (-3)     /* device or host allocation failed */
 #define PFC_E_IO (-4)        /* file read/write failure */
 #define PFC_E_STATE (-5)     /* call not valid in the object's current state */
+#define PFC_E_NONFINITE (-6) /* a run's fields became non-finite (NaN or Inf) */
 
 #define PFC_MODEL_MISFIT 0
 #define PFC_MODEL_CVD 1
@@ -129,10 +130,21 @@ int pfc_run_get_fields(pfc_run *r, double *phi, double *con);
 int pfc_run_get_fields_f32(pfc_run *r, float *phi, float *con);
 /* Replace the state with the given real fields (double, reference layout). */
 int pfc_run_set_fields(pfc_run *r, const double *phi, const double *con);
+/* Same from FP32 fields (the values a VTI checkpoint holds): copied to the device as
+ * they are (asynchronously from pinned host memory), the means summed on the device.
+ * Returns when the new state is in place. */
+int pfc_run_set_fields_f32(pfc_run *r, const float *phi, const float *con);
 
 /* ENERGYC2 of the current state: sum(e)/L/M/N and sum(phi)/L/M/N as written to
  * energy.txt (MIS:1081-1085).  Valid after pfc_run_advance(..., analysis=1). */
 int pfc_run_energy(pfc_run *r, double *e_over_p, double *mass_over_p);
+
+/* Whether a fused-path (mixed or FP32) run has met a non-finite nonlinear term since it
+ * was created or since the last call (*flag = 1: its fields hold NaN or Inf).  Waits for
+ * the run's queued steps.  The engine fails such a run alone (PFC_EV_FAILED with
+ * PFC_E_NONFINITE) and keeps the others running.  (No reference counterpart: the
+ * reference keeps stepping and writes the NaN fields.) */
+int pfc_run_nonfinite(pfc_run *r, int *flag);
 
 /* FP64 k = 0 modes of phi and con divided by P (the conserved means). */
 int pfc_run_means(const pfc_run *r, double *phi_mean, double *con_mean);

@@ -444,6 +444,7 @@ static void free_run(pfc_run *r) {
     if (!r) return;
     release_kcoef(r);
     if (r->dev_mem) cudaFree(r->dev_mem);
+    if (r->h_nonfinite) cudaFreeHost((void *)r->h_nonfinite);
     if (r->f64) fp64_destroy(r->f64);
     delete r;
 }
@@ -472,8 +473,6 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
         (p->grainx <= 0 || p->grainy <= 0 || p->grainz <= 0 || p->grainx > p->L || p->grainy > p->M || p->grainz > p->N))
         return set_error(PFC_E_INVALID, "grain counts must be in [1, grid extent]");
     if (!(p->axx >= 0.0f)) return set_error(PFC_E_INVALID, "axx must be >= 0");
-    if (p->axx > 0.0f && p->model == PFC_MODEL_MISFIT && !fused)
-        return set_error(PFC_E_INVALID, "stochastic noise (axx > 0) runs on the fused (mixed, FP32) paths only");
     Context *ctx = nullptr;
     int rc = get_context(p->device, &ctx);
     if (rc != PFC_OK) return rc;
@@ -583,6 +582,19 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
     d.noise_amp = (p->model == PFC_MODEL_MISFIT && r->b0 != 0.0f) ? p->dt * r->b0 : 0.0f;
     d.noise_key = noise_key(p->seed);
     d.noise_amp_d = (p->model == PFC_MODEL_MISFIT && r->b0 != 0.0f) ? (double)p->dt * (double)r->b0 : 0.0;
+    if (fused) {
+        int *hf = nullptr;
+        cudaError_t ce = cudaHostAlloc(reinterpret_cast<void **>(&hf), sizeof(int), cudaHostAllocMapped);
+        if (ce == cudaSuccess) {
+            *hf = 0;
+            r->h_nonfinite = hf;
+            ce = cudaHostGetDevicePointer(reinterpret_cast<void **>(&d.nonfinite), hf, 0);
+        }
+        if (ce != cudaSuccess) {
+            free_run(r);
+            return cuda_error(ce, "run status word");
+        }
+    }
     if (fused) {
         cudaError_t ce = cudaMemcpyAsync(r->d_desc, &d, sizeof(RunDesc), cudaMemcpyHostToDevice, r->stream);
         if (ce != cudaSuccess) {
@@ -1161,6 +1173,21 @@ extern "C" int pfc_run_set_fields(pfc_run *r, const double *phi, const double *c
     return fp32_from_real(r, false);
 }
 
+// FP32 host fields: one cudaMemcpyAsync per field straight into the run's real-field
+// arrays (asynchronous when the host arrays are pinned), the FP64 means summed on the
+// device, then the row-space state built as for pfc_run_set_fields.
+extern "C" int pfc_run_set_fields_f32(pfc_run *r, const float *phi, const float *con) {
+    if (!r || !phi || !con) return set_error(PFC_E_INVALID, "null argument");
+    PFC_CUDA_TRY(cudaSetDevice(r->p.device));
+    if (!fused_path(r->p.precision)) {
+        std::vector<double> a(phi, phi + r->P), b(con, con + r->P);
+        return fp64_set_fields(r, a.data(), b.data());
+    }
+    PFC_CUDA_TRY(cudaMemcpyAsync(r->desc.psi_real, phi, r->P * sizeof(float), cudaMemcpyHostToDevice, r->stream));
+    PFC_CUDA_TRY(cudaMemcpyAsync(r->desc.con_real, con, r->P * sizeof(float), cudaMemcpyHostToDevice, r->stream));
+    return fp32_from_real(r, true);
+}
+
 extern "C" int pfc_run_energy(pfc_run *r, double *e_over_p, double *mass_over_p) {
     if (!r) return set_error(PFC_E_INVALID, "null run");
     PFC_CUDA_TRY(cudaSetDevice(r->p.device));
@@ -1171,6 +1198,16 @@ extern "C" int pfc_run_energy(pfc_run *r, double *e_over_p, double *mass_over_p)
     PFC_SYNC_CHECKED(r->ctx, r->stream);
     if (e_over_p) *e_over_p = s[0] / r->L / r->M / r->N;
     if (mass_over_p) *mass_over_p = s[1] / r->L / r->M / r->N;
+    return PFC_OK;
+}
+
+extern "C" int pfc_run_nonfinite(pfc_run *r, int *flag) {
+    if (!r || !flag) return set_error(PFC_E_INVALID, "null argument");
+    if (!fused_path(r->p.precision)) return set_error(PFC_E_INVALID, "the check belongs to the fused paths");
+    PFC_CUDA_TRY(cudaSetDevice(r->p.device));
+    PFC_SYNC_CHECKED(r->ctx, r->stream);
+    *flag = *r->h_nonfinite != 0 ? 1 : 0;
+    *r->h_nonfinite = 0;
     return PFC_OK;
 }
 

@@ -17,7 +17,8 @@
 // Twiddles come from a per-length table computed on the host in double and rounded
 // once to the working precision, laid out by stage (twiddle_offset): the R factors
 // exp(-2 pi i r k / (Ns R)), r < R, that one butterfly of a stage needs are
-// contiguous, so a thread fetches them with R/2 (FP32) or R (FP64) 16-byte loads.
+// contiguous, so an FP32 thread fetches them with R/2 16-byte loads; an FP64 thread
+// loads the base factor r = 1 and forms the others (twiddle_powers).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -240,6 +241,21 @@ template <int R> __device__ __forceinline__ void load_twiddles(const double2 *__
     for (int i = 0; i < R; ++i) t[i] = __ldg(p + i);
 }
 
+// FP64 stages multiply by the powers w^r, r < R, of one loaded base factor
+// w = exp(-2 pi i k / (Ns R)) (table entry k*R + 1) instead of loading all R factors: a
+// double2 factor is 16 bytes, as much L1 traffic per element as the data itself.  Each
+// power is a product of two lower powers (p[r] = p[r/2] p[r - r/2]), so it carries at most
+// log2(R) + 1 roundings of double (~5e-16), well below what a loaded FP32 factor carries.
+template <int R, bool FWD> __device__ __forceinline__ void twiddle_powers(double2 (&v)[R], double2 w) {
+    double2 p[R];
+    p[0] = make_double2(1.0, 0.0);
+    p[1] = w;
+#pragma unroll
+    for (int r = 2; r < R; ++r) p[r] = cmul(p[r / 2], p[r - r / 2]);
+#pragma unroll
+    for (int r = 1; r < R; ++r) v[r] = FWD ? cmul(v[r], p[r]) : cmulc(v[r], p[r]);
+}
+
 // Memory spaces a stage reads from / writes to.
 enum : int { SP_SMEM = 0, SP_GLOBAL = 1, SP_REGS = 2 };
 
@@ -300,10 +316,14 @@ __device__ __forceinline__ void stage(const CI *__restrict__ in, typename nodedu
             const int b = w % NB, j = w / NB;
             const int k = j % NS;
             if constexpr (NS > 1) {
-                C t[R];
-                load_twiddles<R>(tw + twiddle_offset(NS) + k * R, t);
+                if constexpr (std::is_same<C, double2>::value) {
+                    twiddle_powers<R, FWD>(v[q], __ldg(tw + twiddle_offset(NS) + k * R + 1));
+                } else {
+                    C t[R];
+                    load_twiddles<R>(tw + twiddle_offset(NS) + k * R, t);
 #pragma unroll
-                for (int r = 1; r < R; ++r) v[q][r] = FWD ? cmul(v[q][r], t[r]) : cmulc(v[q][r], t[r]);
+                    for (int r = 1; r < R; ++r) v[q][r] = FWD ? cmul(v[q][r], t[r]) : cmulc(v[q][r], t[r]);
+                }
             }
             dftR<R, FWD>(v[q]);
             if constexpr (OUT != SP_REGS) {

@@ -79,6 +79,7 @@ struct pfc_run {
     bool energy_valid = false;
     pfc::Fp64State *f64 = nullptr;
     bool kcoef_held = false;        // holds a reference on the shared coefficient table
+    volatile int *h_nonfinite = nullptr;  // fused paths: host view of RunDesc::nonfinite (mapped pinned)
     std::vector<double> kd_host;    // mixed path: the double k-vectors (lengths L and M)
 };
 

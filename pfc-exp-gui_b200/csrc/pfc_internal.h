@@ -62,6 +62,9 @@ struct RunDesc {
     const double2 *kc2d;
     const double *kdl, *kdm;
     double noise_amp_d;  // dt * b0 in double (0 = off)
+    // set to 1 (device-visible, mapped pinned host memory) by a row-step kernel that met a
+    // non-finite nonlinear term (NaN / Inf in the run's fields); the engine fails the run
+    int *nonfinite;
     // per-CTA partial sums written by the analysis row kernel: [2 * L] doubles
     double *partials;
     // batched runs only: slots of (energy sum, mass sum) that launch_reduce_runs fills

@@ -634,6 +634,13 @@ int quantum(pfc_engine *e) {
         j->run->fields_valid = j->spec.kind == PFC_JOB_CVD;
         j->run->energy_valid = false;
     }
+    // a run whose fields went non-finite in this quantum fails alone; the others go on
+    // (their kernels never read another run's data)
+    for (Job *j : std::vector<Job *>(e->active)) {
+        if (*j->run->h_nonfinite == 0) continue;
+        ckpt.erase(std::remove(ckpt.begin(), ckpt.end(), j), ckpt.end());
+        finish_job(e, j, PFC_EV_FAILED, PFC_E_NONFINITE);
+    }
     for (Job *j : ckpt) {
         const int rc = misfit_checkpoint(e, j);
         if (rc != PFC_OK) return rc;

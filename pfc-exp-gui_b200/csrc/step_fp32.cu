@@ -225,6 +225,7 @@ __global__ void __launch_bounds__(RowCfg<M>::NT, 2) k_row_step(const RunDesc *__
     const float inv_c0 = 1.0f / d.k.para_c0, inv_1mc0 = 1.0f / (1.0f - d.k.para_c0);
     float2 out[PTS];
     float mi = 0.f, mj = 0.f;
+    bool bad = false;
 #pragma unroll
     for (int q = 0; q < PTS; ++q) {
         const int w = threadIdx.x + q * NT;
@@ -236,11 +237,13 @@ __global__ void __launch_bounds__(RowCfg<M>::NT, 2) k_row_step(const RunDesc *__
             out[q] = make_float2(t.inn, t.inc);
             mi = fmaxf(mi, fabsf(t.inn));
             mj = fmaxf(mj, fabsf(t.inc));
+            bad |= !(isfinite(t.inn) && isfinite(t.inc));
         }
     }
     block_max_put(wmax[2], mi);
     block_max_put(wmax[3], mj);
-    __syncthreads();
+    // a non-finite term marks the run (fmaxf would pass over a NaN)
+    if (__syncthreads_or(bad) && threadIdx.x == 0) *d.nonfinite = 1;
     // inc rides as 2^e2 * inc beside inn
     const int e2 = balance_exp(block_max_get<NW>(wmax[2]), block_max_get<NW>(wmax[3]));
     const float s2 = pow2f(e2);

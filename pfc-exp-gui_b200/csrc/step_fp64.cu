@@ -9,7 +9,10 @@
 // the fused FP32 path is measured against; it is not tuned beyond coalesced access.
 //
 // The noise term (Gauss + p5, MIS:490-491) is omitted when b0 == 0: it is then a
-// signed zero.
+// signed zero.  With axx > 0 (Misfit) the reference's own sequential generator runs on
+// the host each step (gauss_host: polar Box-Muller on one splitmix64 stream per step,
+// MIS:951-981), so the noise field is the reference's value for value; it is uploaded,
+// transformed (p5) and added in the update as MAINEQUATIONC2_NOI does (MIS:983-1014).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -28,6 +31,8 @@ struct Fp64State {
     double *C2Ad, *C2Bd;        // pure-FP64 tables
     double *kd;                 // pure-FP64 k-vectors, lengths L, M, N
     double *partials;           // energy partial sums
+    double2 *nois, *noisf;      // noise field and its transform (Misfit with b0 != 0)
+    std::vector<float> host_noise;
     int exact;                  // 1: reference float roundings, 0: pure FP64
     void *mem;
 };
@@ -195,18 +200,31 @@ __global__ void k64_inc2mix(const double2 *in1, const double2 *in2, const double
     }
 }
 
-// MAINEQUATIONC2MIX / MAINEQUATIONC2_NOI with b0 == 0 (MIS:928-1014, CVD:865-886)
+// MAINEQUATIONC2MIX / MAINEQUATIONC2_NOI (MIS:928-1014, CVD:865-886).  noisf != null
+// adds the noise term dt*b0 * xi^ * |k| * mask * lowpass (MIS:1002-1003): the masks
+// detrx = (l == 0), detrxn = (l == L/2), detry = (m == 0), detryn = (m == M/2) keep the
+// real part (weight sqrt(|0.5 + 0.5 (detrx + detrxn)(detry + detryn)|)) and the
+// imaginary part (sqrt(|0.5 - 0.5 (...)(...)|)) of the transformed white noise.
 __global__ void k64_main_eq(double2 *phiHat, double2 *conHat, const double2 *outn, const double2 *outc,
                             const float *kl, const float *km, const float *kn, const double *kd, int L, int M, int N,
-                            float mn, float mc, float alpha, float dt, int exact) {
+                            float mn, float mc, float alpha, float dt, int exact, const double2 *noisf, float b0) {
     const long P = (long)L * M * N;
     GRID_LOOP(i, P) {
         const int n = (int)(i % N), m = (int)((i / N) % M), l = (int)(i / ((long)N * M));
+        const double dm = (double)((l == 0) + (l == L / 2)) * (double)((m == 0) + (m == M / 2));
         if (exact) {
             const float ks = __fadd_rn(__fadd_rn(__fmul_rn(kl[l], kl[l]), __fmul_rn(km[m], km[m])), __fmul_rn(kn[n], kn[n]));
             const float an = __fmul_rn(__fmul_rn(mn, dt), ks);
-            const float R1 = (float)(phiHat[i].x - (double)an * outn[i].x);
-            const float R2 = (float)(phiHat[i].y - (double)an * outn[i].y);
+            double nre = 0.0, nim = 0.0;
+            if (noisf) {
+                const double sk = (double)__fsqrt_rn(ks);
+                const double lp = 0.5 - 0.5 * tanh((sk - 2.0 * PI_REF) / 0.1);
+                const double db = (double)__fmul_rn(dt, b0);  // dt * b0 in float, as the reference forms it
+                nre = db * noisf[i].x * sk * sqrt(fabs(0.5 + 0.5 * dm)) * lp;
+                nim = db * noisf[i].y * sk * sqrt(fabs(0.5 - 0.5 * dm)) * lp;
+            }
+            const float R1 = (float)(phiHat[i].x - (double)an * outn[i].x + nre);
+            const float R2 = (float)(phiHat[i].y - (double)an * outn[i].y + nim);
             phiHat[i] = make_double2((double)R1 / (1.0 + (double)an), (double)R2 / (1.0 + (double)an));
             const float ac = __fmul_rn(__fmul_rn(mc, dt), ks);
             const float R3 = (float)(conHat[i].x - (double)ac * outc[i].x);
@@ -217,7 +235,15 @@ __global__ void k64_main_eq(double2 *phiHat, double2 *conHat, const double2 *out
             // pure FP64: k-vectors in double
             const double ks = kd[l] * kd[l] + kd[L + m] * kd[L + m] + kd[L + M + n] * kd[L + M + n];
             const double an = (double)mn * dt * ks, ac = (double)mc * dt * ks, dc = (double)mc * dt * alpha * ks * ks;
-            phiHat[i] = make_double2((phiHat[i].x - an * outn[i].x) / (1.0 + an), (phiHat[i].y - an * outn[i].y) / (1.0 + an));
+            double nre = 0.0, nim = 0.0;
+            if (noisf) {
+                const double sk = sqrt(ks);
+                const double lp = 0.5 - 0.5 * tanh((sk - 2.0 * PI_REF) / 0.1);
+                nre = (double)dt * (double)b0 * noisf[i].x * sk * sqrt(fabs(0.5 + 0.5 * dm)) * lp;
+                nim = (double)dt * (double)b0 * noisf[i].y * sk * sqrt(fabs(0.5 - 0.5 * dm)) * lp;
+            }
+            phiHat[i] = make_double2((phiHat[i].x - an * outn[i].x + nre) / (1.0 + an),
+                                     (phiHat[i].y - an * outn[i].y + nim) / (1.0 + an));
             conHat[i] = make_double2((conHat[i].x - ac * outc[i].x) / (1.0 + dc), (conHat[i].y - ac * outc[i].y) / (1.0 + dc));
         }
     }
@@ -341,14 +367,46 @@ static unsigned grid_for(long P) {
         if (_e != cudaSuccess) return cuda_error(_e, #expr); \
     } while (0)
 
+// Gauss (MIS:951-981): the reference's noise field of loop index `timestep`, value for
+// value: one splitmix64 stream (pfc_common.h:165-176) keyed by the base seed, the rank
+// (0 in one process) and the step, polar Box-Muller with rejection, f * v1 per point.
+// Sequential by construction (each point's draws depend on the rejections before it).
+static void gauss_host(uint32_t seed, int timestep, std::vector<float> &out) {
+    uint64_t st = (uint64_t)seed;
+    st ^= (uint64_t)((unsigned int)(0 + 1)) * 2654435761ULL;
+    st ^= (uint64_t)((unsigned int)timestep) * 374761393ULL;
+    auto u01 = [&st]() {
+        uint64_t z = (st += 0x9e3779b97f4a7c15ULL);
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+        z ^= z >> 31;
+        return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    };
+    for (size_t i = 0; i < out.size(); ++i) {
+        float v1 = 0.0f, v2 = 0.0f, r2 = 2.0f;
+        while (r2 >= 1.0f || r2 <= 0.0f) {
+            v1 = (float)(2.0 * u01() - 1.0);
+            v2 = (float)(2.0 * u01() - 1.0);
+            r2 = v1 * v1 + v2 * v2;
+        }
+        const float f = (float)std::sqrt(-2. * logf(r2) / r2);
+        out[i] = f * v1;
+    }
+}
+
+// real noise values (float, staged in the first half of the noisf buffer) -> complex doubles
+__global__ void k64_widen_noise(const float *in, double2 *out, long P) {
+    GRID_LOOP(i, P) out[i] = make_double2((double)in[i], 0.0);
+}
+
 int fp64_create(pfc_run *r) {
-    Fp64State *s = new Fp64State();
-    std::memset(s, 0, sizeof(*s));
+    Fp64State *s = new Fp64State();  // value-initialised: every pointer null
     const size_t cz = (size_t)r->P * sizeof(double2);
     const size_t fz = ((size_t)r->P * sizeof(float) + 255) / 256 * 256;
     const size_t dz = ((size_t)r->P * sizeof(double) + 255) / 256 * 256;
     const size_t kz = ((size_t)(r->L + r->M + r->N) * sizeof(double) + 255) / 256 * 256;
-    const size_t bytes = 22 * cz + 2 * fz + 2 * dz + kz + (2 * EBLOCKS + 16) * sizeof(double);
+    const bool noise = r->p.model == PFC_MODEL_MISFIT && r->b0 != 0.0f;
+    const size_t bytes = (22 + (noise ? 2 : 0)) * cz + 2 * fz + 2 * dz + kz + (2 * EBLOCKS + 16) * sizeof(double);
     cudaError_t e = cudaMalloc(&s->mem, bytes);
     if (e != cudaSuccess) {
         delete s;
@@ -374,6 +432,13 @@ int fp64_create(pfc_run *r) {
     s->kd = (double *)m;
     m += kz;
     s->partials = (double *)m;
+    m += (2 * EBLOCKS + 16) * sizeof(double);
+    if (noise) {
+        s->nois = (double2 *)m;
+        m += cz;
+        s->noisf = (double2 *)m;
+        s->host_noise.resize(r->P);
+    }
     s->exact = r->p.precision == PFC_PRECISION_FP64 ? 1 : 0;
     r->f64 = s;
     // C2AK / C2BK tables (MIS:700-750) evaluated on the host exactly as the reference does
@@ -475,8 +540,17 @@ int fp64_advance(pfc_run *r, int nsteps) {
         TRY(fft3d(r, s->inn, s->outn, true));   // p8
         TRY(fft3d(r, s->inc, s->outc, true));   // p9
         TRY(fft3d(r, s->con, s->conHat, true)); // p6
+        if (s->nois) {
+            // Gauss (MIS:951-981) for this step's loop index, then p5
+            gauss_host(r->p.seed, r->t + it, s->host_noise);
+            TRY(cudaMemcpyAsync(s->noisf, s->host_noise.data(), P * sizeof(float), cudaMemcpyHostToDevice, r->stream));
+            k64_widen_noise<<<grid_for(P), 256, 0, r->stream>>>((const float *)s->noisf, s->nois, P);
+            TRY(cudaGetLastError());
+            TRY(fft3d(r, s->nois, s->noisf, true));  // p5
+        }
         k64_main_eq<<<grid_for(P), 256, 0, r->stream>>>(s->phiHat, s->conHat, s->outn, s->outc, kl, km, kn, s->kd, r->L, r->M,
-                                                        r->N, k.dynamic_mn, k.dynamic_mc, k.para_alpha, r->p.dt, exact);
+                                                        r->N, k.dynamic_mn, k.dynamic_mc, k.para_alpha, r->p.dt, exact,
+                                                        s->nois ? s->noisf : nullptr, r->b0);
         TRY(cudaGetLastError());
         k64_gra_pre<<<grid_for(P), 256, 0, r->stream>>>(s->conHat, kl, km, kn, s->kd, s->gra1, s->gra2, s->gra3, r->L, r->M,
                                                         r->N, exact);

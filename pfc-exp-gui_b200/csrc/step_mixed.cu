@@ -172,6 +172,7 @@ __global__ void __launch_bounds__(MRowCfg<M>::NT, MRowCfg<M>::MINB) k_mrow_step(
     const double invM = 1.0 / (double)M;
     const CoefsD kc = coefs_d(d.k);
     double2 out[PTS];
+    bool bad = false;
 #pragma unroll
     for (int q = 0; q < PTS; ++q) {
         const int w = threadIdx.x + q * NT;
@@ -181,9 +182,11 @@ __global__ void __launch_bounds__(MRowCfg<M>::NT, MRowCfg<M>::MINB) k_mrow_step(
             const TermsD t =
                 point_terms_d(kc, z1.x * invM + d.psi_mean, z1.y * invM + d.con_mean, z2.x * invM, z2.y * invM);
             out[q] = make_double2(t.inn, t.inc);
+            bad |= !(isfinite(t.inn) && isfinite(t.inc));
         }
     }
-    __syncthreads();  // every thread has read the inverse transforms
+    // every thread has read the inverse transforms; a non-finite term marks the run
+    if (__syncthreads_or(bad) && threadIdx.x == 0) *d.nonfinite = 1;
 #pragma unroll
     for (int q = 0; q < PTS; ++q) {
         const int w = threadIdx.x + q * NT;

@@ -27,7 +27,7 @@ FP64_PURE = 2
 MIXED = 3  # FP32 arrays in HBM, FP64 arithmetic (the default precision)
 
 PFC_OK = 0
-PFC_E_INVALID, PFC_E_CUDA, PFC_E_NOMEM, PFC_E_IO, PFC_E_STATE = -1, -2, -3, -4, -5
+PFC_E_INVALID, PFC_E_CUDA, PFC_E_NOMEM, PFC_E_IO, PFC_E_STATE, PFC_E_NONFINITE = -1, -2, -3, -4, -5, -6
 
 
 class PfcError(RuntimeError):
@@ -128,6 +128,8 @@ def lib():
         "pfc_run_set_fields": ([vp, dp, dp], C.c_int),
         "pfc_run_energy": ([vp, dp, dp], C.c_int),
         "pfc_run_means": ([vp, dp, dp], C.c_int),
+        "pfc_run_set_fields_f32": ([vp, fp, fp], C.c_int),
+        "pfc_run_nonfinite": ([vp, P(C.c_int)], C.c_int),
         "pfc_batch_create": ([P(vp), C.c_int, P(vp)], C.c_int),
         "pfc_batch_destroy": ([vp], C.c_int),
         "pfc_batch_advance": ([vp, C.c_int], C.c_int),
@@ -236,12 +238,24 @@ class Run:
         s = (self.L, self.M, self.N)
         return phi.reshape(s), con.reshape(s)
 
-    def fields_f32(self):
-        phi = np.empty(self.P, np.float32)
-        con = np.empty(self.P, np.float32)
+    def fields_f32(self, out=None):
+        """FP32 real fields (phi, con) shaped (L, M, N); `out` = (phi, con) float32 arrays of
+        P elements (e.g. pinned host buffers) to fill instead of new ones."""
+        if out is None:
+            phi = np.empty(self.P, np.float32)
+            con = np.empty(self.P, np.float32)
+        else:
+            phi, con = out
         _check(lib().pfc_run_get_fields_f32(self.h, _fp(phi), _fp(con)), "pfc_run_get_fields_f32")
         s = (self.L, self.M, self.N)
         return phi.reshape(s), con.reshape(s)
+
+    def set_fields_f32(self, phi, con):
+        """Replace the state with FP32 real fields (copied as they are; pinned arrays make
+        the copy asynchronous)."""
+        phi = np.ascontiguousarray(phi, np.float32).ravel()
+        con = np.ascontiguousarray(con, np.float32).ravel()
+        _check(lib().pfc_run_set_fields_f32(self.h, _fp(phi), _fp(con)), "pfc_run_set_fields_f32")
 
     def set_fields(self, phi, con):
         phi = np.ascontiguousarray(phi, np.float64).ravel()
@@ -252,6 +266,12 @@ class Run:
         e, d = C.c_double(), C.c_double()
         _check(lib().pfc_run_energy(self.h, C.byref(e), C.byref(d)), "pfc_run_energy")
         return e.value, d.value
+
+    def nonfinite(self) -> bool:
+        """True when the run met a NaN / Inf nonlinear term since creation or the last call."""
+        f = C.c_int()
+        _check(lib().pfc_run_nonfinite(self.h, C.byref(f)), "pfc_run_nonfinite")
+        return bool(f.value)
 
     def means(self):
         a, b = C.c_double(), C.c_double()

@@ -131,6 +131,44 @@ def test_engine_results_same_alone_and_in_mix():
     mix.close()
 
 
+def test_engine_fails_a_nonfinite_run_alone():
+    """A run whose fields go NaN (con0 > 1 puts log((1 - c) / (1 - c0)) out of its domain,
+    a host-side way to make one run fail) gets PFC_EV_FAILED with PFC_E_NONFINITE; the
+    runs batched with it finish, bit for bit as when they run alone."""
+    good = [params(P.MODEL_MISFIT, 128, 128, seed=11), params(P.MODEL_MISFIT, 128, 128, seed=12),
+            params(P.MODEL_CVD, 64, 64, seed=3)]
+    kinds = [P.JOB_MISFIT, P.JOB_MISFIT, P.JOB_CVD]
+    alone = P.Engine()
+    ref = []
+    for k, p in zip(kinds, good):
+        j = alone.submit(k, p, steps=60, mod=30)
+        drain(alone, [j])
+        ref.append(alone.fields(j))
+    alone.close()
+    mix = P.Engine(quantum_steps=32)
+    bad = mix.submit(P.JOB_MISFIT, params(P.MODEL_MISFIT, 128, 128, seed=13, con0=1.5), steps=60, mod=30)
+    ids = [mix.submit(k, p, steps=60, mod=30) for k, p in zip(kinds, good)]
+    ev = drain(mix, [bad] + ids)
+    last = ev[bad][-1]
+    assert last.type == P.EV_FAILED and last.status == P.PFC_E_NONFINITE, (last.type, last.status)
+    assert last.step <= 32  # caught at the end of its first quantum
+    for j, (rphi, rcon) in zip(ids, ref):
+        assert ev[j][-1].type == P.EV_DONE
+        phi, con = mix.fields(j)
+        assert same_bits(phi, rphi) and same_bits(con, rcon)
+    mix.close()
+
+
+def test_run_reports_nonfinite_fields():
+    r = P.Run(params(P.MODEL_MISFIT, 64, 64, con0=1.5))
+    r.advance(2)
+    assert r.nonfinite()
+    assert not r.nonfinite()  # the flag is cleared once reported
+    ok = P.Run(params(P.MODEL_MISFIT, 64, 64))
+    ok.advance(5)
+    assert not ok.nonfinite()
+
+
 def run_cli(args, outdir):
     subprocess.run([P.CLI_PATH] + args + ["--outdir", outdir], check=True, stdout=subprocess.DEVNULL,
                    stderr=subprocess.DEVNULL)

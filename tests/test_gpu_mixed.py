@@ -66,8 +66,9 @@ def test_mixed_matches_pure_fp64_oracle(model, L, M, steps):
     assert err <= 1e-6
     e, d = r.energy()
     oe, od = o.energy()
-    # the energy moves with the fields (a 3e-7 field deviation shifts CVD's e/P ~ 0.03 by ~1e-7)
-    assert abs(e - oe) <= 1e-6 * abs(oe) + 1e-8
+    # the energy density's derivative in the fields is O(1): the energy moves by at most the
+    # field deviation (CVD 64^2: 3.2e-7 in the fields, 8.2e-8 in e/P ~ 0.03)
+    assert abs(e - oe) <= err + 1e-9
     # the run starts from the FP32 initial fields (the reference's Float32 checkpoint values),
     # whose mean differs from the double initial fields' by up to ~1e-9 on CVD grids
     assert abs(d - od) <= 1e-9 * abs(od) + 5e-9

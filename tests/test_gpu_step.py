@@ -334,6 +334,25 @@ def test_noise_stream_is_deterministic_and_per_step():
         assert np.array_equal(s.fields_f32()[0].view(np.uint32), t.fields_f32()[0].view(np.uint32))
 
 
-def test_noise_rejected_on_fp64_path():
-    with pytest.raises(P.PfcError):
-        gpu_run(P.MODEL_MISFIT, 64, 64, precision=P.FP64, axx=0.005)
+def test_fp64_noise_matches_reference_run():
+    """--axx > 0 on the plain FP64 path runs the reference's own sequential generator
+    (Gauss, MIS:951-981) on the host, so the reference-exact mode follows the reference
+    program's noisy run (golden case: 64^2, --axx 0.005 --seed 11) within the FP64
+    path's bar, and the pure mode follows the oracle's pure mode."""
+    d, meta, fields = golden_case("misfit_64_noise")
+    r = gpu_run(P.MODEL_MISFIT, 64, 64, precision=P.FP64, seed=11, axx=float(np.float32(0.005)))
+    for kd in (3, 6):
+        r.advance(3)
+        phi, con = r.fields_f32()
+        err = max(np.abs(phi - fields[f"phi_{kd}"]).max(), np.abs(con - fields[f"con_{kd}"]).max())
+        print(f"FP64 path with noise, step {kd}: {err:.3e} from the reference run")
+        assert err <= 1e-6
+    a = gpu_run(P.MODEL_MISFIT, 64, 64, precision=P.FP64_PURE, seed=11, axx=0.005)
+    o = oracle_run(P.MODEL_MISFIT, 64, 64, exact=0, seed=11, axx=0.005)
+    a.advance(6)
+    o.step(6)
+    assert np.abs(a.fields()[0] - o.fields()[0]).max() <= 1e-11
+    # the noise moved the fields: the same run without it differs
+    q = gpu_run(P.MODEL_MISFIT, 64, 64, precision=P.FP64, seed=11)
+    q.advance(6)
+    assert np.abs(q.fields_f32()[0] - fields["phi_6"]).max() > 1e-4
