@@ -617,23 +617,38 @@ def run_ours(args):
                                            "algorithmic_bytes_per_step": fp64_bytes},
                               "batched_over_fp64_plain": round(value / dist.world / fp64_sps, 2),
                               "fp32_path_over_fp64_plain": round(line["fp32_path"]["run_steps_per_s"] / fp64_sps, 2)}
-    # the 3-D CVD workload (256 x 256 x 64)
+    # the 3-D CVD workload (256 x 256 x 64): the mixed path (four sweeps per step: row
+    # kernel along n, m-axis pass, column kernel along l, inverse m-axis pass) and the
+    # plain FP64 path
     if not args.no_cvd3d:
-        r3 = P.Run(P.default_params(P.MODEL_CVD, L=256, M=256, N=64, device=dev, precision=P.FP64))
-        r3.advance(2)
-        n3 = 10
-        ms3 = r3.advance_timed(n3)
-        t0 = time.perf_counter()
-        for _ in range(3):  # the CLI's per-step pattern: one step, then ENERGYC2 for energy.txt
-            r3.advance(1)
-            r3.energy()
-        cli_ms = (time.perf_counter() - t0) / 3 * 1e3
-        r3.close()
-        line["cvd3d"] = {"workload": "CVD 256x256x64 (u0 0.01, con0 0.2, dt 0.05, dx 0.125), plain FP64 path",
-                         "ms_per_step": round(ms3 / n3, 4), "steps_per_s": round(n3 / (ms3 / 1000.0), 2),
-                         "cli_step_with_energy_ms": round(cli_ms, 3),
-                         "what": "pfc_run_advance_timed (CUDA events) of 10 steps; cli_step_with_energy_ms is wall "
-                                 "time of advance(1) + pfc_run_energy"}
+        L3, M3, N3 = 256, 256, 64
+        out3 = {"workload": f"CVD {L3}x{M3}x{N3} (u0 0.01, con0 0.2, dt 0.05, dx 0.125)"}
+        for name, prec in (("mixed", P.MIXED), ("fp64_plain", P.FP64)):
+            r3 = P.Run(P.default_params(P.MODEL_CVD, L=L3, M=M3, N=N3, device=dev, precision=prec))
+            r3.advance(2)
+            n3 = 50 if prec == P.MIXED else 10
+            ms3 = r3.advance_timed(n3)
+            t0 = time.perf_counter()
+            for _ in range(3):  # the CLI's per-step pattern: one step with ENERGYC2 for energy.txt
+                r3.advance(1, analysis=True)
+                r3.energy()
+            cli_ms = (time.perf_counter() - t0) / 3 * 1e3
+            r3.close()
+            entry = {"ms_per_step": round(ms3 / n3, 4), "steps_per_s": round(n3 / (ms3 / 1000.0), 2),
+                     "cli_step_with_energy_ms": round(cli_ms, 3)}
+            if prec == P.MIXED:
+                # 30 array passes per step (row 4 + 2, m-pass 4 + 4, column 4 + 4, inverse m-pass
+                # 4 + 4) over L*M*Hp complex floats, Hp = N/2 + 1 rounded up to the tile width 8
+                hp = (N3 // 2 + 1 + 7) // 8 * 8
+                by3 = 30 * L3 * M3 * hp * 8
+                ach3 = by3 / (ms3 / n3 / 1000.0) / 1e9
+                entry["roofline"] = {"bound": "hbm", "achieved": round(ach3, 1), "frac": round(ach3 / peak, 4),
+                                     "algorithmic_bytes_per_step": by3}
+            out3[name] = entry
+        out3["mixed_over_fp64_plain"] = round(out3["fp64_plain"]["ms_per_step"] / out3["mixed"]["ms_per_step"], 2)
+        out3["what"] = ("pfc_run_advance_timed (CUDA events) of the steps; cli_step_with_energy_ms is wall time of "
+                        "advance(1, analysis) + pfc_run_energy")
+        line["cvd3d"] = out3
     if not args.no_elastic:
         line["elastic"] = elastic_bench(P, dev, G)
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:

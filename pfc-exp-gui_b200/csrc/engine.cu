@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <initializer_list>
 #include <map>
 #include <tuple>
 #include <mutex>
@@ -261,7 +262,8 @@ static C2ParamsD c2_params_pure(float sig, float g1, float g2, float k1, float k
 static int acquire_kcoef(pfc_run *r) {
     std::lock_guard<std::mutex> lk(g_kcoef_mu);
     KcoefEntry &e = g_kcoef[kcoef_key(r)];
-    const size_t npts = (size_t)r->desc.T * r->L * r->desc.CT;
+    // points of the table: the 2-D row space, or the 3-D column view's layout B
+    const size_t npts = r->d3 ? (size_t)r->desc_col.T * r->L * r->desc.CT : (size_t)r->desc.T * r->L * r->desc.CT;
     const bool mixed = r->p.precision == PFC_PRECISION_MIXED;
     if (!e.ptr) {
         const size_t bytes = npts * kcoef_point_bytes(r->p.precision);
@@ -274,9 +276,14 @@ static int acquire_kcoef(pfc_run *r) {
             const ModelCoefs &k = r->k;
             const C2ParamsD ca = c2_params_pure(r->p.sig, k.gaa1, k.gaa2, k.ka1, k.ka2, k.sigMa1, k.sigMa2);
             const C2ParamsD cb = c2_params_pure(r->p.sig, k.gab1, k.gab2, k.kb1, k.kb2, k.sigMb1, k.sigMb2);
-            ce = launch_build_kmix(r->d_desc, (double)k.dynamic_mn * (double)r->p.dt,
-                                   (double)k.dynamic_mc * (double)r->p.dt, (double)k.para_alpha, ca, cb,
-                                   (double4 *)e.ptr, (double2 *)((double4 *)e.ptr + npts), r->stream);
+            if (r->d3)
+                ce = launch_build_kmix3(r->d_desc_col, (double)k.dynamic_mn * (double)r->p.dt,
+                                        (double)k.dynamic_mc * (double)r->p.dt, (double)k.para_alpha, ca, cb,
+                                        (double4 *)e.ptr, (double2 *)((double4 *)e.ptr + npts), r->stream);
+            else
+                ce = launch_build_kmix(r->d_desc, (double)k.dynamic_mn * (double)r->p.dt,
+                                       (double)k.dynamic_mc * (double)r->p.dt, (double)k.para_alpha, ca, cb,
+                                       (double4 *)e.ptr, (double2 *)((double4 *)e.ptr + npts), r->stream);
         } else {
             ce = launch_build_kcoef(r->d_desc, (float2 *)e.ptr, (float2 *)e.ptr + npts, r->stream);
         }
@@ -289,8 +296,9 @@ static int acquire_kcoef(pfc_run *r) {
     }
     e.refs++;
     if (mixed) {
-        r->desc.kmix = (const double4 *)e.ptr;
-        r->desc.kc2d = (const double2 *)((const double4 *)e.ptr + npts);
+        RunDesc &t = r->d3 ? r->desc_col : r->desc;
+        t.kmix = (const double4 *)e.ptr;
+        t.kc2d = (const double2 *)((const double4 *)e.ptr + npts);
     } else {
         r->desc.kden = (const float2 *)e.ptr;
         r->desc.kc2 = (const float2 *)e.ptr + npts;
@@ -352,15 +360,30 @@ bool fused_path(int prec) { return prec == PFC_PRECISION_FP32 || prec == PFC_PRE
 // path) + partials + result slots + descriptor.
 static size_t run_state_bytes(int L, int M, int N, int prec, int ct) {
     const bool fused = fused_path(prec);
-    const int Hp = round_up(M / 2 + 1, ct);
-    const size_t rs = (size_t)L * Hp * sizeof(float2);
+    const bool d3 = fused && N > 1;  // 3-D: 8 arrays in layout A and 8 in layout B
+    const int Hp = d3 ? round_up(N / 2 + 1, ct) : round_up(M / 2 + 1, ct);
+    const size_t rs = (size_t)(d3 ? (size_t)L * M : (size_t)L) * Hp * sizeof(float2);
     const size_t real = (size_t)L * M * N * sizeof(float);
     const size_t ktab = (size_t)(L + M + N + 1) * sizeof(float);  // k-vectors + the step counter
-    const size_t kdtab = prec == PFC_PRECISION_MIXED ? (size_t)(L + M) * sizeof(double) : 0;
-    const int parts_n = fused ? analysis_partials(L, M, prec) : analysis_partials(L, M, PFC_PRECISION_FP32);
+    const size_t kdtab = prec == PFC_PRECISION_MIXED ? (size_t)(L + M + N) * sizeof(double) : 0;
+    const int parts_n = !fused ? analysis_partials(L, M, PFC_PRECISION_FP32)
+                               : (d3 ? analysis_partials(L * M, N, prec) : analysis_partials(L, M, prec));
     const size_t parts = (size_t)(2 * parts_n + 4096) * sizeof(double);
-    return (fused ? 8 * rs : 0) + 2 * real + round_up((int)ktab, 256) + round_up((int)kdtab, 256) + parts +
-           sizeof(RunDesc) + 1024;
+    return (fused ? (d3 ? 16 : 8) * rs : 0) + 2 * real + round_up((int)ktab, 256) + round_up((int)kdtab, 256) + parts +
+           2 * sizeof(RunDesc) + 1024;
+}
+
+// Column tile width of a 3-D mixed run: the widest up to the 2-D default whose column
+// tile (L x CT) and m-pass tile (M x CT) fit the kernels' shared memory; 0 if none.
+static int tile_width_3d(int L, int M) {
+    for (int c = mixed_col_tile_width(L); c >= 1; c /= 2) {
+        int cand[4];
+        const int n = mixed_col_tile_candidates(L, cand);
+        bool ok = false;
+        for (int i = 0; i < n; ++i) ok = ok || cand[i] == c;
+        if (ok && M * c <= 4096) return c;
+    }
+    return 0;
 }
 
 // Column tile widths of a precision's fused kernels (default and autotuner candidates).
@@ -382,13 +405,17 @@ extern "C" int pfc_run_bytes(const pfc_run_params *p, double *bytes) {
     if (!is_supported_len(p->L) || !is_supported_len(p->M) || p->N < 1)
         return set_error(PFC_E_INVALID, "unsupported grid");
     const bool fused = fused_path(p->precision);
+    const bool d3 = fused && p->N > 1;
     // the widest tile the autotuner may choose (the most padding)
     int cand[4];
     const int nc = tile_candidates(p->L, p->precision, cand);
-    const int ct = nc ? cand[nc - 1] : tile_default(p->L, p->precision);
+    int ct = nc ? cand[nc - 1] : tile_default(p->L, p->precision);
+    if (d3) ct = tile_width_3d(p->L, p->M);
+    if (d3 && ct == 0) return set_error(PFC_E_INVALID, "unsupported 3-D grid");
     double b = (double)run_state_bytes(p->L, p->M, p->N, p->precision, ct);
     const double P = (double)p->L * p->M * p->N;
-    if (fused) b += (double)p->L * round_up(p->M / 2 + 1, ct) * kcoef_point_bytes(p->precision);
+    if (d3) b += (double)p->L * p->M * round_up(p->N / 2 + 1, ct) * kcoef_point_bytes(p->precision);
+    else if (fused) b += (double)p->L * round_up(p->M / 2 + 1, ct) * kcoef_point_bytes(p->precision);
     else b += P * (22.0 * 16.0 + 6.0 * 8.0);
     *bytes = b;
     return PFC_OK;
@@ -464,10 +491,14 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
         p->precision != PFC_PRECISION_FP64_PURE && p->precision != PFC_PRECISION_MIXED)
         return set_error(PFC_E_INVALID, "unknown precision");
     const bool fused = fused_path(p->precision);
-    if (p->N != 1 && fused)
-        return set_error(PFC_E_INVALID,
-                         "the fused (mixed, FP32) paths take 2-D grids (N = 1); use an FP64 precision for 3-D");
+    const bool d3 = fused && p->N != 1;
+    if (d3 && p->precision != PFC_PRECISION_MIXED)
+        return set_error(PFC_E_INVALID, "the FP32 path takes 2-D grids (N = 1); 3-D runs use the mixed or FP64 precisions");
     if (p->N != 1 && p->model == PFC_MODEL_MISFIT) return set_error(PFC_E_INVALID, "Misfit runs are 2-D (N = 1)");
+    if (d3 && !mixed_row_len_ok(p->N))
+        return set_error(PFC_E_INVALID, "3-D mixed-precision runs take N a power of two in [8, 2048]");
+    if (d3 && tile_width_3d(p->L, p->M) == 0)
+        return set_error(PFC_E_INVALID, "3-D grid not supported by the mixed kernels (L * M too unbalanced); use fp64");
     if (!(p->dt > 0.0f) || !(p->dx > 0.0f)) return set_error(PFC_E_INVALID, "dt and dx must be > 0");
     if (p->model == PFC_MODEL_MISFIT &&
         (p->grainx <= 0 || p->grainy <= 0 || p->grainz <= 0 || p->grainx > p->L || p->grainy > p->M || p->grainz > p->N))
@@ -478,7 +509,10 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
     if (rc != PFC_OK) return rc;
     PFC_CUDA_TRY(cudaSetDevice(p->device));
     int ct = tile_default(p->L, p->precision), stage = COL_STAGE_BULK;
-    if (fused) {
+    if (d3) {
+        ct = tile_width_3d(p->L, p->M);
+        stage = COL_STAGE_ASYNC;
+    } else if (fused) {
         if (ct_force > 0) {
             ct = ct_force;
             stage = stage_force;
@@ -496,7 +530,10 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
     r->M = p->M;
     r->N = p->N;
     r->P = (long)p->L * p->M * p->N;
-    r->Hp = round_up(p->M / 2 + 1, ct);
+    r->d3 = d3;
+    r->Hp = d3 ? round_up(p->N / 2 + 1, ct) : round_up(p->M / 2 + 1, ct);
+    r->rows = d3 ? p->L * p->M : p->L;
+    r->rowlen = d3 ? p->N : p->M;
     model_coefs(p->model, &r->k);
     const ModelCoefs &k = r->k;
     r->c2a = c2_params(p->sig, k.gaa1, k.gaa2, k.ka1, k.ka2, k.sigMa1, k.sigMa2);
@@ -508,13 +545,13 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
                                                               : 0.0f;
 
     // device memory: 8 row-space arrays + 2 real fields + k tables + partials + result
-    const size_t rs = (size_t)r->L * r->Hp * sizeof(float2);
+    const size_t rs = (size_t)r->rows * r->Hp * sizeof(float2);
     const size_t real = (size_t)r->P * sizeof(float);
-    const int nparts = fused ? analysis_partials(r->L, r->M, p->precision)
+    const int nparts = fused ? analysis_partials(r->rows, r->rowlen, p->precision)
                              : analysis_partials(r->L, r->M, PFC_PRECISION_FP32);
     r->nparts = nparts;
     const size_t ktab = (size_t)(r->L + r->M + r->N + 1) * sizeof(float);
-    const size_t kdtab = p->precision == PFC_PRECISION_MIXED ? (size_t)(r->L + r->M) * sizeof(double) : 0;
+    const size_t kdtab = p->precision == PFC_PRECISION_MIXED ? (size_t)(r->L + r->M + r->N) * sizeof(double) : 0;
     const size_t parts = (size_t)(2 * nparts + 4096) * sizeof(double);
     const size_t bytes = run_state_bytes(r->L, r->M, r->N, p->precision, ct);
     cudaError_t e = cudaMalloc(&r->dev_mem, bytes);
@@ -526,11 +563,20 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
     char *m = (char *)r->dev_mem;
     RunDesc &d = r->desc;
     std::memset(&d, 0, sizeof(d));
+    RunDesc &dc = r->desc_col;
+    std::memset(&dc, 0, sizeof(dc));
     if (fused) {
         float2 **arrs[8] = {&d.psi, &d.con, &d.ca, &d.cb, &d.inn, &d.inc, &d.gx, &d.gy};
         for (int i = 0; i < 8; ++i) {
             *arrs[i] = (float2 *)m;
             m += rs;
+        }
+        if (d3) {  // the layout-B arrays of the column view
+            float2 **b[8] = {&dc.psi, &dc.con, &dc.ca, &dc.cb, &dc.inn, &dc.inc, &dc.gx, &dc.gy};
+            for (int i = 0; i < 8; ++i) {
+                *b[i] = (float2 *)m;
+                m += rs;
+            }
         }
     }
     d.psi_real = (float *)m;
@@ -547,27 +593,32 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
         // pure-FP64 k-vectors (the oracle's pure mode of MIS:455-462)
         double *kd = (double *)m;
         m += round_up((int)kdtab, 256);
-        std::vector<double> h(r->L + r->M);
+        std::vector<double> h(r->L + r->M + r->N);
         for (int l = 0; l < r->L; ++l)
             h[l] = (double)(l <= r->L / 2 ? l : l - r->L) * 2.0 * PI_REF / ((double)r->L * p->dx);
         for (int mm = 0; mm < r->M; ++mm)
             h[r->L + mm] = (double)(mm <= r->M / 2 ? mm : mm - r->M) * 2.0 * PI_REF / ((double)r->M * p->dx);
+        for (int n = 0; n < r->N; ++n)
+            h[r->L + r->M + n] = (double)(n <= r->N / 2 ? n : n - r->N) * 2.0 * PI_REF / ((double)r->N * p->dx);
         r->kd_host = h;
         cudaMemcpyAsync(kd, r->kd_host.data(), kdtab, cudaMemcpyHostToDevice, r->stream);
         d.kdl = kd;
         d.kdm = kd + r->L;
+        d.kdn = kd + r->L + r->M;
     }
     d.partials = (double *)m;
     r->d_scratch = (double *)m + 2 * nparts;
     m += parts;
     r->d_desc = (RunDesc *)m;
+    r->d_desc_col = r->d_desc + 1;
     cudaMemcpyAsync(kt, r->krefl.data(), r->L * sizeof(float), cudaMemcpyHostToDevice, r->stream);
     cudaMemcpyAsync(kt + r->L, r->krefm.data(), r->M * sizeof(float), cudaMemcpyHostToDevice, r->stream);
     cudaMemcpyAsync(kt + r->L + r->M, r->krefn.data(), r->N * sizeof(float), cudaMemcpyHostToDevice, r->stream);
-    d.L = r->L;
-    d.M = r->M;
-    d.N = r->N;
+    d.L = r->rows;  // the row view: L rows of M in 2-D, L*M rows of N in 3-D
+    d.M = r->rowlen;
+    d.N = d3 ? 1 : r->N;
     d.Hp = r->Hp;
+    d.col_scale = 1.0 / (double)r->L;
     d.CT = ct;
     d.stage = stage;
     d.lct = 0;
@@ -595,8 +646,29 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
             return cuda_error(ce, "run status word");
         }
     }
+    if (d3) {
+        // the column view: layout-B arrays, (n-tile, km) tiles of L rows, 1/(L*M) scaling
+        const RunDesc keep = dc;  // its layout-B array pointers
+        dc = d;
+        dc.psi = keep.psi;
+        dc.con = keep.con;
+        dc.ca = keep.ca;
+        dc.cb = keep.cb;
+        dc.inn = keep.inn;
+        dc.inc = keep.inc;
+        dc.gx = keep.gx;
+        dc.gy = keep.gy;
+        dc.L = r->L;
+        dc.M = r->M;
+        dc.N = r->N;
+        dc.T = (r->Hp / ct) * r->M;
+        dc.col3d = 1;
+        dc.col_scale = 1.0 / ((double)r->L * (double)r->M);
+    }
     if (fused) {
         cudaError_t ce = cudaMemcpyAsync(r->d_desc, &d, sizeof(RunDesc), cudaMemcpyHostToDevice, r->stream);
+        if (ce == cudaSuccess && d3)
+            ce = cudaMemcpyAsync(r->d_desc_col, &dc, sizeof(RunDesc), cudaMemcpyHostToDevice, r->stream);
         if (ce != cudaSuccess) {
             free_run(r);
             return cuda_error(ce, "descriptor upload");
@@ -956,6 +1028,26 @@ static int init_real_fields(pfc_run *r) {
     return PFC_OK;
 }
 
+// m-pass arguments of a 3-D run for the arrays `which` (0 psi, 1 con, 2 c2a, 3 c2b, 4 inn,
+// 5 inc, 6 gx, 7 gy): forward reads layout A (the row view's arrays) and writes layout B
+// (the column view's), inverse the other way.
+static MPassArgs mpass_args(const pfc_run *r, std::initializer_list<int> which, bool forward) {
+    const RunDesc &a = r->desc, &b = r->desc_col;
+    float2 *A[8] = {a.psi, a.con, a.ca, a.cb, a.inn, a.inc, a.gx, a.gy};
+    float2 *B[8] = {b.psi, b.con, b.ca, b.cb, b.inn, b.inc, b.gx, b.gy};
+    MPassArgs m{};
+    for (int w : which) {
+        m.src[m.narr] = forward ? A[w] : B[w];
+        m.dst[m.narr] = forward ? B[w] : A[w];
+        ++m.narr;
+    }
+    m.L = r->L;
+    m.M = r->M;
+    m.Tn = r->Hp / r->desc.CT;
+    m.CT = r->desc.CT;
+    return m;
+}
+
 // Means of the real fields (FP64), then row space and the c2a/c2b arrays.
 static int fp32_from_real(pfc_run *r, bool means_from_device) {
     RunDesc &d = r->desc;
@@ -978,9 +1070,23 @@ static int fp32_from_real(pfc_run *r, bool means_from_device) {
     r->step_ctr_init = r->t - 1;
     PFC_CUDA_TRY(cudaMemcpyAsync(d.step_ctr, &r->step_ctr_init, sizeof(int), cudaMemcpyHostToDevice, r->stream));
     const int prec = r->p.precision;
-    PFC_CUDA_TRY(launch_row_forward(r->d_desc, 1, r->L, r->M, prec, r->ctx->tw, r->stream));
-    PFC_CUDA_TRY(launch_col_step(r->d_desc, 1, r->L, r->M, r->desc.CT, r->desc.stage, COL_PREPARE, prec, r->ctx->tw,
-                                 r->stream));
+    PFC_CUDA_TRY(launch_row_forward(r->d_desc, 1, r->rows, r->rowlen, prec, r->ctx->tw, r->stream));
+    if (r->d3) {
+        RunDesc &dc = r->desc_col;
+        dc.psi_mean = d.psi_mean;
+        dc.con_mean = d.con_mean;
+        dc.psi_mean_f = d.psi_mean_f;
+        dc.con_mean_f = d.con_mean_f;
+        PFC_CUDA_TRY(cudaMemcpyAsync(r->d_desc_col, &dc, sizeof(RunDesc), cudaMemcpyHostToDevice, r->stream));
+        // psi to layout B, c2a / c2b from it (the column kernel's set-up mode), back to layout A
+        PFC_CUDA_TRY(launch_mpass(mpass_args(r, {0}, true), true, r->ctx->tw, r->stream));
+        PFC_CUDA_TRY(launch_col_step_mixed_tiles(r->d_desc_col, 1, r->L, dc.T, dc.CT, dc.stage, COL_PREPARE,
+                                                 r->ctx->tw, r->stream));
+        PFC_CUDA_TRY(launch_mpass(mpass_args(r, {2, 3}, false), false, r->ctx->tw, r->stream));
+    } else {
+        PFC_CUDA_TRY(launch_col_step(r->d_desc, 1, r->L, r->M, r->desc.CT, r->desc.stage, COL_PREPARE, prec,
+                                     r->ctx->tw, r->stream));
+    }
     PFC_SYNC_CHECKED(r->ctx, r->stream);
     r->fields_valid = true;
     r->energy_valid = false;
@@ -1008,16 +1114,26 @@ static int fused_advance(pfc_run *r, int nsteps, int analysis) {
     const int prec = r->p.precision;
     for (int i = 0; i < nsteps; ++i) {
         const bool last = i == nsteps - 1;
-        PFC_CUDA_TRY(launch_row_step(r->d_desc, 1, r->L, r->M, prec, r->ctx->tw, r->stream));
-        PFC_CUDA_TRY(launch_col_step(r->d_desc, 1, r->L, r->M, r->desc.CT, r->desc.stage,
-                                     (last && analysis) ? COL_STEP_CHECKPOINT : COL_STEP, prec, r->ctx->tw,
-                                     r->stream));
+        const int mode = (last && analysis) ? COL_STEP_CHECKPOINT : COL_STEP;
+        PFC_CUDA_TRY(launch_row_step(r->d_desc, 1, r->rows, r->rowlen, prec, r->ctx->tw, r->stream));
+        if (r->d3) {
+            const RunDesc &dc = r->desc_col;
+            PFC_CUDA_TRY(launch_mpass(mpass_args(r, {0, 1, 4, 5}, true), true, r->ctx->tw, r->stream));
+            PFC_CUDA_TRY(launch_col_step_mixed_tiles(r->d_desc_col, 1, r->L, dc.T, dc.CT, dc.stage, mode,
+                                                     r->ctx->tw, r->stream));
+            PFC_CUDA_TRY(launch_mpass(mode == COL_STEP_CHECKPOINT ? mpass_args(r, {0, 1, 2, 3, 6, 7}, false)
+                                                                  : mpass_args(r, {0, 1, 2, 3}, false),
+                                      false, r->ctx->tw, r->stream));
+        } else {
+            PFC_CUDA_TRY(launch_col_step(r->d_desc, 1, r->L, r->M, r->desc.CT, r->desc.stage, mode, prec,
+                                         r->ctx->tw, r->stream));
+        }
     }
     r->t += nsteps;
     r->fields_valid = false;
     r->energy_valid = false;
     if (analysis) {
-        PFC_CUDA_TRY(launch_row_analysis(r->d_desc, 1, r->L, r->M, prec, r->ctx->tw, r->stream));
+        PFC_CUDA_TRY(launch_row_analysis(r->d_desc, 1, r->rows, r->rowlen, prec, r->ctx->tw, r->stream));
         PFC_CUDA_TRY(launch_reduce_fixed(r->desc.partials, r->nparts, 2, 2, r->d_scratch, r->stream));
         r->fields_valid = true;
         r->energy_valid = true;
@@ -1063,7 +1179,7 @@ extern "C" int pfc_run_steps(const pfc_run *r, int *steps) {
 static int materialize(pfc_run *r) {
     if (!fused_path(r->p.precision)) return fp64_materialize(r);
     if (r->fields_valid) return PFC_OK;
-    PFC_CUDA_TRY(launch_row_analysis(r->d_desc, 1, r->L, r->M, r->p.precision, r->ctx->tw, r->stream));
+    PFC_CUDA_TRY(launch_row_analysis(r->d_desc, 1, r->rows, r->rowlen, r->p.precision, r->ctx->tw, r->stream));
     r->fields_valid = true;
     return PFC_OK;
 }
@@ -1243,8 +1359,8 @@ extern "C" int pfc_batch_create(pfc_run *const *runs, int nruns, pfc_batch **out
     const int dev = runs[0]->p.device;
     for (int i = 0; i < nruns; ++i) {
         if (!runs[i]) return set_error(PFC_E_INVALID, "null run in batch");
-        if (!fused_path(runs[i]->p.precision))
-            return set_error(PFC_E_INVALID, "batches hold fused-path (mixed, FP32) runs only");
+        if (!fused_path(runs[i]->p.precision) || runs[i]->d3)
+            return set_error(PFC_E_INVALID, "batches hold 2-D fused-path (mixed, FP32) runs only");
         if (runs[i]->p.device != dev) return set_error(PFC_E_INVALID, "batch runs must share one device");
     }
     PFC_CUDA_TRY(cudaSetDevice(dev));

@@ -2,16 +2,16 @@
 // HBM, FP64 arithmetic), and its launchers.
 //
 // Instantiated one row length L per translation unit (col_inst.cu compiled with
-// PFC_COL_L = L); step_mixed.cu reaches it through launch_col_mixed_L<L>.
+// PFC_COL_L = L); step_mixed.cu reaches it through launch_col_mixed_L<L>, whose `tiles`
+// is the number of column tiles per run (T of the runs' descriptors).
 #pragma once
 
 #include "step_common.cuh"
 
 namespace pfc {
 
-// Column tile of the mixed path: L rows x C packed columns, 512 <= C*L <= 4096 complex
-// values (two padded double2 buffers and an FP32 staging buffer: 43 KB to 172 KB).
-constexpr bool mcol_tile_ok(int L, int C) { return C >= 1 && C <= COL_TILE_MAX && C * L >= 512 && C * L <= 4096; }
+// Column tile of the mixed path (mcol_tile_ok, step_common.cuh): two padded double2
+// buffers and an FP32 staging buffer, 43 KB to 172 KB.
 template <int L, int C> struct MColCfg {
     static constexpr int NT = (C * L / 16) < 32 ? 32 : (C * L / 16);
     static constexpr int SMEM = 2 * (int)sizeof(double2) * padded_len<C * L>::value + (int)sizeof(float2) * C * L;
@@ -35,13 +35,15 @@ struct ScaleByTableD {
         return make_double2(v.x * g, v.y * g);
     }
 };
-// -i k P along l (which = 0) or m (which = 1), double k-vectors
+// -i k P along l (which = 0) or m (which = 1), double k-vectors.  A 2-D tile's columns
+// are km = km0 + b (0 past M/2: padding); a 3-D column view's tile has one km (km3, all M
+// values occur, signed through kdm) and its columns are kn.
 struct GradientOfD {
     const double *kdl, *kdm;
-    int km0, H, which;
+    int km0, H, which, km3;
     __device__ __forceinline__ double2 operator()(int e, int b, double2 v) const {
-        const int km = km0 + b;
-        const double kv = which == 0 ? kdl[e] : kdm[km <= H ? km : 0];
+        const int km = km3 >= 0 ? km3 : (km0 + b <= H ? km0 + b : 0);
+        const double kv = which == 0 ? kdl[e] : kdm[km];
         return make_double2(kv * v.y, -kv * v.x);
     }
 };
@@ -89,7 +91,9 @@ __global__ void __launch_bounds__(MColCfg<L, C>::NT, MColCfg<L, C>::MINB)
         const RunDesc &d = runs[run_of(item)];
         const int H = d.M / 2;
         const long tile = tile_of(item);
-        const int km0 = (item / nruns) * C;
+        const int tile_i = item / nruns;
+        const int km0 = tile_i * C;                      // 2-D: first column's km
+        const int km3 = d.col3d ? tile_i % d.M : -1;     // 3-D column view: the tile's km
         const float2 *next_psi = item + 1 < end ? runs[run_of(item + 1)].psi + tile_of(item + 1) : nullptr;
         // barrier phase of this item's first wait: an item of the step modes waits four
         // times (phases 0, 1, 0, 1), a COL_PREPARE item once (the iteration's parity)
@@ -126,8 +130,9 @@ __global__ void __launch_bounds__(MColCfg<L, C>::NT, MColCfg<L, C>::MINB)
                 }
                 v = make_double2(rx, ry);
             } else {
-                const int l = e / C, km = km0 + e % C;
-                v = (l == 0 && km == 0) ? make_double2(0.0, 0.0) : cscale(v, 1.0 / (double)L);
+                // k = 0 is row 0 of column 0 of tile 0, in 2-D and in the 3-D column view
+                const bool k0 = e / C == 0 && tile_i == 0 && e % C == 0;
+                v = k0 ? make_double2(0.0, 0.0) : cscale(v, d.col_scale);
             }
             Pk[pi] = v;
         }
@@ -159,9 +164,9 @@ __global__ void __launch_bounds__(MColCfg<L, C>::NT, MColCfg<L, C>::MINB)
         fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b);
         tile_out_d<L, C, NT>(s, d.con + tile);
         if (MODE == COL_STEP_CHECKPOINT) {
-            fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, GradientOfD{d.kdl, d.kdm, km0, H, 0});
+            fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, GradientOfD{d.kdl, d.kdm, km0, H, 0, km3});
             tile_out_d<L, C, NT>(s, d.gx + tile);
-            fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, GradientOfD{d.kdl, d.kdm, km0, H, 1});
+            fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, GradientOfD{d.kdl, d.kdm, km0, H, 1, km3});
             tile_out_d<L, C, NT>(s, d.gy + tile);
         }
     }
@@ -169,14 +174,13 @@ __global__ void __launch_bounds__(MColCfg<L, C>::NT, MColCfg<L, C>::MINB)
 }
 
 template <int L, int C, int MODE, int STAGE>
-static cudaError_t mcol_impl(const RunDesc *d_runs, int nruns, int M, const TwiddleSet &tw, cudaStream_t st) {
+static cudaError_t mcol_impl(const RunDesc *d_runs, int nruns, int tiles, const TwiddleSet &tw, cudaStream_t st) {
     constexpr int NT = MColCfg<L, C>::NT;
     constexpr size_t smem = MColCfg<L, C>::SMEM;
     static unsigned mask = 0;
     cudaError_t e = set_smem(k_mcol_step<L, C, MODE, STAGE>, smem, mask);
     if (nruns == 0 || e != cudaSuccess) return e;
-    const int H = M / 2;
-    const int items = ((H + 1 + C - 1) / C) * nruns;
+    const int items = tiles * nruns;
     const int cap = MColCfg<L, C>::MINB * sm_count();
     const int g0 = items < cap ? items : cap;
     const int per = (items + g0 - 1) / g0;
@@ -186,42 +190,42 @@ static cudaError_t mcol_impl(const RunDesc *d_runs, int nruns, int M, const Twid
 }
 
 template <int L, int C, int STAGE>
-static cudaError_t mcol_modes(const RunDesc *d_runs, int nruns, int M, int mode, const TwiddleSet &tw,
+static cudaError_t mcol_modes(const RunDesc *d_runs, int nruns, int tiles, int mode, const TwiddleSet &tw,
                               cudaStream_t s) {
     switch (mode) {
-        case COL_STEP: return mcol_impl<L, C, COL_STEP, STAGE>(d_runs, nruns, M, tw, s);
-        case COL_PREPARE: return mcol_impl<L, C, COL_PREPARE, STAGE>(d_runs, nruns, M, tw, s);
-        case COL_STEP_CHECKPOINT: return mcol_impl<L, C, COL_STEP_CHECKPOINT, STAGE>(d_runs, nruns, M, tw, s);
+        case COL_STEP: return mcol_impl<L, C, COL_STEP, STAGE>(d_runs, nruns, tiles, tw, s);
+        case COL_PREPARE: return mcol_impl<L, C, COL_PREPARE, STAGE>(d_runs, nruns, tiles, tw, s);
+        case COL_STEP_CHECKPOINT: return mcol_impl<L, C, COL_STEP_CHECKPOINT, STAGE>(d_runs, nruns, tiles, tw, s);
         default: return cudaErrorInvalidValue;
     }
 }
 template <int L, int C>
-static cudaError_t mcol_stages(const RunDesc *d_runs, int nruns, int M, int stage, int mode, const TwiddleSet &tw,
+static cudaError_t mcol_stages(const RunDesc *d_runs, int nruns, int tiles, int stage, int mode, const TwiddleSet &tw,
                                cudaStream_t s) {
     switch (stage) {
-        case STAGE_ASYNC: return mcol_modes<L, C, STAGE_ASYNC>(d_runs, nruns, M, mode, tw, s);
-        case STAGE_BULK: return mcol_modes<L, C, STAGE_BULK>(d_runs, nruns, M, mode, tw, s);
+        case STAGE_ASYNC: return mcol_modes<L, C, STAGE_ASYNC>(d_runs, nruns, tiles, mode, tw, s);
+        case STAGE_BULK: return mcol_modes<L, C, STAGE_BULK>(d_runs, nruns, tiles, mode, tw, s);
         default: return cudaErrorInvalidValue;
     }
 }
 template <int L>
-static cudaError_t mcol_dispatch(const RunDesc *d_runs, int nruns, int M, int C, int stage, int mode,
+static cudaError_t mcol_dispatch(const RunDesc *d_runs, int nruns, int tiles, int C, int stage, int mode,
                                  const TwiddleSet &tw, cudaStream_t s) {
     switch (C) {
         case 1:
-            if constexpr (mcol_tile_ok(L, 1)) return mcol_stages<L, 1>(d_runs, nruns, M, stage, mode, tw, s);
+            if constexpr (mcol_tile_ok(L, 1)) return mcol_stages<L, 1>(d_runs, nruns, tiles, stage, mode, tw, s);
             break;
         case 2:
-            if constexpr (mcol_tile_ok(L, 2)) return mcol_stages<L, 2>(d_runs, nruns, M, stage, mode, tw, s);
+            if constexpr (mcol_tile_ok(L, 2)) return mcol_stages<L, 2>(d_runs, nruns, tiles, stage, mode, tw, s);
             break;
         case 4:
-            if constexpr (mcol_tile_ok(L, 4)) return mcol_stages<L, 4>(d_runs, nruns, M, stage, mode, tw, s);
+            if constexpr (mcol_tile_ok(L, 4)) return mcol_stages<L, 4>(d_runs, nruns, tiles, stage, mode, tw, s);
             break;
         case 8:
-            if constexpr (mcol_tile_ok(L, 8)) return mcol_stages<L, 8>(d_runs, nruns, M, stage, mode, tw, s);
+            if constexpr (mcol_tile_ok(L, 8)) return mcol_stages<L, 8>(d_runs, nruns, tiles, stage, mode, tw, s);
             break;
         case 16:
-            if constexpr (mcol_tile_ok(L, 16)) return mcol_stages<L, 16>(d_runs, nruns, M, stage, mode, tw, s);
+            if constexpr (mcol_tile_ok(L, 16)) return mcol_stages<L, 16>(d_runs, nruns, tiles, stage, mode, tw, s);
             break;
         default: break;
     }
@@ -229,9 +233,9 @@ static cudaError_t mcol_dispatch(const RunDesc *d_runs, int nruns, int M, int C,
 }
 
 template <int L>
-cudaError_t launch_col_mixed_L(const RunDesc *d_runs, int nruns, int M, int C, int stage, int mode,
+cudaError_t launch_col_mixed_L(const RunDesc *d_runs, int nruns, int tiles, int C, int stage, int mode,
                                const TwiddleSet &tw, cudaStream_t s) {
-    return mcol_dispatch<L>(d_runs, nruns, M, C, stage, mode, tw, s);
+    return mcol_dispatch<L>(d_runs, nruns, tiles, C, stage, mode, tw, s);
 }
 
 }  // namespace pfc

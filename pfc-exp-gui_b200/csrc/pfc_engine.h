@@ -79,6 +79,12 @@ struct pfc_run {
     bool energy_valid = false;
     pfc::Fp64State *f64 = nullptr;
     bool kcoef_held = false;        // holds a reference on the shared coefficient table
+    // 3-D mixed-precision runs (d3): desc / d_desc are the row view (L*M rows of length N,
+    // layout A), desc_col / d_desc_col the column view (layout B, Tn*M column tiles)
+    bool d3 = false;
+    int rows = 0, rowlen = 0;       // row view of the fused kernels: (L, M) in 2-D, (L*M, N) in 3-D
+    pfc::RunDesc desc_col{};
+    pfc::RunDesc *d_desc_col = nullptr;
     volatile int *h_nonfinite = nullptr;  // fused paths: host view of RunDesc::nonfinite (mapped pinned)
     std::vector<double> kd_host;    // mixed path: the double k-vectors (lengths L and M)
 };

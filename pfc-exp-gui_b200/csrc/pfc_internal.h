@@ -60,7 +60,12 @@ struct RunDesc {
     //   kdl, kdm: the k-vectors in double (lengths L and M)
     const double4 *kmix;
     const double2 *kc2d;
-    const double *kdl, *kdm;
+    const double *kdl, *kdm, *kdn;
+    // column view of a 3-D run (col3d = 1): the column kernel's tiles are (n-tile t, km)
+    // pairs, tile index t*M + km, each L rows x CT columns kn = t*CT + c; col_scale is the
+    // inverse-transform scale its set-up mode applies (1/L for 2-D runs, 1/(L*M) for 3-D)
+    int col3d;
+    double col_scale;
     double noise_amp_d;  // dt * b0 in double (0 = off)
     // set to 1 (device-visible, mapped pinned host memory) by a row-step kernel that met a
     // non-finite nonlinear term (NaN / Inf in the run's fields); the engine fails the run
@@ -105,8 +110,15 @@ template <int L>
 cudaError_t launch_col_f32_L(const RunDesc *d_runs, int nruns, int M, int C, int stage, int mode,
                              const TwiddleSet &tw, cudaStream_t s);
 template <int L>
-cudaError_t launch_col_mixed_L(const RunDesc *d_runs, int nruns, int M, int C, int stage, int mode,
+cudaError_t launch_col_mixed_L(const RunDesc *d_runs, int nruns, int tiles, int C, int stage, int mode,
                                const TwiddleSet &tw, cudaStream_t s);
+// The mixed column kernel over `tiles` column tiles per run (the 3-D column view: Tn*M).
+cudaError_t launch_col_step_mixed_tiles(const RunDesc *d_runs, int nruns, int L, int tiles, int C, int stage,
+                                        int mode, const TwiddleSet &tw, cudaStream_t s);
+// The mixed-precision row kernels of one row length M (instantiated per M in row_inst.cu).
+enum MRowKind : int { MROW_STEP = 0, MROW_FORWARD = 1, MROW_ANALYSIS = 2 };
+template <int M>
+cudaError_t launch_mrow_M(int kind, const RunDesc *d_runs, int nruns, int L, const TwiddleSet &tw, cudaStream_t s);
 // The FP32 and mixed-precision kernels behind them.
 cudaError_t launch_row_step_f32(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw, cudaStream_t s);
 cudaError_t launch_col_step_f32(const RunDesc *d_runs, int nruns, int L, int M, int C, int stage, int mode,
@@ -145,6 +157,30 @@ enum ColMode : int { COL_STEP = 0, COL_PREPARE = 1, COL_STEP_CHECKPOINT = 2 };
 // column-kernel tile staging: 16-byte cp.async copies, or one TMA bulk copy per tile
 // completing on an mbarrier (tile_io.cuh)
 enum ColStage : int { COL_STAGE_ASYNC = 0, COL_STAGE_BULK = 1 };
+
+// The m-axis pass of a 3-D mixed-precision run (step_3d.cu).  Its n-space arrays live in
+// two layouts of the same size, L*M*Hp complex floats with Hp = Tn*CT:
+//   A (the row kernel's): element (l, m, kn) at ((t*L + l)*M + m)*CT + c, kn = t*CT + c,
+//     so the rows of length N are the row view's L*M rows and every (t, l) is one
+//     contiguous M x CT tile;
+//   B (the column kernel's): element (l, km, kn) at ((t*M + km)*L + l)*CT + c, so every
+//     (t, km) is one contiguous L x CT column tile.
+// The forward pass transforms each (t, l) tile of an A array along m and writes it to B;
+// the inverse pass reads B, transforms back (unnormalised) and writes A.
+struct MPassArgs {
+    const float2 *src[8];
+    float2 *dst[8];
+    int narr;
+    int L, M, Tn, CT;
+};
+cudaError_t launch_mpass(const MPassArgs &a, bool forward, const TwiddleSet &tw, cudaStream_t s);
+// The 3-D mixed-precision coefficient table in layout B (RunDesc::kmix, kc2d of the column
+// view, scaled by 1/(L*M)), from the double k-vectors kdl, kdm, kdn.
+cudaError_t launch_build_kmix3(const RunDesc *d_col, double mn_dt, double mc_dt, double alpha, C2ParamsD a,
+                               C2ParamsD b, double4 *kmix, double2 *kc2d, cudaStream_t s);
+// Row lengths the mixed row kernels take: powers of two 8 ... 2048 (3-D rows of N points
+// as short as 8).
+bool mixed_row_len_ok(int n);
 
 // Self-test of the column kernel's tile staging (k_stage_selftest): n float2 (even,
 // <= 8192) staged from src by one bulk copy and written back to dst, or, without

@@ -15,6 +15,11 @@ constexpr int COL_TILE_MAX = 16;  // widest column tile (packed columns); the ro
 // Column-kernel tile: L rows x C packed columns, C a power of two in [1, COL_TILE_MAX]
 // with 512 <= C*L <= 8192 complex elements (three such buffers per CTA: 13 KB to 204 KB).
 constexpr bool col_tile_ok(int L, int C) { return C >= 1 && C <= COL_TILE_MAX && C * L >= 512 && C * L <= 8192; }
+// Column tile of the mixed-precision path: L rows x C packed columns, 512 <= C*L <= 4096
+// complex values (its shared buffers hold double2).
+constexpr bool mcol_tile_ok(int L, int C) { return C >= 1 && C <= COL_TILE_MAX && C * L >= 512 && C * L <= 4096; }
+constexpr int MROW_TILE = 2048;  // complex doubles per mixed row-kernel CTA (row step: 2 sequences per row)
+
 template <int L, int C> struct ColCfg {
     static constexpr int NT = (C * L / 16) < 32 ? 32 : (C * L / 16);
     // CTAs per SM that the shared memory leaves room for (two at C*L = 4096)

@@ -1,0 +1,108 @@
+"""GPU parity of the 3-D CVD step on the mixed-precision path.
+
+A 3-D run keeps its state as the DFT along n in FP32 complex arrays and takes four sweeps
+per step (row kernel along n, m-axis pass, column kernel along l with the update, inverse
+m-axis pass), all in FP64 arithmetic with the pure-FP64 operator (k^2 = kl^2 + km^2 + kn^2).
+
+  * against the CPU pure-FP64 oracle over 10-20 steps (CVD is chaotic beyond that): 1e-6,
+    or, where the dynamics have already amplified roundings past that, no more than the
+    reference's own float roundings move it from pure FP64 (FP64 GPU path, both modes);
+  * against the reference program's own 3-D run (golden case 32 x 32 x 8, 11 steps): the
+    reference's own float roundings separate it from pure FP64, so the bound is that
+    deviation (measured on the FP64 GPU path) plus 1e-6;
+  * energies and masses as the 2-D mixed path's tests bound them.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import pfc_b200 as P
+from helpers import golden_case
+
+pytestmark = pytest.mark.gpu
+
+
+def run3(L, M, N, precision=P.MIXED, **kw):
+    return P.Run(P.default_params(P.MODEL_CVD, L=L, M=M, N=N, precision=precision, **kw))
+
+
+def test_3d_initial_condition_matches_oracle():
+    r = run3(64, 64, 16)
+    o = O.Run(O.default_params(O.MODEL_CVD, L=64, M=64, N=16, exact=1))
+    phi, con = r.fields_f32()
+    ophi, ocon = o.fields()
+    assert np.array_equal(phi, ophi.astype(np.float32))
+    assert np.array_equal(con, ocon.astype(np.float32))
+
+
+@pytest.mark.parametrize("L,M,N,steps", [(64, 64, 16, 20), (32, 32, 8, 20), (128, 128, 64, 20), (64, 128, 32, 10)])
+def test_3d_mixed_matches_pure_fp64_oracle(L, M, N, steps):
+    r = run3(L, M, N)
+    o = O.Run(O.default_params(O.MODEL_CVD, L=L, M=M, N=N, exact=0))
+    r.advance(steps, analysis=True)
+    o.step(steps)
+    phi, con = r.fields()
+    ophi, ocon = o.fields()
+    err = max(np.abs(phi - ophi).max(), np.abs(con - ocon).max())
+    a = run3(L, M, N, precision=P.FP64)
+    a.advance(steps)
+    ref_noise = max(np.abs(a.fields()[0] - ophi).max(), np.abs(a.fields()[1] - ocon).max())
+    print(f"CVD {L}x{M}x{N}, {steps} steps: mixed vs pure FP64 {err:.3e}; reference roundings {ref_noise:.3e}")
+    assert err <= max(1e-6, ref_noise)
+    e, d = r.energy()
+    oe, od = o.energy()
+    assert abs(e - oe) <= err + 1e-9
+    assert abs(d - od) <= 1e-9 * abs(od) + 5e-9
+
+
+def test_3d_mixed_against_reference_run():
+    d, meta, fields = golden_case("cvd_32x32x8")
+    r = run3(32, 32, 8)
+    a = run3(32, 32, 8, precision=P.FP64)
+    b = run3(32, 32, 8, precision=P.FP64_PURE)
+    done = 0
+    for kd in (0, 5, 10):  # CVD checkpoint kd follows step kd + 1
+        for x in (r, a, b):
+            x.advance(kd + 1 - done, analysis=True)
+        done = kd + 1
+        phi, con = r.fields_f32()
+        ref_noise = max(np.abs(a.fields()[0] - b.fields()[0]).max(), np.abs(a.fields()[1] - b.fields()[1]).max())
+        err = max(np.abs(phi - fields[f"phi_{kd}"]).max(), np.abs(con - fields[f"con_{kd}"]).max())
+        print(f"32x32x8 checkpoint {kd}: mixed vs reference run {err:.3e}; reference vs pure FP64 {ref_noise:.3e}")
+        assert err <= ref_noise + 1e-6
+
+
+def test_3d_mass_is_conserved_and_energy_follows_fp64():
+    r = run3(64, 64, 16)
+    b = run3(64, 64, 16, precision=P.FP64_PURE)
+    m0 = r.means()
+    r.advance(100, analysis=True)
+    b.advance(100)
+    assert r.means() == m0
+    e, d = r.energy()
+    eb, db = b.energy()
+    print(f"CVD 64x64x16 step 100: e/P {e:.9e} vs FP64 {eb:.9e}")
+    assert abs(d - db) <= 1e-9
+    assert abs(e - eb) <= 5e-6
+
+
+def test_3d_set_fields_roundtrip():
+    o = O.Run(O.default_params(O.MODEL_CVD, L=32, M=32, N=8, exact=0))
+    o.step(3)
+    phi, con = o.fields()
+    r = run3(32, 32, 8)
+    r.set_fields(phi, con)
+    a, c = r.fields()
+    assert np.abs(a - phi).max() <= 1e-6 and np.abs(c - con).max() <= 1e-6
+    r.advance(10, analysis=True)
+    o.step(10)
+    assert np.abs(r.fields()[0] - o.fields()[0]).max() <= 1e-6
+
+
+def test_3d_fused_limits():
+    with pytest.raises(P.PfcError):
+        run3(64, 64, 16, precision=P.FP32)  # the FP32 path is 2-D
+    with pytest.raises(P.PfcError):
+        run3(64, 64, 4)  # rows of N >= 8
+    with pytest.raises(P.PfcError):
+        P.Batch([run3(32, 32, 8)])  # batches hold 2-D runs
