@@ -12,8 +12,8 @@
 // Files are byte-compatible with the reference writers (VTI/PVTI at
 // misfit_uniform_time_seed_fftw_early.cpp:1588-1810, text files with std::fixed and
 // precision(4)).  Additive options: --grid LxMxN (runtime grid; default 256x256x1)
-// and --precision mixed|fp32|fp64|fp64-pure (default mixed on 2-D grids: FP32 arrays,
-// FP64 arithmetic; fp64 on 3-D grids, which the fused paths do not take).  Output
+// and --precision mixed|fp32|fp64|fp64-pure (default mixed: FP32 arrays, FP64
+// arithmetic, on every 2-D grid and on 3-D grids with N >= 8; fp64 elsewhere).  Output
 // paths are prefixed with --outdir
 // instead of changing the process working directory.
 #include <algorithm>
@@ -104,6 +104,14 @@ bool parse_grid(const char *v, int &L, int &M, int &N) {
     N = c;
     return true;
 }
+// Without --precision: the mixed path wherever its kernels take the grid (2-D grids, and
+// 3-D grids with N >= 8 whose m-pass tile fits), else the plain FP64 path.
+int default_precision(pfc_run_params p) {
+    p.precision = PFC_PRECISION_MIXED;
+    double b = 0.0;
+    return pfc_run_bytes(&p, &b) == PFC_OK ? PFC_PRECISION_MIXED : PFC_PRECISION_FP64;
+}
+
 bool parse_precision(const char *v, int &out) {
     if (!v) return false;
     std::string s(v);
@@ -150,7 +158,7 @@ struct SimOpts {
     unsigned int seed;
     int grainx, grainy, grainz;
     int L = 256, M = 256, N = 1;
-    int precision = -1;  // -1: mixed on 2-D grids, FP64 on 3-D grids
+    int precision = -1;  // -1: default_precision (mixed where its kernels take the grid)
     int resume = -1;  // --resume <kd>: continue from the run's own checkpoint kd
     std::string outdir;
 };
@@ -203,7 +211,7 @@ void misfit_usage(const char *argv0) {
          << "  --axx <float>       Noise base intensity (default: 0)\n"
          << "  --outdir <path>     Output directory (default: current dir)\n"
          << "  --grid <LxMxN>      Grid (default: 256x256x1)\n"
-         << "  --precision <p>     mixed, fp32, fp64 or fp64-pure (default: mixed on 2-D grids, fp64 on 3-D)\n"
+         << "  --precision <p>     mixed, fp32, fp64 or fp64-pure (default: mixed; fp64 on 3-D grids it does not take)\n"
          << "  --resume <kd>       Continue from checkpoint kd in --outdir\n"
          << "  -h, --help          Show this help\n";
 }
@@ -399,7 +407,7 @@ int run_misfit_cli(int argc, char **argv) {
     p.grainy = o.grainy;
     p.grainz = o.grainz;
     p.seed = o.seed;
-    p.precision = o.precision >= 0 ? o.precision : (N == 1 ? PFC_PRECISION_MIXED : PFC_PRECISION_FP64);
+    p.precision = o.precision >= 0 ? o.precision : default_precision(p);
     RunGuard g;
     if (pfc_run_create(&p, &g.r) != PFC_OK) return gpu_fail("run setup");
     pfc_run *r = g.r;
@@ -468,7 +476,7 @@ void cvd_usage(const char *argv0) {
          << "  --seed <uint>       Random seed base (default: 20200604)\n"
          << "  --outdir <path>     Output directory (default: current dir)\n"
          << "  --grid <LxMxN>      Grid (default: 256x256x1)\n"
-         << "  --precision <p>     mixed, fp32, fp64 or fp64-pure (default: mixed on 2-D grids, fp64 on 3-D)\n"
+         << "  --precision <p>     mixed, fp32, fp64 or fp64-pure (default: mixed; fp64 on 3-D grids it does not take)\n"
          << "  --resume <kd>       Continue from checkpoint kd in --outdir\n"
          << "  -h, --help          Show this help\n";
 }
@@ -580,7 +588,7 @@ int run_cvd_cli(int argc, char **argv) {
     p.dt = o.dt;
     p.dx = o.dx;
     p.seed = o.seed;
-    p.precision = o.precision >= 0 ? o.precision : (N == 1 ? PFC_PRECISION_MIXED : PFC_PRECISION_FP64);
+    p.precision = o.precision >= 0 ? o.precision : default_precision(p);
     RunGuard g;
     if (pfc_run_create(&p, &g.r) != PFC_OK) return gpu_fail("run setup");
     pfc_run *r = g.r;

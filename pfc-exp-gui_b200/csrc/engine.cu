@@ -411,7 +411,8 @@ extern "C" int pfc_run_bytes(const pfc_run_params *p, double *bytes) {
     const int nc = tile_candidates(p->L, p->precision, cand);
     int ct = nc ? cand[nc - 1] : tile_default(p->L, p->precision);
     if (d3) ct = tile_width_3d(p->L, p->M);
-    if (d3 && ct == 0) return set_error(PFC_E_INVALID, "unsupported 3-D grid");
+    if (d3 && (ct == 0 || !mixed_row_len_ok(p->N) || p->precision != PFC_PRECISION_MIXED))
+        return set_error(PFC_E_INVALID, "3-D grid not taken by the fused paths");
     double b = (double)run_state_bytes(p->L, p->M, p->N, p->precision, ct);
     const double P = (double)p->L * p->M * p->N;
     if (d3) b += (double)p->L * p->M * round_up(p->N / 2 + 1, ct) * kcoef_point_bytes(p->precision);

@@ -189,13 +189,24 @@ def test_cli_fp64_precision_3d(tmp_path):
         vals, _, _ = read_vti(out / f"phi_{kd}_0.vti")
         assert np.abs(vals - fields[f"phi_{kd}"]).max() <= 1e-6
     check_cvd_analysis_files(out, d, (0, 5, 10), 1e-5)
-    # without --precision a 3-D grid runs on the FP64 path (the FP32 path takes 2-D grids)
+    # without --precision a 3-D grid with N >= 8 runs on the mixed path (--precision mixed):
+    # its fields stay within the reference's own float-rounding distance from this FP64 run
     out2 = tmp_path / "cvd3_default"
     r = run_cli(["--model", "cvd", "--grid", "32x32x8", *meta["args"], "--outdir", str(out2)])
     assert r.returncode == 0, r.stderr
-    a, _, _ = read_vti(out / "phi_10_0.vti")
+    out3 = tmp_path / "cvd3_mixed"
+    r = run_cli(["--model", "cvd", "--grid", "32x32x8", "--precision", "mixed", *meta["args"], "--outdir", str(out3)])
+    assert r.returncode == 0, r.stderr
     b, _, _ = read_vti(out2 / "phi_10_0.vti")
-    assert np.array_equal(a, b)
+    c, _, _ = read_vti(out3 / "phi_10_0.vti")
+    assert np.array_equal(b, c)
+    assert np.abs(b - fields["phi_10"]).max() <= 1e-5
+    check_cvd_analysis_files(out2, d, (0, 5, 10), 1e-4)
+    # a 3-D grid the mixed kernels do not take (N < 8) defaults to the FP64 path
+    out4 = tmp_path / "cvd3_n4"
+    r = run_cli(["--model", "cvd", "--grid", "32x32x4", "--steps", "2", "--mod", "1", "--outdir", str(out4)])
+    assert r.returncode == 0, r.stderr
+    assert (out4 / "phi_1_0.vti").exists()
 
 
 def test_cli_batch_file_errors(tmp_path):
