@@ -88,10 +88,12 @@ int get_context(int device, Context **out) {
         c->fault = f;
         c->tw.fault = fd;
     }
-    // twiddles for n = 2^1 .. 2^11 in the stage layout of the transforms (twiddle_offset,
-    // fft_core.cuh): stage (Ns, R) entry k*R + r = exp(-2 pi i j / n), j = r*k*n/(Ns*R),
-    // in double, rounded once for FP32.  Each length gets 2n entries (enough for every
-    // stage table up to n = 2048; 16-byte aligned starts).
+    // twiddles for n = 2^1 .. 2^11: the FP32 tables in the stage layout of the radix-16
+    // transforms (twiddle_offset, fft_core.cuh), stage (Ns, R) entry k*R + r =
+    // exp(-2 pi i j / n), j = r*k*n/(Ns*R), computed in double and rounded once; the FP64
+    // tables plain, entry j = exp(-2 pi i j / n) for j < n (an FP64 stage loads its base
+    // factor from them and forms the powers).  Each length gets 2n entries (enough for
+    // every stage table up to n = 2048; 16-byte aligned starts).
     size_t total = 0;
     for (int lg = 1; lg <= 11; ++lg) total += (size_t)2 << lg;
     std::vector<double2> h64(total, make_double2(0.0, 0.0));
@@ -108,7 +110,6 @@ int get_context(int device, Context **out) {
                     for (int r = 0; r < R; ++r) {
                         const long j = (long)r * k * (n / (ns * R));
                         const double a = 2.0 * M_PI * (double)j / (double)n;
-                        h64[at + (size_t)k * R + r] = make_double2(std::cos(a), -std::sin(a));
                         h32[at + (size_t)k * R + r] = make_float2((float)std::cos(a), (float)-std::sin(a));
                     }
                 at += (size_t)ns * R;
@@ -117,6 +118,10 @@ int get_context(int device, Context **out) {
             rem /= R;
         }
         if (at - off > (size_t)2 * n) return set_error(PFC_E_INVALID, "twiddle table overflow");
+        for (int j = 0; j < n; ++j) {
+            const double a = 2.0 * M_PI * (double)j / (double)n;
+            h64[off + (size_t)j] = make_double2(std::cos(a), -std::sin(a));
+        }
         off += (size_t)2 * n;
     }
     char *mem = nullptr;

@@ -186,21 +186,23 @@ template <int R, bool FWD, typename C> __device__ __forceinline__ void dftR(C *a
 }
 
 // ---------------------------------------------------------------------------
-// Radix plan: N = 16^a * r with r in {1, 2, 4, 8}; the small radix comes last.
+// Radix plan: N = RM^a * r with RM the main radix and r < RM a power of two; the small
+// radix comes last.  The main radix may follow the element type (main_radix); it is 16
+// for both FP32 and FP64.  (FP64 transforms were measured with radix 8 too: twice the
+// threads and half the registers per thread, but the extra shared-memory stage made
+// the mixed step 8 % slower at 1024^2.)
 // ---------------------------------------------------------------------------
-template <int N> struct radix_plan {
-    static constexpr int log2n = (N <= 1) ? 0 : 1 + radix_plan<N / 2>::log2n;
-    static constexpr int n16 = log2n / 4;
-    static constexpr int tail = 1 << (log2n % 4);  // 1, 2, 4 or 8
-    static constexpr int stages = n16 + (tail > 1 ? 1 : 0);
-    static constexpr int last_radix = tail > 1 ? tail : 16;
+template <typename C> struct main_radix {
+    static constexpr int value = 16;
 };
-template <> struct radix_plan<1> {
-    static constexpr int log2n = 0;
-    static constexpr int n16 = 0;
-    static constexpr int tail = 1;
-    static constexpr int stages = 0;
-    static constexpr int last_radix = 1;
+__host__ __device__ constexpr int clog2(int n) { return n <= 1 ? 0 : 1 + clog2(n / 2); }
+template <int N, int RM = 16> struct radix_plan {
+    static constexpr int log2n = clog2(N);
+    static constexpr int lr = clog2(RM);
+    static constexpr int nmain = log2n / lr;
+    static constexpr int tail = 1 << (log2n % lr);
+    static constexpr int stages = nmain + (tail > 1 ? 1 : 0);
+    static constexpr int last_radix = tail > 1 ? tail : (log2n == 0 ? 1 : RM);
 };
 
 template <int N, int NB, int NT, int R> struct StageShape {
@@ -209,10 +211,11 @@ template <int N, int NB, int NT, int R> struct StageShape {
     static constexpr bool EXACT = ITEMS % NT == 0;
 };
 
-// Twiddle table of one length: every stage but the first (which has Ns = 1 and no
-// twiddles) owns Ns*R entries, entry k*R + r = exp(-2 pi i r k / (Ns R)).  All stages
-// before the last have radix 16, so the stage with Ns = 16^m starts at
-// 16 * (16 + 256 + ... + 16^(m-1)) = 16 (Ns - 16) / 15.
+// FP32 twiddle table of one length (radix-16 plans): every stage but the first (which has
+// Ns = 1 and no twiddles) owns Ns*R entries, entry k*R + r = exp(-2 pi i r k / (Ns R)).
+// All stages before the last have radix 16, so the stage with Ns = 16^m starts at
+// 16 * (16 + 256 + ... + 16^(m-1)) = 16 (Ns - 16) / 15.  (The FP64 table of a length N
+// holds exp(-2 pi i j / N), j < N: a butterfly's base factor is entry k N / (Ns R).)
 __host__ __device__ constexpr int twiddle_offset(int Ns) { return Ns < 16 ? 0 : 16 * ((Ns - 16) / 15); }
 // entries of the whole table of length N (at most 2N for N <= 2048)
 __host__ __device__ constexpr int twiddle_entries(int N) {
@@ -317,7 +320,7 @@ __device__ __forceinline__ void stage(const CI *__restrict__ in, typename nodedu
             const int k = j % NS;
             if constexpr (NS > 1) {
                 if constexpr (std::is_same<C, double2>::value) {
-                    twiddle_powers<R, FWD>(v[q], __ldg(tw + twiddle_offset(NS) + k * R + 1));
+                    twiddle_powers<R, FWD>(v[q], __ldg(tw + k * (N / (NS * R))));
                 } else {
                     C t[R];
                     load_twiddles<R>(tw + twiddle_offset(NS) + k * R, t);
@@ -344,21 +347,23 @@ __device__ __forceinline__ void stage(const CI *__restrict__ in, typename nodedu
     if (OUT == SP_SMEM) __syncthreads();
 }
 
-// Values a thread holds after a transform that ends in registers.
-template <int N, int NB, int NT> struct RegOut {
-    typedef radix_plan<N> P;
+// Values a thread holds after a transform of element type C that ends in registers.
+template <int N, int NB, int NT, typename C = float2> struct RegOut {
+    typedef radix_plan<N, main_radix<C>::value> P;
     static constexpr int R = P::last_radix;
     static constexpr int PER_T = StageShape<N, NB, NT, R>::PER_T;
     static constexpr int NS = N / R;  // Ns of the last stage
 };
 
-// The radix-16 stages between the first and the last, in place in shared memory.
+// The main-radix stages between the first and the last, in place in shared memory.
 template <int N, int NB, int NT, int NS, int LAST_NS, bool FWD, typename C>
-__device__ __forceinline__ void middle_stages(C *s, const C *__restrict__ tw,
-                                              C (&v)[StageShape<N, NB, NT, 16>::PER_T][16]) {
+__device__ __forceinline__ void middle_stages(
+    C *s, const C *__restrict__ tw,
+    C (&v)[StageShape<N, NB, NT, main_radix<C>::value>::PER_T][main_radix<C>::value]) {
+    constexpr int RM = main_radix<C>::value;
     if constexpr (NS < LAST_NS) {
-        stage<N, NB, NT, 16, NS, FWD, SP_SMEM, SP_SMEM>(s, s, tw, v);
-        middle_stages<N, NB, NT, NS * 16, LAST_NS, FWD>(s, tw, v);
+        stage<N, NB, NT, RM, NS, FWD, SP_SMEM, SP_SMEM>(s, s, tw, v);
+        middle_stages<N, NB, NT, NS * RM, LAST_NS, FWD>(s, tw, v);
     }
 }
 
@@ -383,9 +388,10 @@ template <int N, int NB, int NT, bool FWD, int IN, int OUT, typename C, typename
           typename CI = C>
 __device__ __forceinline__ void fft(const CI *src, C *s, typename nodeduce<C>::type *dst,
                                     const C *__restrict__ tw,
-                                    C (&last)[RegOut<N, NB, NT>::PER_T][RegOut<N, NB, NT>::R], XF xf = XF(),
+                                    C (&last)[RegOut<N, NB, NT, C>::PER_T][RegOut<N, NB, NT, C>::R], XF xf = XF(),
                                     AF af = AF()) {
-    typedef radix_plan<N> P;
+    constexpr int RM = main_radix<C>::value;
+    typedef radix_plan<N, RM> P;
     if constexpr (P::stages == 1) {
         stage<N, NB, NT, P::last_radix, 1, FWD, IN, OUT>(src, dst, tw, last, xf);
         if constexpr (!std::is_same<AF, NoHook>::value) {
@@ -393,21 +399,21 @@ __device__ __forceinline__ void fft(const CI *src, C *s, typename nodeduce<C>::t
             af();
         }
     } else {
-        typedef StageShape<N, NB, NT, 16> S16;
-        C v[S16::PER_T][16];
-        // first stage (radix 16): src -> scratch
-        stage<N, NB, NT, 16, 1, FWD, IN, SP_SMEM>(src, s, tw, v, xf);
+        typedef StageShape<N, NB, NT, RM> SM;
+        C v[SM::PER_T][RM];
+        // first stage (main radix): src -> scratch
+        stage<N, NB, NT, RM, 1, FWD, IN, SP_SMEM>(src, s, tw, v, xf);
         af();
-        middle_stages<N, NB, NT, 16, RegOut<N, NB, NT>::NS, FWD>(s, tw, v);
+        middle_stages<N, NB, NT, RM, RegOut<N, NB, NT, C>::NS, FWD>(s, tw, v);
         // last stage: scratch -> dst / registers
-        stage<N, NB, NT, P::last_radix, RegOut<N, NB, NT>::NS, FWD, SP_SMEM, OUT>(s, dst, tw, last);
+        stage<N, NB, NT, P::last_radix, RegOut<N, NB, NT, C>::NS, FWD, SP_SMEM, OUT>(s, dst, tw, last);
     }
 }
 
 // Convenience: in-place FFT of a padded shared array.
 template <int N, int NB, int NT, bool FWD, typename C>
 __device__ __forceinline__ void fft_smem(C *s, const C *__restrict__ tw) {
-    C last[RegOut<N, NB, NT>::PER_T][RegOut<N, NB, NT>::R];
+    C last[RegOut<N, NB, NT, C>::PER_T][RegOut<N, NB, NT, C>::R];
     fft<N, NB, NT, FWD, SP_SMEM, SP_SMEM>(s, s, s, tw, last);
 }
 

@@ -13,7 +13,7 @@ namespace pfc {
 // Column tile of the mixed path (mcol_tile_ok, step_common.cuh): two padded double2
 // buffers and an FP32 staging buffer, 43 KB to 172 KB.
 template <int L, int C> struct MColCfg {
-    static constexpr int NT = (C * L / 16) < 32 ? 32 : (C * L / 16);
+    static constexpr int NT = (C * L / 16) < 32 ? 32 : (C * L / 16);  // one radix-16 butterfly per thread
     static constexpr int SMEM = 2 * (int)sizeof(double2) * padded_len<C * L>::value + (int)sizeof(float2) * C * L;
     static constexpr int FIT = (228 * 1024) / (SMEM + 1024);  // CTAs per SM the shared memory leaves room for
     static constexpr int MINB = FIT > 8 ? 8 : (FIT < 1 ? 1 : FIT);
@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(MColCfg<L, C>::NT, MColCfg<L, C>::MINB)
     k_mcol_step(const RunDesc *__restrict__ runs, int nruns, int per, const double2 *__restrict__ tw, int *fault) {
     constexpr int NT = MColCfg<L, C>::NT;
     constexpr int SPAD = padded_len<C * L>::value;
-    typedef RegOut<L, C, NT> RO;
+    typedef RegOut<L, C, NT, double2> RO;
     extern __shared__ __align__(16) double2 smd[];
     __shared__ __align__(8) unsigned long long stage_bar;
     double2 *s = smd;                                         // FFT scratch

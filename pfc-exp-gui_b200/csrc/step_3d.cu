@@ -19,7 +19,7 @@
 namespace pfc {
 
 template <int M, int C> struct MPassCfg {
-    static constexpr int NT = (M * C / 16) < 32 ? 32 : (M * C / 16);
+    static constexpr int NT = (M * C / 16) < 32 ? 32 : (M * C / 16);  // one radix-16 butterfly per thread
 };
 
 template <int M, int C, bool FWD>
