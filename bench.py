@@ -175,13 +175,19 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(grid, batch, kernel):
-    """DRAM bytes per launch of `kernel` ("col" or "row") from the committed ncu summary, scaled to this batch."""
+def profiled_kernel(kernel):
+    """The committed ncu figures of one kernel (profiles/roofline_traffic.json), or None."""
     p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     if not os.path.exists(p):
         return None
-    j = json.load(open(p))
-    per_run = j.get(f"{kernel}_kernel_dram_bytes_per_run", {}).get(str(grid))
+    return json.load(open(p)).get("kernels", {}).get(kernel)
+
+
+def profiled_traffic(grid, batch, kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary (bytes per run of
+    the profiled launch, times this batch)."""
+    k = profiled_kernel(kernel)
+    per_run = None if k is None else k.get("dram_bytes_per_run", {}).get(str(grid))
     return None if per_run is None else per_run * batch
 
 
@@ -309,31 +315,36 @@ def drain_engine(P, eng, n, timeout_s=900.0):
     return done
 
 
-def sweep_bench(P, dev, nruns=64, steps=2000, master_seed=4242, reps=3):
+PREC_NAMES = {0: "fp32", 1: "fp64", 2: "fp64-pure", 3: "mixed"}
+
+
+def sweep_bench(P, dev, precision, nruns=64, steps=2000, master_seed=4242, reps=3):
     """64 Misfit runs of mixed grids {128, 256, 512}^2, u0 and con0 from the GUI's value
-    lists, drawn with splitmix64 from a master seed; 2000 steps, one checkpoint (mod 2000).
-    Timed as one engine sweep (all submitted at once) and as sequential GPU runs (the
-    same engine with one run resident at a time, as the GUI's one-process queue)."""
+    lists, drawn with splitmix64 from a master seed; 2000 steps, one checkpoint (mod 2000),
+    at the given precision.  Timed as one engine sweep (all submitted at once) and as
+    sequential GPU runs (the same engine with one run resident at a time, as the GUI's
+    one-process queue)."""
     rng = SplitMix64(master_seed)
     jobs = []
     for i in range(nruns):
         g = (128, 256, 512)[rng.next() % 3]
         u0 = (0.02, 0.05, 0.08, 0.11)[rng.next() % 4]
         con0 = (0.1, 0.2, 0.3, 0.4)[rng.next() % 4]
-        jobs.append(P.default_params(P.MODEL_MISFIT, L=g, M=g, seed=1000 + i, u0=u0, con0=con0, device=dev))
+        jobs.append(P.default_params(P.MODEL_MISFIT, L=g, M=g, seed=1000 + i, u0=u0, con0=con0, device=dev,
+                                     precision=precision))
 
     # the autotuner picks each grid's column tile width once per process; it runs here,
     # before either arm is timed, so both arms use the same widths
     t_tune = time.perf_counter()
-    widths = {g: P.tile_width(g, g, device=dev)[0] for g in sorted({p.L for p in jobs})}
+    widths = {g: P.tile_width(g, g, device=dev, precision=precision)[0] for g in sorted({p.L for p in jobs})}
     tune_s = time.perf_counter() - t_tune
 
     def run(max_active):
         eng = P.Engine(device=dev, max_active=max_active)
         # warm-up: one short job per grid, with a checkpoint, so that neither arm pays the
         # first use of a grid's kernels (module loading) inside its timed region
-        warm = [eng.submit(P.JOB_MISFIT, P.default_params(P.MODEL_MISFIT, L=g, M=g, device=dev), steps=40, mod=20)
-                for g in widths]
+        warm = [eng.submit(P.JOB_MISFIT, P.default_params(P.MODEL_MISFIT, L=g, M=g, device=dev, precision=precision),
+                           steps=40, mod=20) for g in widths]
         drain_engine(P, eng, len(warm))
         for w in warm:
             eng.release(w)
@@ -356,7 +367,8 @@ def sweep_bench(P, dev, nruns=64, steps=2000, master_seed=4242, reps=3):
     grids = {}
     for p in jobs:
         grids[p.L] = grids.get(p.L, 0) + 1
-    return {"runs": nruns, "steps": steps, "grids": {f"{g}^2": n for g, n in sorted(grids.items())},
+    return {"runs": nruns, "steps": steps, "precision": PREC_NAMES[precision],
+            "grids": {f"{g}^2": n for g, n in sorted(grids.items())},
             "master_seed": master_seed,
             "batched_s": round(wall_b, 3), "sequential_gpu_s": round(wall_s, 3),
             "batched_s_rounds": [round(w, 3) for w, _ in rounds_b],
@@ -435,10 +447,11 @@ def serve_bench(P, dev, n_req=48, lam=4.0, seed=777, budget=150e9):
             "what": "engine with continuous batching; latency = submission to DONE (results and events ready)"}
 
 
-def step_roofline(P, batch, G, B, reps=20):
+def step_roofline(P, batch, G, B, names, reps=20):
     """Event-timed row and column kernel launches of a batch, each against the HBM peak
     with its algorithmic bytes (row: 4 row-space arrays read, 2 written; column: 4 + 4;
-    8 bytes per complex half-spectrum element)."""
+    8 bytes per complex half-spectrum element), the DRAM traffic the committed ncu
+    capture measured, and (FP64-arithmetic kernels) the FP64 pipe's active fraction there."""
     row_ms, col_ms = batch.kernel_times(reps)
     H1 = G // 2 + 1
     by = {"row": B * G * H1 * 8 * 6, "col": B * G * H1 * 8 * 8}
@@ -447,7 +460,11 @@ def step_roofline(P, batch, G, B, reps=20):
     for name, ms_k in (("row", row_ms), ("col", col_ms)):
         ach = by[name] / (ms_k / 1000.0) / 1e9
         out[name] = {"launch_ms": round(ms_k, 5), "algorithmic_bytes_per_launch": by[name],
-                     "achieved": round(ach, 1), "frac": round(ach / peak, 4)}
+                     "achieved": round(ach, 1), "frac": round(ach / peak, 4),
+                     "traffic": profiled_traffic(G, B, names[name])}
+        prof = profiled_kernel(names[name])
+        if prof and prof.get("fp64_pipe_active_pct") is not None:
+            out[name]["fp64_pipe_active_pct_profiled"] = prof["fp64_pipe_active_pct"]
     return out
 
 
@@ -513,9 +530,9 @@ def run_ours(args):
     value = total_run_steps / (ms_max / 1000.0)
 
     # per-kernel roofline (dominant kernel), timed with events on the library stream
-    kern = step_roofline(P, batch, G, B)
-    dom = "col" if kern["col"]["launch_ms"] >= kern["row"]["launch_ms"] else "row"
     names = {"row": "k_mrow_step", "col": "k_mcol_step"}
+    kern = step_roofline(P, batch, G, B, names)
+    dom = "col" if kern["col"]["launch_ms"] >= kern["row"]["launch_ms"] else "row"
     peak, peak_kind = measured_peak()
 
     # end to end through the public API: FP32 host fields from pinned memory in, B runs x K
@@ -567,10 +584,10 @@ def run_ours(args):
                                                        for k, (a, b) in stage_trials.items()}},
         "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": kern[dom]["achieved"], "peak": peak,
                      "unit": "GB/s", "frac": kern[dom]["frac"], "peak_source": peak_kind,
-                     "traffic": profiled_traffic(G, B, dom),
+                     "traffic": kern[dom]["traffic"],
                      "algorithmic_bytes_per_launch": kern[dom]["algorithmic_bytes_per_launch"],
                      "launch_ms": kern[dom]["launch_ms"],
-                     "per_kernel": {names[k]: dict(v, traffic=profiled_traffic(G, B, k)) for k, v in kern.items()}},
+                     "per_kernel": {names[k]: v for k, v in kern.items()}},
         "e2e": {"value": round(e2e_value, 2), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "steps": args.steps, "pinned_host_buffers": pin,
                 "what": "pfc_run_set_fields_f32 (FP32 host fields) + pfc_batch_advance(K) + pfc_run_get_fields_f32, "
@@ -588,7 +605,7 @@ def run_ours(args):
     b32 = P.Batch(runs32)
     b32.advance(5)
     ms32 = b32.advance_timed(min(args.steps, 200))
-    k32 = step_roofline(P, b32, G, B)
+    k32 = step_roofline(P, b32, G, B, {"row": "k_row_step", "col": "k_col_step"})
     line["fp32_path"] = {"run_steps_per_s": round(B * min(args.steps, 200) / (ms32 / 1000.0), 2),
                          "ms_per_step": round(ms32 / min(args.steps, 200), 5),
                          "column_tile_width": P.tile_width(G, G, device=dev, precision=P.FP32)[0],
@@ -658,7 +675,10 @@ def run_ours(args):
             line["cpu_baseline"] = {"value": None, "error": str(e)}
     # sweep and serving workloads, each rank on its own GPU (rank 0 reports its own)
     if not args.no_sweep:
-        line["sweep"] = sweep_bench(P, dev)
+        # the sweep workload names FP32 arithmetic with FP64 reductions (the FP32 path);
+        # the same sweep on the default mixed-precision path beside it
+        line["sweep"] = sweep_bench(P, dev, P.FP32)
+        line["sweep"]["mixed_precision"] = sweep_bench(P, dev, P.MIXED)
     if not args.no_serve:
         line["serving"] = serve_bench(P, dev, n_req=args.serve_requests, seed=777 + dist.rank)
     if dist.rank == 0:

@@ -120,6 +120,11 @@ int pfc_set_col_staging(int device, int L, int M, int precision, int stage);
  * the kernel's device time.  Uses its own fault word, not the device's. */
 int pfc_selftest_tile_stage(int device, int issue, int n, double limit_ms, int *timed_out, int *match, double *ms);
 
+/* Self-test of the mixed path's double-precision logarithm (the table-driven log of its
+ * pointwise terms): y[i] = that log of x[i] for n host doubles (1 <= n <= 2^24),
+ * evaluated on the device. */
+int pfc_selftest_log(int device, const double *x, double *y, int n);
+
 /* Steps taken so far. */
 int pfc_run_steps(const pfc_run *r, int *steps);
 

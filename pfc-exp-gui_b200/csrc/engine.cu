@@ -124,10 +124,19 @@ int get_context(int device, Context **out) {
         }
         off += (size_t)2 * n;
     }
+    // log_tab's breakpoints F_j = 1 + j/128: (log F_j, 1/F_j), each rounded once
+    std::vector<double2> hlog(LOG_TABLE_SIZE);
+    for (int j = 0; j < LOG_TABLE_SIZE; ++j) {
+        const double F = 1.0 + j / 128.0;
+        hlog[j] = make_double2(std::log(F), 1.0 / F);
+    }
+    const size_t tw_bytes = total * (sizeof(double2) + sizeof(float2));
     char *mem = nullptr;
-    PFC_CUDA_TRY(cudaMalloc(&mem, total * (sizeof(double2) + sizeof(float2))));
+    PFC_CUDA_TRY(cudaMalloc(&mem, tw_bytes + LOG_TABLE_SIZE * sizeof(double2)));
     PFC_CUDA_TRY(cudaMemcpy(mem, h64.data(), total * sizeof(double2), cudaMemcpyHostToDevice));
     PFC_CUDA_TRY(cudaMemcpy(mem + total * sizeof(double2), h32.data(), total * sizeof(float2), cudaMemcpyHostToDevice));
+    PFC_CUDA_TRY(cudaMemcpy(mem + tw_bytes, hlog.data(), LOG_TABLE_SIZE * sizeof(double2), cudaMemcpyHostToDevice));
+    c->tw.logt = reinterpret_cast<const double2 *>(mem + tw_bytes);
     c->tw_mem = mem;
     off = 0;
     for (int lg = 1; lg <= 11; ++lg) {
@@ -237,9 +246,9 @@ static KcoefKey kcoef_key(const pfc_run *r) {
 }
 
 // Bytes per k point of the shared table: (kden, kc2) float2 pairs on the FP32 path,
-// (kmix, kc2d) = double4 + double2 on the mixed path.
+// four doubles (kfn, kfc, kc2a, kc2b) on the mixed path.
 static size_t kcoef_point_bytes(int prec) {
-    return prec == PFC_PRECISION_MIXED ? sizeof(double4) + sizeof(double2) : 2 * sizeof(float2);
+    return prec == PFC_PRECISION_MIXED ? 4 * sizeof(double) : 2 * sizeof(float2);
 }
 
 // Pure-FP64 C2 parameters (the oracle's pure mode of MIS:700-750): crossover, peak
@@ -284,11 +293,11 @@ static int acquire_kcoef(pfc_run *r) {
             if (r->d3)
                 ce = launch_build_kmix3(r->d_desc_col, (double)k.dynamic_mn * (double)r->p.dt,
                                         (double)k.dynamic_mc * (double)r->p.dt, (double)k.para_alpha, ca, cb,
-                                        (double4 *)e.ptr, (double2 *)((double4 *)e.ptr + npts), r->stream);
+                                        (double *)e.ptr, r->stream);
             else
                 ce = launch_build_kmix(r->d_desc, (double)k.dynamic_mn * (double)r->p.dt,
                                        (double)k.dynamic_mc * (double)r->p.dt, (double)k.para_alpha, ca, cb,
-                                       (double4 *)e.ptr, (double2 *)((double4 *)e.ptr + npts), r->stream);
+                                       (double *)e.ptr, r->stream);
         } else {
             ce = launch_build_kcoef(r->d_desc, (float2 *)e.ptr, (float2 *)e.ptr + npts, r->stream);
         }
@@ -302,8 +311,11 @@ static int acquire_kcoef(pfc_run *r) {
     e.refs++;
     if (mixed) {
         RunDesc &t = r->d3 ? r->desc_col : r->desc;
-        t.kmix = (const double4 *)e.ptr;
-        t.kc2d = (const double2 *)((const double4 *)e.ptr + npts);
+        const double *pl = (const double *)e.ptr;
+        t.kfn = pl;
+        t.kfc = pl + npts;
+        t.kc2a = pl + 2 * npts;
+        t.kc2b = pl + 3 * npts;
     } else {
         r->desc.kden = (const float2 *)e.ptr;
         r->desc.kc2 = (const float2 *)e.ptr + npts;
@@ -324,8 +336,7 @@ static void release_kcoef(pfc_run *r) {
     }
     r->desc.kden = nullptr;
     r->desc.kc2 = nullptr;
-    r->desc.kmix = nullptr;
-    r->desc.kc2d = nullptr;
+    for (RunDesc *t : {&r->desc, &r->desc_col}) t->kfn = t->kfc = t->kc2a = t->kc2b = nullptr;
 }
 
 // k-vectors exactly as MIS:455-462 (float storage, double arithmetic).
@@ -599,13 +610,15 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
         // pure-FP64 k-vectors (the oracle's pure mode of MIS:455-462)
         double *kd = (double *)m;
         m += round_up((int)kdtab, 256);
+        // entry i = s(i) * dk, s(i) the signed index, dk = 2 pi / (n dx): the product the
+        // column kernel forms for l without a load
         std::vector<double> h(r->L + r->M + r->N);
-        for (int l = 0; l < r->L; ++l)
-            h[l] = (double)(l <= r->L / 2 ? l : l - r->L) * 2.0 * PI_REF / ((double)r->L * p->dx);
-        for (int mm = 0; mm < r->M; ++mm)
-            h[r->L + mm] = (double)(mm <= r->M / 2 ? mm : mm - r->M) * 2.0 * PI_REF / ((double)r->M * p->dx);
-        for (int n = 0; n < r->N; ++n)
-            h[r->L + r->M + n] = (double)(n <= r->N / 2 ? n : n - r->N) * 2.0 * PI_REF / ((double)r->N * p->dx);
+        d.dkl = 2.0 * PI_REF / ((double)r->L * p->dx);
+        d.dkm = 2.0 * PI_REF / ((double)r->M * p->dx);
+        d.dkn = 2.0 * PI_REF / ((double)r->N * p->dx);
+        for (int l = 0; l < r->L; ++l) h[l] = (double)(l <= r->L / 2 ? l : l - r->L) * d.dkl;
+        for (int mm = 0; mm < r->M; ++mm) h[r->L + mm] = (double)(mm <= r->M / 2 ? mm : mm - r->M) * d.dkm;
+        for (int n = 0; n < r->N; ++n) h[r->L + r->M + n] = (double)(n <= r->N / 2 ? n : n - r->N) * d.dkn;
         r->kd_host = h;
         cudaMemcpyAsync(kd, r->kd_host.data(), kdtab, cudaMemcpyHostToDevice, r->stream);
         d.kdl = kd;
@@ -639,6 +652,8 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
     d.noise_amp = (p->model == PFC_MODEL_MISFIT && r->b0 != 0.0f) ? p->dt * r->b0 : 0.0f;
     d.noise_key = noise_key(p->seed);
     d.noise_amp_d = (p->model == PFC_MODEL_MISFIT && r->b0 != 0.0f) ? (double)p->dt * (double)r->b0 : 0.0;
+    d.mn_dt = (double)r->k.dynamic_mn * (double)p->dt;
+    d.mc_dt = (double)r->k.dynamic_mc * (double)p->dt;
     if (fused) {
         int *hf = nullptr;
         cudaError_t ce = cudaHostAlloc(reinterpret_cast<void **>(&hf), sizeof(int), cudaHostAllocMapped);
@@ -939,6 +954,24 @@ extern "C" int pfc_selftest_tile_stage(int device, int issue, int n, double limi
     if (f) cudaFreeHost(f);
     if (d) cudaFree(d);
     if (e != cudaSuccess) return cuda_error(e, "pfc_selftest_tile_stage");
+    return PFC_OK;
+}
+
+extern "C" int pfc_selftest_log(int device, const double *x, double *y, int n) {
+    if (!x || !y) return set_error(PFC_E_INVALID, "null argument");
+    if (n < 1 || n > (1 << 24)) return set_error(PFC_E_INVALID, "n must be in [1, 2^24]");
+    Context *c = nullptr;
+    int rc = get_context(device, &c);
+    if (rc != PFC_OK) return rc;
+    PFC_CUDA_TRY(cudaSetDevice(device));
+    double *d = nullptr;
+    cudaError_t e = cudaMalloc(&d, 2 * sizeof(double) * (size_t)n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d, x, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = launch_log_selftest(d, d + n, n, c->tw.logt, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(y, d + n, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (d) cudaFree(d);
+    if (e != cudaSuccess) return cuda_error(e, "pfc_selftest_log");
     return PFC_OK;
 }
 

@@ -11,10 +11,12 @@
 namespace pfc {
 
 // Column tile of the mixed path (mcol_tile_ok, step_common.cuh): two padded double2
-// buffers and an FP32 staging buffer, 43 KB to 172 KB.
+// buffers, an FP32 staging buffer and a coefficient plane slot, 47 KB to 205 KB.
 template <int L, int C> struct MColCfg {
     static constexpr int NT = (C * L / 16) < 32 ? 32 : (C * L / 16);  // one radix-16 butterfly per thread
-    static constexpr int SMEM = 2 * (int)sizeof(double2) * padded_len<C * L>::value + (int)sizeof(float2) * C * L;
+    static_assert(NT % C == 0, "a thread's elements share one tile column");
+    static constexpr int SMEM = 2 * (int)sizeof(double2) * padded_len<C * L>::value + (int)sizeof(float2) * C * L +
+                                (int)sizeof(double) * C * L;
     static constexpr int FIT = (228 * 1024) / (SMEM + 1024);  // CTAs per SM the shared memory leaves room for
     static constexpr int MINB = FIT > 8 ? 8 : (FIT < 1 ? 1 : FIT);
 };
@@ -25,16 +27,27 @@ __device__ __forceinline__ float2 narrow(double2 v) { return make_float2((float)
 // ---------------------------------------------------------------------------
 // Column kernel.
 // ---------------------------------------------------------------------------
-// multiplier of an inverse transform's first stage: P * C2A (which = 0) or C2B (which = 1)
+// multiplier of an inverse transform's first stage: P * C2A or C2B (one plane of the table)
 struct ScaleByTableD {
-    const double2 *tab;
-    int C, which;
+    const double *tab;
+    int C;
     __device__ __forceinline__ double2 operator()(int e, int b, double2 v) const {
-        const double2 t = tab[e * C + b];
-        const double g = which == 0 ? t.x : t.y;
+        const double g = tab[e * C + b];
         return make_double2(v.x * g, v.y * g);
     }
 };
+// The column part of k^2 for tile column b: km^2 of column km0 + b (2-D; 0 past M/2, the
+// padding), or km^2 + kn^2 of a 3-D column view's tile (km = km3, kn = kn0 + b, 0 past N/2).
+__device__ __forceinline__ double col_k2(const RunDesc &d, int b, int km0, int km3, int kn0) {
+    if (km3 < 0) {
+        const int km = km0 + b;
+        const double k = km <= d.M / 2 ? d.kdm[km] : 0.0;
+        return k * k;
+    }
+    const int kn = kn0 + b;
+    const double km = d.kdm[km3], kz = kn <= d.N / 2 ? d.kdn[kn] : 0.0;
+    return km * km + kz * kz;
+}
 // -i k P along l (which = 0) or m (which = 1), double k-vectors.  A 2-D tile's columns
 // are km = km0 + b (0 past M/2: padding); a 3-D column view's tile has one km (km3, all M
 // values occur, signed through kdm) and its columns are kn.
@@ -61,9 +74,13 @@ template <int L, int C, int NT> __device__ __forceinline__ void tile_out_d(const
 // con, the field's tile is transformed forward into the parked buffer P, the nonlinear
 // term's tile forward into s, the update runs in P, and each output is an inverse
 // transform whose first stage reads P through a multiplier.  Inputs are staged (FP32)
-// into Q by cp.async or one TMA bulk copy per tile (bounded waits; a CTA whose copy
-// does not arrive sets the context's fault word and returns), each issued as soon as
-// the previous transform's first stage has read Q.
+// into Q by cp.async or one TMA bulk copy per tile, each issued as soon as the previous
+// transform's first stage has read Q.  The coefficient planes the item reads (fn, C2A,
+// C2B, fc; C2A and C2B only in the set-up mode) pass through the shared slot Tt, one TMA
+// bulk copy each on a second barrier, each issued once the previous plane's last reader
+// has passed a barrier, so that a transform's time covers the copy.  Waits are bounded: a
+// CTA whose copy does not arrive sets the context's fault word, gives the copies still in
+// flight a last bounded wait, and returns.
 template <int L, int C, int MODE, int STAGE>
 __global__ void __launch_bounds__(MColCfg<L, C>::NT, MColCfg<L, C>::MINB)
     k_mcol_step(const RunDesc *__restrict__ runs, int nruns, int per, const double2 *__restrict__ tw, int *fault) {
@@ -71,22 +88,31 @@ __global__ void __launch_bounds__(MColCfg<L, C>::NT, MColCfg<L, C>::MINB)
     constexpr int SPAD = padded_len<C * L>::value;
     typedef RegOut<L, C, NT, double2> RO;
     extern __shared__ __align__(16) double2 smd[];
-    __shared__ __align__(8) unsigned long long stage_bar;
-    double2 *s = smd;                                         // FFT scratch
-    double2 *Pk = smd + SPAD;                                 // parked spectrum
-    float2 *Q = reinterpret_cast<float2 *>(smd + 2 * SPAD);  // FP32 staging buffer (16-byte aligned)
-    const int T = runs[0].T;                                  // all runs of a launch share L, M and CT
+    __shared__ __align__(8) unsigned long long stage_bar, table_bar;
+    double2 *s = smd;                                                  // FFT scratch
+    double2 *Pk = smd + SPAD;                                          // parked spectrum
+    float2 *Q = reinterpret_cast<float2 *>(smd + 2 * SPAD);           // FP32 staging buffer (16-byte aligned)
+    double *Tt = reinterpret_cast<double *>(Q + L * C);                // coefficient plane slot (16-byte aligned)
+    const int T = runs[0].T;                                           // all runs of a launch share L, M and CT
     const int items = nruns * T;
     const int first = blockIdx.x * per;
     const int end = first + per < items ? first + per : items;
     if (first >= end) return;
     double2 b[RO::PER_T][RO::R];
     typedef Stager<L, C, NT, STAGE> ST;
-    const ST st{smem_u32(&stage_bar), Q};
+    const ST st{smem_u32(&stage_bar), Q, true, smem_u32(&table_bar)};
+    const TableStager ts{smem_u32(&table_bar), Tt, (unsigned)(L * C * sizeof(double)), smem_u32(&stage_bar),
+                         STAGE == STAGE_BULK};
     st.init();
+    ts.init();
     auto run_of = [&](int it) { return it % nruns; };
     auto tile_of = [&](int it) { return (long)(it / nruns) * L * C; };
+    // a table wait that gave up: cp.async input copies in flight land before the return
+    auto table_failed = [&]() { st.finish(); };
+    // k_l of row l in a run of spacing dkl (its kdl table's entry, formed without a load)
+    auto kl_of = [](int l, double dkl) { return (double)(l <= L / 2 ? l : l - L) * dkl; };
     st.issue(runs[run_of(first)].psi + tile_of(first));
+    ts.issue(MODE == COL_PREPARE ? runs[run_of(first)].kc2a + tile_of(first) : runs[run_of(first)].kfn + tile_of(first));
     for (int item = first; item < end; ++item) {
         const RunDesc &d = runs[run_of(item)];
         const int H = d.M / 2;
@@ -94,9 +120,15 @@ __global__ void __launch_bounds__(MColCfg<L, C>::NT, MColCfg<L, C>::MINB)
         const int tile_i = item / nruns;
         const int km0 = tile_i * C;                      // 2-D: first column's km
         const int km3 = d.col3d ? tile_i % d.M : -1;     // 3-D column view: the tile's km
-        const float2 *next_psi = item + 1 < end ? runs[run_of(item + 1)].psi + tile_of(item + 1) : nullptr;
-        // barrier phase of this item's first wait: an item of the step modes waits four
-        // times (phases 0, 1, 0, 1), a COL_PREPARE item once (the iteration's parity)
+        // this thread's column (NT is a multiple of C: the same b for all its elements)
+        const double kb2 = MODE == COL_PREPARE ? 0.0 : col_k2(d, threadIdx.x % C, km0, km3, (tile_i / d.M) * C);
+        const double dkl = d.dkl;
+        const bool more = item + 1 < end;
+        const RunDesc *dn = more ? &runs[run_of(item + 1)] : nullptr;
+        const float2 *next_psi = more ? dn->psi + tile_of(item + 1) : nullptr;
+        // barrier phases: an item of the step modes waits four times on each barrier
+        // (phases 0, 1, 0, 1); a COL_PREPARE item once on the input barrier (the
+        // iteration's parity) and twice on the table barrier (0, 1)
         const unsigned p0 = MODE == COL_PREPARE ? (unsigned)(item - first) & 1u : 0u;
 
         // ---- phi ----
@@ -107,6 +139,7 @@ __global__ void __launch_bounds__(MColCfg<L, C>::NT, MColCfg<L, C>::MINB)
             fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, Pk, tw, b, Identity(), Prefetch<ST>{st, d.inn + tile});
             if (!st.wait(1u, fault)) return;
             fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, s, tw, b, Identity(), Prefetch<ST>{st, d.con + tile});
+            if (!ts.wait(0u, fault)) return table_failed();  // fn
         }
         const int nstep = (MODE != COL_PREPARE && d.noise_amp != 0.0f) ? *d.step_ctr : -1;
         for (int e = threadIdx.x; e < L * C; e += NT) {
@@ -114,17 +147,18 @@ __global__ void __launch_bounds__(MColCfg<L, C>::NT, MColCfg<L, C>::MINB)
             double2 v = Pk[pi];
             if (MODE != COL_PREPARE) {
                 // (psi^ - Mn dt k^2 N^ [+ dt b0 xi^ |k| lowpass]) / (1 + Mn dt k^2) / L as
-                // fn/L * psi^ - (an fn/L) * N^; the table is 0 at k = 0 and past M/2
-                const double4 f = d.kmix[tile + e];
-                const double2 nh = s[pi];
-                double rx = v.x * f.x - f.y * nh.x, ry = v.y * f.x - f.y * nh.y;
+                // fn/L * (psi^ - an N^), an = Mn dt k^2; fn is 0 at k = 0 and past M/2
+                const double fn = Tt[e];
                 const int l = e / C, km = km0 + e % C;
+                const double kl = kl_of(l, dkl);
+                const double ks = fma(kl, kl, kb2), an = d.mn_dt * ks;
+                const double2 nh = s[pi];
+                double rx = fn * (v.x - an * nh.x), ry = fn * (v.y - an * nh.y);
                 if (nstep >= 0 && km <= H) {
                     // MAINEQUATIONC2_NOI's noise term (MIS:1002-1003), lowpass at |k| = 2 pi
                     const float2 xi = noise_mode(d.noise_key, nstep, l, km, L, d.M);
-                    const double kl = d.kdl[l], kmv = d.kdm[km];
-                    const double sk = sqrt(kl * kl + kmv * kmv);
-                    const double wn = d.noise_amp_d * sk * (0.5 - 0.5 * tanh((sk - 2.0 * 3.1415926) / 0.1)) * f.x;
+                    const double sk = sqrt(ks);
+                    const double wn = d.noise_amp_d * sk * (0.5 - 0.5 * tanh((sk - 2.0 * 3.1415926) / 0.1)) * fn;
                     rx += wn * (double)xi.x;
                     ry += wn * (double)xi.y;
                 }
@@ -138,12 +172,16 @@ __global__ void __launch_bounds__(MColCfg<L, C>::NT, MColCfg<L, C>::MINB)
         }
         __syncthreads();
         if (MODE != COL_PREPARE) {
+            ts.issue(d.kc2a + tile);  // every thread has read fn
             fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b);
             tile_out_d<L, C, NT>(s, d.psi + tile);
         }
-        fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, ScaleByTableD{d.kc2d + tile, C, 0});
+        if (!ts.wait(MODE == COL_PREPARE ? 0u : 1u, fault)) return table_failed();  // C2A
+        fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, ScaleByTableD{Tt, C}, TableFetch{ts, d.kc2b + tile});
         tile_out_d<L, C, NT>(s, d.ca + tile);
-        fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, ScaleByTableD{d.kc2d + tile, C, 1});
+        if (!ts.wait(MODE == COL_PREPARE ? 1u : 0u, fault)) return table_failed();  // C2B
+        const double *after_c2b = MODE == COL_PREPARE ? (more ? dn->kc2a + tile_of(item + 1) : nullptr) : d.kfc + tile;
+        fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, ScaleByTableD{Tt, C}, TableFetch{ts, after_c2b});
         tile_out_d<L, C, NT>(s, d.cb + tile);
         if (MODE == COL_PREPARE) continue;
 
@@ -152,15 +190,19 @@ __global__ void __launch_bounds__(MColCfg<L, C>::NT, MColCfg<L, C>::MINB)
         fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, Pk, tw, b, Identity(), Prefetch<ST>{st, d.inc + tile});
         if (!st.wait(1u, fault)) return;
         fft<L, C, NT, true, SP_GLOBAL, SP_SMEM>(Q, s, s, tw, b, Identity(), Prefetch<ST>{st, next_psi});
+        if (!ts.wait(1u, fault)) return table_failed();  // fc
         for (int e = threadIdx.x; e < L * C; e += NT) {
             const int pi = spad(e);
-            // (c^ - Mc dt k^2 I^) / (1 + Mc dt alpha k^4) / L as fc/L * c^ - (ac fc/L) * I^
-            const double4 f = d.kmix[tile + e];
+            // (c^ - Mc dt k^2 I^) / (1 + Mc dt alpha k^4) / L as fc/L * (c^ - ac I^), ac = Mc dt k^2
+            const double fc = Tt[e];
+            const double kl = kl_of(e / C, dkl);
+            const double ac = d.mc_dt * fma(kl, kl, kb2);
             const double2 ih = s[pi];
             const double2 v = Pk[pi];
-            Pk[pi] = make_double2(v.x * f.z - f.w * ih.x, v.y * f.z - f.w * ih.y);
+            Pk[pi] = make_double2(fc * (v.x - ac * ih.x), fc * (v.y - ac * ih.y));
         }
         __syncthreads();
+        if (more) ts.issue(dn->kfn + tile_of(item + 1));  // every thread has read fc
         fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b);
         tile_out_d<L, C, NT>(s, d.con + tile);
         if (MODE == COL_STEP_CHECKPOINT) {

@@ -36,12 +36,13 @@ __device__ __forceinline__ CoefsD coefs_d(const ModelCoefs &k) {
     c.inv_1mc0 = 1.0 / (1.0 - (double)k.para_c0);
     return c;
 }
-__device__ __forceinline__ TermsD point_terms_d(const CoefsD &k, double psi, double c, double a, double b) {
+__device__ __forceinline__ TermsD point_terms_d(const CoefsD &k, double psi, double c, double a, double b,
+                                              const double2 *__restrict__ lt) {
     const double psi2 = psi * psi;
     const double in1 = -k.niu * psi2 * 0.5 + k.ksi * psi2 * psi * (1.0 / 3.0);
-    const double lc = log(c * k.inv_c0);
+    const double lc = log_tab(c * k.inv_c0, lt);
     const double omc = 1.0 - c;
-    const double l1c = log(omc * k.inv_1mc0);
+    const double l1c = log_tab(omc * k.inv_1mc0, lt);
     const double in2 = k.w * (c * lc + omc * l1c);
     const double c2 = c * c, omc2 = omc * omc;
     const double in3 = -(1.0 - 3.0 * c2 + 2.0 * c2 * c) * a - (1.0 - 3.0 * omc2 + 2.0 * omc2 * omc) * b;
@@ -70,8 +71,8 @@ __device__ __forceinline__ void build_pair_d(double2 *s, int NB, int b, int k, i
 // Row step: 4 row-space arrays in, 2 out.
 // ---------------------------------------------------------------------------
 template <int M>
-__global__ void __launch_bounds__(MRowCfg<M>::NT, MRowCfg<M>::MINB) k_mrow_step(const RunDesc *__restrict__ runs,
-                                                                                const double2 *__restrict__ tw) {
+__global__ void __launch_bounds__(MRowCfg<M>::NT, MRowCfg<M>::MINB)
+    k_mrow_step(const RunDesc *__restrict__ runs, const double2 *__restrict__ tw, const double2 *__restrict__ lt) {
     constexpr int RPC = MRowCfg<M>::RPC, NB = MRowCfg<M>::NB, NT = MRowCfg<M>::NT, H = M / 2;
     extern __shared__ double2 sd[];
     const RunDesc &d = runs[blockIdx.y];
@@ -106,7 +107,7 @@ __global__ void __launch_bounds__(MRowCfg<M>::NT, MRowCfg<M>::MINB) k_mrow_step(
             const int r = w % RPC, m = w / RPC;
             const double2 z1 = sd[spad(m * NB + 2 * r)], z2 = sd[spad(m * NB + 2 * r + 1)];
             const TermsD t =
-                point_terms_d(kc, z1.x * invM + d.psi_mean, z1.y * invM + d.con_mean, z2.x * invM, z2.y * invM);
+                point_terms_d(kc, z1.x * invM + d.psi_mean, z1.y * invM + d.con_mean, z2.x * invM, z2.y * invM, lt);
             out[q] = make_double2(t.inn, t.inc);
             bad |= !(isfinite(t.inn) && isfinite(t.inc));
         }
@@ -171,7 +172,8 @@ __global__ void __launch_bounds__(MRowCfg<M>::NT) k_mrow_forward(const RunDesc *
 // ---------------------------------------------------------------------------
 template <int M>
 __global__ void __launch_bounds__(MRowCfg<M>::NT) k_mrow_analysis(const RunDesc *__restrict__ runs,
-                                                                  const double2 *__restrict__ tw) {
+                                                                  const double2 *__restrict__ tw,
+                                                                  const double2 *__restrict__ lt) {
     constexpr int RPC = MRowCfg<M>::RPC, NT = MRowCfg<M>::NT, H = M / 2;
     constexpr int NB = 3 * RPC;
     extern __shared__ double2 sd[];
@@ -211,7 +213,7 @@ __global__ void __launch_bounds__(MRowCfg<M>::NT) k_mrow_analysis(const RunDesc 
         d.con_real[(size_t)l * M + m] = (float)c;
         const double psi2 = psi * psi;
         const double e_id = psi2 * 0.5 - kc.niu * psi2 * psi * (1.0 / 6.0) + kc.ksi * psi2 * psi2 * (1.0 / 12.0);
-        const double lc = log(c * kc.inv_c0), omc = 1.0 - c, l1c = log(omc * kc.inv_1mc0);
+        const double lc = log_tab(c * kc.inv_c0, lt), omc = 1.0 - c, l1c = log_tab(omc * kc.inv_1mc0, lt);
         const double e_mix = (psi + 1.0) * kc.w * (c * lc + omc * l1c);
         const double c2 = c * c, omc2 = omc * omc;
         const double in3 = -(1.0 - 3.0 * c2 + 2.0 * c2 * c) * a - (1.0 - 3.0 * omc2 + 2.0 * omc2 * omc) * b;
@@ -257,7 +259,7 @@ static cudaError_t mrow_step_impl(const RunDesc *d_runs, int nruns, int L, const
     cudaError_t e = set_smem(k_mrow_step<M>, smem, mask);
     if (nruns == 0 || e != cudaSuccess) return e;
     dim3 grid((L + RPC - 1) / RPC, nruns);
-    k_mrow_step<M><<<grid, NT, smem, st>>>(d_runs, tw.f64[log2i(M)]);
+    k_mrow_step<M><<<grid, NT, smem, st>>>(d_runs, tw.f64[log2i(M)], tw.logt);
     return cudaGetLastError();
 }
 
@@ -283,7 +285,7 @@ static cudaError_t mrow_analysis_impl(const RunDesc *d_runs, int nruns, int L, c
     cudaError_t e = set_smem(k_mrow_analysis<M>, smem, mask);
     if (nruns == 0 || e != cudaSuccess) return e;
     dim3 grid((L + RPC - 1) / RPC, nruns);
-    k_mrow_analysis<M><<<grid, NT, smem, st>>>(d_runs, tw.f64[log2i(M)]);
+    k_mrow_analysis<M><<<grid, NT, smem, st>>>(d_runs, tw.f64[log2i(M)], tw.logt);
     return cudaGetLastError();
 }
 

@@ -54,13 +54,18 @@ struct RunDesc {
     float dt;
     ModelCoefs k;
     C2Params c2a, c2b;
-    // mixed-precision runs (FP32 storage, FP64 arithmetic) only, pure-FP64 operator:
-    //   kmix = (fn/L, an*fn/L, fc/L, ac*fc/L) with an = Mn dt k^2, ac = Mc dt k^2,
-    //          fn = 1/(1 + an), fc = 1/(1 + Mc dt alpha k^4); kc2d = (C2A(k), C2B(k));
-    //   kdl, kdm: the k-vectors in double (lengths L and M)
-    const double4 *kmix;
-    const double2 *kc2d;
+    // mixed-precision runs (FP32 storage, FP64 arithmetic) only, pure-FP64 operator, one
+    // double per k-point in four planes of the column kernel's tile layout (0 at k = 0 and
+    // in the padding columns): kfn = fn*S, kfc = fc*S, kc2a = C2A(k), kc2b = C2B(k), with
+    // fn = 1/(1 + Mn dt k^2), fc = 1/(1 + Mc dt alpha k^4) and S the scale of the
+    // unnormalised inverse transforms (1/L, or 1/(L*M) for a 3-D column view);
+    // mn_dt = Mn dt and mc_dt = Mc dt (the column kernel forms an = mn_dt k^2 and
+    // ac = mc_dt k^2 from the k-vectors); kdl, kdm, kdn: the k-vectors in double, entry
+    // i = s(i) * dkl (dkm, dkn) with s(i) = i for i <= n/2, else i - n, and dk = 2 pi / (n dx)
+    const double *kfn, *kfc, *kc2a, *kc2b;
+    double mn_dt, mc_dt;
     const double *kdl, *kdm, *kdn;
+    double dkl, dkm, dkn;
     // column view of a 3-D run (col3d = 1): the column kernel's tiles are (n-tile t, km)
     // pairs, tile index t*M + km, each L rows x CT columns kn = t*CT + c; col_scale is the
     // inverse-transform scale its set-up mode applies (1/L for 2-D runs, 1/(L*M) for 3-D)
@@ -82,13 +87,16 @@ struct RunDesc {
     int *step_ctr;
 };
 
-// Twiddle tables exp(-2 pi i j / n) for n = 2^1 .. 2^11, FP32 and FP64, and the
+// Twiddle tables exp(-2 pi i j / n) for n = 2^1 .. 2^11, FP32 and FP64, the logarithm
+// table of the mixed path's pointwise terms, and the
 // context's fault word: a device-visible int in mapped pinned host memory that a
 // kernel sets to nonzero when one of its bounded waits gives up (the host reads it
 // after synchronising and reports PFC_E_CUDA).
+constexpr int LOG_TABLE_SIZE = 129;  // breakpoints j = 0 .. 128 of log_tab
 struct TwiddleSet {
     const float2 *f32[12];
     const double2 *f64[12];
+    const double2 *logt;  // log_tab's table (step_common.cuh): (log F_j, 1/F_j), F_j = 1 + j/128
     int *fault;
 };
 
@@ -148,9 +156,10 @@ cudaError_t launch_build_kcoef(const RunDesc *d_run, float2 *kden, float2 *kc2, 
 struct C2ParamsD {
     double kc, e1, e2, k1, k2, gg1, gg2;
 };
-// The mixed-precision table of one run (RunDesc::kmix, kc2d), from its double k-vectors.
+// The mixed-precision table of one run, from its double k-vectors: planes = four planes
+// of T*L*CT doubles (kfn, kfc, kc2a, kc2b in that order; RunDesc's mixed-path fields).
 cudaError_t launch_build_kmix(const RunDesc *d_run, double mn_dt, double mc_dt, double alpha, C2ParamsD a,
-                              C2ParamsD b, double4 *kmix, double2 *kc2d, cudaStream_t s);
+                              C2ParamsD b, double *planes, cudaStream_t s);
 
 // column-kernel modes
 enum ColMode : int { COL_STEP = 0, COL_PREPARE = 1, COL_STEP_CHECKPOINT = 2 };
@@ -174,10 +183,12 @@ struct MPassArgs {
     int L, M, Tn, CT;
 };
 cudaError_t launch_mpass(const MPassArgs &a, bool forward, const TwiddleSet &tw, cudaStream_t s);
-// The 3-D mixed-precision coefficient table in layout B (RunDesc::kmix, kc2d of the column
-// view, scaled by 1/(L*M)), from the double k-vectors kdl, kdm, kdn.
+// y[i] = log_tab(x[i]) (step_common.cuh) for device arrays of n doubles.
+cudaError_t launch_log_selftest(const double *x, double *y, int n, const double2 *tab, cudaStream_t s);
+// The 3-D mixed-precision coefficient table in layout B (the four planes of the column
+// view, fn and fc scaled by 1/(L*M)), from the double k-vectors kdl, kdm, kdn.
 cudaError_t launch_build_kmix3(const RunDesc *d_col, double mn_dt, double mc_dt, double alpha, C2ParamsD a,
-                               C2ParamsD b, double4 *kmix, double2 *kc2d, cudaStream_t s);
+                               C2ParamsD b, double *planes, cudaStream_t s);
 // Row lengths the mixed row kernels take: powers of two 8 ... 2048 (3-D rows of N points
 // as short as 8).
 bool mixed_row_len_ok(int n);

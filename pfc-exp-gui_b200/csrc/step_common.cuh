@@ -38,6 +38,34 @@ __device__ __forceinline__ float c2_ref(const C2Params &p, float ks) {
     return (float)(exp(-(double)p.q2 * (double)p.q2) * exp(-(d * d) / (double)p.gg2));
 }
 
+// Natural logarithm in double for the mixed path's pointwise terms, by the table-driven
+// method of P. T. P. Tang (ACM TOMS 16(4):378-400, 1990): x = 2^e m with m in [1, 2),
+// F = 1 + j/128 the breakpoint nearest m (j = 0 .. 128), and
+//   log x = e ln2 + log F + log1p(r),  r = (m - F) / F,  |r| <= 2^-8,
+// log1p(r) by its Taylor series through r^7 (truncation below 2^-59 relative).  m - F is
+// exact (m and F are within a factor of two); tab[j] = (log F, 1/F) in double, built on
+// the host (LOG_TABLE_SIZE entries).  Absolute error below 3e-16 on [1/2, 2], a few
+// units in the last place elsewhere.  Zero, negative, subnormal, infinite and NaN
+// arguments take log() itself (the IEEE special values the run's non-finite check sees).
+__device__ __forceinline__ double log_tab(double x, const double2 *__restrict__ tab) {
+    if (!(x >= 0x1p-1022 && x <= 0x1.fffffffffffffp+1023)) return log(x);
+    const long long bits = __double_as_longlong(x);
+    const int e = (int)(bits >> 52) - 1023;
+    const long long mant = bits & 0x000fffffffffffffLL;
+    const int j = (int)((mant + (1LL << 44)) >> 45);  // nearest multiple of 2^-7
+    const double m = __longlong_as_double(mant | 0x3ff0000000000000LL);
+    const double2 t = __ldg(tab + j);
+    const double r = (m - (1.0 + (double)j * 0.0078125)) * t.y;
+    double q = 1.0 / 7.0;
+    q = fma(q, r, -1.0 / 6.0);
+    q = fma(q, r, 0.2);
+    q = fma(q, r, -0.25);
+    q = fma(q, r, 1.0 / 3.0);
+    q = fma(q, r, -0.5);
+    const double p = fma(q * r, r, r);  // r + r^2 (-1/2 + r/3 - ...)
+    return fma((double)e, 0.6931471805599453, t.x) + p;
+}
+
 // Row-space element (l, km) of a run: column-tile-major, ((km/CT)*L + l)*CT + km%CT.
 __device__ __forceinline__ long rs_index(const RunDesc &d, int l, int km) {
     return ((long)(km >> d.lct) * d.L + l) * d.CT + (km & (d.CT - 1));

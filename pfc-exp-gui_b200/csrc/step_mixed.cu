@@ -55,8 +55,16 @@ __device__ __forceinline__ double c2_pure(const C2ParamsD &p, double ks) {
     return p.e2 * exp(-(s - p.k2) * (s - p.k2) / p.gg2);
 }
 
+// Plane p of a table of n points: kfn, kfc, kc2a, kc2b (p = 0 .. 3).
+__device__ __forceinline__ void put_kmix(double *planes, long n, long i, double fn, double fc, double c2a, double c2b) {
+    planes[i] = fn;
+    planes[n + i] = fc;
+    planes[2 * n + i] = c2a;
+    planes[3 * n + i] = c2b;
+}
+
 __global__ void k_build_kmix(const RunDesc *__restrict__ run, double mn_dt, double mc_dt, double alpha, C2ParamsD ca,
-                             C2ParamsD cb, double4 *__restrict__ kmix, double2 *__restrict__ kc2d) {
+                             C2ParamsD cb, double *__restrict__ planes) {
     const RunDesc &d = *run;
     const int H = d.M / 2;
     const long tile = (long)d.L * d.CT, total = (long)d.T * tile;
@@ -65,22 +73,19 @@ __global__ void k_build_kmix(const RunDesc *__restrict__ run, double mn_dt, doub
         const int t = (int)(i / tile), rem = (int)(i % tile);
         const int l = rem / d.CT, km = t * d.CT + rem % d.CT;
         if (km > H || (l == 0 && km == 0)) {
-            kmix[i] = make_double4(0.0, 0.0, 0.0, 0.0);
-            kc2d[i] = make_double2(0.0, 0.0);
+            put_kmix(planes, total, i, 0.0, 0.0, 0.0, 0.0);
             continue;
         }
         const double kl = d.kdl[l], kmv = d.kdm[km];
         const double ks = kl * kl + kmv * kmv;
-        const double an = mn_dt * ks, ac = mc_dt * ks, dc = mc_dt * alpha * ks * ks;
-        const double fn = 1.0 / (1.0 + an) * invL, fc = 1.0 / (1.0 + dc) * invL;
-        kmix[i] = make_double4(fn, an * fn, fc, ac * fc);
-        kc2d[i] = make_double2(c2_pure(ca, ks), c2_pure(cb, ks));
+        const double an = mn_dt * ks, dc = mc_dt * alpha * ks * ks;
+        put_kmix(planes, total, i, 1.0 / (1.0 + an) * invL, 1.0 / (1.0 + dc) * invL, c2_pure(ca, ks), c2_pure(cb, ks));
     }
 }
 
 cudaError_t launch_build_kmix(const RunDesc *d_run, double mn_dt, double mc_dt, double alpha, C2ParamsD a,
-                              C2ParamsD b, double4 *kmix, double2 *kc2d, cudaStream_t s) {
-    k_build_kmix<<<148 * 4, 256, 0, s>>>(d_run, mn_dt, mc_dt, alpha, a, b, kmix, kc2d);
+                              C2ParamsD b, double *planes, cudaStream_t s) {
+    k_build_kmix<<<148 * 4, 256, 0, s>>>(d_run, mn_dt, mc_dt, alpha, a, b, planes);
     return cudaGetLastError();
 }
 
@@ -88,7 +93,7 @@ cudaError_t launch_build_kmix(const RunDesc *d_run, double mn_dt, double mc_dt, 
 // row l, column c holds k = (kl, km, kn = t*CT + c), zero at k = 0 and past kn = N/2; the
 // factors carry the 1/(L*M) of the unnormalised l and m inverse transforms.
 __global__ void k_build_kmix3(const RunDesc *__restrict__ run, double mn_dt, double mc_dt, double alpha, C2ParamsD ca,
-                              C2ParamsD cb, double4 *__restrict__ kmix, double2 *__restrict__ kc2d) {
+                              C2ParamsD cb, double *__restrict__ planes) {
     const RunDesc &d = *run;
     const int N = d.N;
     const long tile = (long)d.L * d.CT, total = (long)d.T * tile;
@@ -97,22 +102,31 @@ __global__ void k_build_kmix3(const RunDesc *__restrict__ run, double mn_dt, dou
         const int ti = (int)(i / tile), rem = (int)(i % tile);
         const int tn = ti / d.M, km = ti % d.M, l = rem / d.CT, kn = tn * d.CT + rem % d.CT;
         if (kn > N / 2 || (l == 0 && km == 0 && kn == 0)) {
-            kmix[i] = make_double4(0.0, 0.0, 0.0, 0.0);
-            kc2d[i] = make_double2(0.0, 0.0);
+            put_kmix(planes, total, i, 0.0, 0.0, 0.0, 0.0);
             continue;
         }
         const double kl = d.kdl[l], kmv = d.kdm[km], knv = d.kdn[kn];
         const double ks = kl * kl + kmv * kmv + knv * knv;
-        const double an = mn_dt * ks, ac = mc_dt * ks, dc = mc_dt * alpha * ks * ks;
-        const double fn = 1.0 / (1.0 + an) * scale, fc = 1.0 / (1.0 + dc) * scale;
-        kmix[i] = make_double4(fn, an * fn, fc, ac * fc);
-        kc2d[i] = make_double2(c2_pure(ca, ks), c2_pure(cb, ks));
+        const double an = mn_dt * ks, dc = mc_dt * alpha * ks * ks;
+        put_kmix(planes, total, i, 1.0 / (1.0 + an) * scale, 1.0 / (1.0 + dc) * scale, c2_pure(ca, ks),
+                 c2_pure(cb, ks));
     }
 }
 
 cudaError_t launch_build_kmix3(const RunDesc *d_col, double mn_dt, double mc_dt, double alpha, C2ParamsD a,
-                               C2ParamsD b, double4 *kmix, double2 *kc2d, cudaStream_t s) {
-    k_build_kmix3<<<148 * 4, 256, 0, s>>>(d_col, mn_dt, mc_dt, alpha, a, b, kmix, kc2d);
+                               C2ParamsD b, double *planes, cudaStream_t s) {
+    k_build_kmix3<<<148 * 4, 256, 0, s>>>(d_col, mn_dt, mc_dt, alpha, a, b, planes);
+    return cudaGetLastError();
+}
+
+__global__ void k_log_selftest(const double *__restrict__ x, double *__restrict__ y, int n,
+                               const double2 *__restrict__ tab) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) y[i] = log_tab(x[i], tab);
+}
+
+cudaError_t launch_log_selftest(const double *x, double *y, int n, const double2 *tab, cudaStream_t s) {
+    const int blocks = (n + 255) / 256 < 148 * 8 ? (n + 255) / 256 : 148 * 8;
+    k_log_selftest<<<blocks, 256, 0, s>>>(x, y, n, tab);
     return cudaGetLastError();
 }
 

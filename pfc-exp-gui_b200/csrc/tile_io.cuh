@@ -114,12 +114,22 @@ __device__ __forceinline__ bool stage_try(unsigned bar, unsigned phase, unsigned
 // all threads: wait for completion `phase` (the parity of the number of copies this
 // barrier completed before it) of the copy in flight.  Returns false, the same in every
 // thread of the CTA, when it did not arrive within limit_ns; the fault word is then set
-// and the caller returns.
+// and the caller returns.  A CTA with a second bulk-copy barrier (has_other) also gives
+// a copy in flight on that one a last wait: one of its two phases is the completed
+// previous one and returns at once, the other ends when its copy lands or after
+// STAGE_DRAIN_NS.
 __device__ __forceinline__ bool tile_wait(unsigned bar, unsigned phase, int *fault,
-                                          unsigned long long limit_ns = STAGE_WAIT_NS) {
+                                          unsigned long long limit_ns = STAGE_WAIT_NS, bool has_other = false,
+                                          unsigned other = 0) {
     const bool ok = stage_try(bar, phase, limit_ns);
     if (__syncthreads_or(!ok)) {
-        if (threadIdx.x == 0) *(volatile int *)fault = 1;
+        if (threadIdx.x == 0) {
+            *(volatile int *)fault = 1;
+            if (has_other) {
+                stage_try(other, 0u, STAGE_DRAIN_NS);
+                stage_try(other, 1u, STAGE_DRAIN_NS);
+            }
+        }
         stage_try(bar, phase, STAGE_DRAIN_NS);  // a last, shorter wait for a copy still in flight
         return false;
     }
@@ -128,8 +138,10 @@ __device__ __forceinline__ bool tile_wait(unsigned bar, unsigned phase, int *fau
 
 // ---- the interface the column kernel uses ----
 template <int L, int C, int NT, int STAGE> struct Stager {
-    unsigned bar;  // STAGE_BULK: shared address of the completion barrier
-    float2 *q;     // staging buffer
+    unsigned bar;    // STAGE_BULK: shared address of the completion barrier
+    float2 *q;       // staging buffer
+    bool has_other;  // the CTA has a second bulk-copy barrier, `other`, to drain on a fault
+    unsigned other;
     // all threads, once, before the first copy
     __device__ __forceinline__ void init() const {
         if constexpr (STAGE == STAGE_BULK) stage_init(bar);
@@ -145,7 +157,7 @@ template <int L, int C, int NT, int STAGE> struct Stager {
     // (STAGE_BULK); false, CTA-uniformly, when a bounded wait gave up
     __device__ __forceinline__ bool wait(unsigned phase, int *fault) const {
         if constexpr (STAGE == STAGE_BULK) {
-            return tile_wait(bar, phase, fault);
+            return tile_wait(bar, phase, fault, STAGE_WAIT_NS, has_other, other);
         } else {
             tile_wait_async();
             return true;
@@ -154,6 +166,31 @@ template <int L, int C, int NT, int STAGE> struct Stager {
     // before the CTA exits: no copy outlives it
     __device__ __forceinline__ void finish() const {
         if constexpr (STAGE == STAGE_ASYNC) asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    }
+};
+
+// A shared slot for one plane of a coefficient table tile (n doubles, a contiguous,
+// 16-byte aligned block of 16-byte multiple size), filled by TMA bulk copies that complete
+// on their own barrier (one copy in flight at a time; bounded waits as tile_wait's).
+struct TableStager {
+    unsigned bar;   // shared address of the completion barrier
+    double *t;      // the slot
+    unsigned bytes;
+    unsigned other;  // the input stager's barrier (STAGE_BULK), drained on a fault
+    bool has_other;
+    __device__ __forceinline__ void init() const { stage_init(bar); }
+    // all threads, after every thread's last read of the slot
+    __device__ __forceinline__ void issue(const double *src) const { stage_issue(bar, src, t, bytes); }
+    __device__ __forceinline__ bool wait(unsigned phase, int *fault) const {
+        return tile_wait(bar, phase, fault, STAGE_WAIT_NS, has_other, other);
+    }
+};
+// a transform's hook: fill the table slot once the first stage has read it
+struct TableFetch {
+    TableStager ts;
+    const double *src;
+    __device__ __forceinline__ void operator()() const {
+        if (src) ts.issue(src);
     }
 };
 

@@ -164,6 +164,7 @@ def lib():
         "pfc_col_staging": ([C.c_int, C.c_int, C.c_int, C.c_int, P(C.c_int), fp, fp, P(C.c_int)], C.c_int),
         "pfc_set_col_staging": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
         "pfc_selftest_tile_stage": ([C.c_int, C.c_int, C.c_int, C.c_double, P(C.c_int), P(C.c_int), dp], C.c_int),
+        "pfc_selftest_log": ([C.c_int, dp, dp, C.c_int], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -32,6 +32,47 @@ def fp64_run(model, L, M, precision, **kw):
     return P.Run(P.default_params(model, L=L, M=M, precision=precision, **kw))
 
 
+def device_log(x):
+    import ctypes as C
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.empty_like(x)
+    dp = C.POINTER(C.c_double)
+    rc = P.lib().pfc_selftest_log(0, x.ctypes.data_as(dp), y.ctypes.data_as(dp), len(x))
+    assert rc == P.PFC_OK
+    return y
+
+
+def test_pointwise_log_matches_libm():
+    """The table-driven log of the pointwise terms (Tang's method) against libm: absolute
+    error <= 3e-16 on [1/2, 2] (where c/c0 and (1-c)/(1-c0) live), <= 5e-16 relative
+    elsewhere, the breakpoints and their neighbours included; IEEE special values as log()."""
+    rng = np.random.default_rng(11)
+    j = np.arange(129.0)
+    bp = 1.0 + j / 128.0
+    x = np.concatenate([
+        np.linspace(0.5, 2.0, 300001), 1.0 + rng.uniform(-1e-3, 1e-3, 100000),
+        1.0 + rng.uniform(-1e-12, 1e-12, 10000), 10.0 ** rng.uniform(-307, 307, 200000),
+        bp, np.nextafter(bp, 0.0), np.nextafter(bp, 3.0), bp + 1.0 / 256.0, np.nextafter(bp + 1.0 / 256.0, 0.0),
+        [np.finfo(np.float64).tiny, np.finfo(np.float64).max, 1.0, np.nextafter(1.0, 0.0), np.nextafter(1.0, 2.0)]])
+    y = device_log(x)
+    ref = np.log(x)
+    err = np.abs(y - ref)
+    inside = (x >= 0.5) & (x <= 2.0)
+    print(f"log: max abs error on [1/2, 2] {err[inside].max():.2e}; "
+          f"max relative error elsewhere {(err[~inside] / np.abs(ref[~inside])).max():.2e}")
+    assert err[inside].max() <= 3e-16
+    assert np.all(err[~inside] <= 5e-16 * np.abs(ref[~inside]))
+    assert y[x == 1.0][0] == 0.0
+    special = np.array([0.0, -0.0, -1.0, np.inf, -np.inf, np.nan, 5e-324, 1e-310])
+    ys = device_log(special)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        rs = np.log(special)
+    assert np.array_equal(np.isnan(ys), np.isnan(rs))
+    inf, fin = np.isinf(rs), np.isfinite(rs)
+    assert np.array_equal(ys[inf], rs[inf])
+    assert np.all(np.abs(ys[fin] - rs[fin]) <= 5e-16 * np.abs(rs[fin]))
+
+
 def test_mixed_is_the_default_precision():
     assert P.default_params(P.MODEL_MISFIT).precision == P.MIXED
     assert P.default_params(P.MODEL_CVD).precision == P.MIXED
