@@ -51,6 +51,8 @@ def parse(argv=None):
     ap.add_argument("--serve-requests", type=int, default=48)
     ap.add_argument("--no-cvd3d", action="store_true", help="skip the 3-D CVD (256x256x64) step measurement")
     ap.add_argument("--no-elastic", action="store_true", help="skip the Elastic Analysis measurement")
+    ap.add_argument("--no-fp32-path", action="store_true",
+                    help="skip the same batch on the FP32-arithmetic fused path")
     ap.add_argument("--tile-width", type=int, default=0,
                     help="fix the column tile width instead of the autotuner's choice (reproducible profiles)")
     ap.add_argument("--staging", choices=["auto", "async", "bulk"], default="auto",
@@ -506,11 +508,12 @@ def run_ours(args):
     dev = dist.local
     G, B = args.grid, args.batch
     prec = P.MIXED
-    if args.tile_width:
-        P.set_tile_width(G, G, args.tile_width, device=dev, precision=prec)
-    if args.staging != "auto":
-        P.set_col_staging(G, G, P.STAGE_ASYNC if args.staging == "async" else P.STAGE_BULK, device=dev,
-                          precision=prec)
+    for pr in (P.MIXED, P.FP32):  # both fused paths: a pinned width or staging skips their autotuner
+        if args.tile_width:
+            P.set_tile_width(G, G, args.tile_width, device=dev, precision=pr)
+        if args.staging != "auto":
+            P.set_col_staging(G, G, P.STAGE_ASYNC if args.staging == "async" else P.STAGE_BULK, device=dev,
+                              precision=pr)
     runs = []
     for i in range(B):
         p = P.default_params(P.MODEL_MISFIT, L=G, M=G, N=1, seed=1000 + i + 100000 * dist.rank, device=dev,
@@ -598,22 +601,23 @@ def run_ours(args):
     batch.close()
     for r in runs:
         r.close()
-    # the FP32-arithmetic fused path on the same batch (faster, but 7e-5 from pure FP64 after
-    # 200 steps at 1024^2, outside the 1e-5 bound)
-    runs32 = [P.Run(P.default_params(P.MODEL_MISFIT, L=G, M=G, seed=1000 + i, device=dev, precision=P.FP32))
-              for i in range(B)]
-    b32 = P.Batch(runs32)
-    b32.advance(5)
-    ms32 = b32.advance_timed(min(args.steps, 200))
-    k32 = step_roofline(P, b32, G, B, {"row": "k_row_step", "col": "k_col_step"})
-    line["fp32_path"] = {"run_steps_per_s": round(B * min(args.steps, 200) / (ms32 / 1000.0), 2),
-                         "ms_per_step": round(ms32 / min(args.steps, 200), 5),
-                         "column_tile_width": P.tile_width(G, G, device=dev, precision=P.FP32)[0],
-                         "per_kernel": {"k_row_step": k32["row"], "k_col_step": k32["col"]},
-                         "what": "the same batch on the FP32-arithmetic path (opt-in --precision fp32)"}
-    b32.close()
-    for r in runs32:
-        r.close()
+    if not args.no_fp32_path:
+        # the FP32-arithmetic fused path on the same batch (faster, but 7e-5 from pure FP64 after
+        # 200 steps at 1024^2, outside the 1e-5 bound)
+        runs32 = [P.Run(P.default_params(P.MODEL_MISFIT, L=G, M=G, seed=1000 + i, device=dev, precision=P.FP32))
+                  for i in range(B)]
+        b32 = P.Batch(runs32)
+        b32.advance(5)
+        ms32 = b32.advance_timed(min(args.steps, 200))
+        k32 = step_roofline(P, b32, G, B, {"row": "k_row_step", "col": "k_col_step"})
+        line["fp32_path"] = {"run_steps_per_s": round(B * min(args.steps, 200) / (ms32 / 1000.0), 2),
+                             "ms_per_step": round(ms32 / min(args.steps, 200), 5),
+                             "column_tile_width": P.tile_width(G, G, device=dev, precision=P.FP32)[0],
+                             "per_kernel": {"k_row_step": k32["row"], "k_col_step": k32["col"]},
+                             "what": "the same batch on the FP32-arithmetic path (opt-in --precision fp32)"}
+        b32.close()
+        for r in runs32:
+            r.close()
     # the plain FP64 GPU path (one run, the reference's step structure) on the same grid
     if not args.no_fp64_plain:
         r64 = P.Run(P.default_params(P.MODEL_MISFIT, L=G, M=G, N=1, seed=1000, device=dev, precision=P.FP64))
@@ -632,8 +636,9 @@ def run_ours(args):
                               "roofline": {"bound": "hbm", "achieved": round(ach64, 1),
                                            "frac": round(ach64 / peak, 4),
                                            "algorithmic_bytes_per_step": fp64_bytes},
-                              "batched_over_fp64_plain": round(value / dist.world / fp64_sps, 2),
-                              "fp32_path_over_fp64_plain": round(line["fp32_path"]["run_steps_per_s"] / fp64_sps, 2)}
+                              "batched_over_fp64_plain": round(value / dist.world / fp64_sps, 2)}
+        if "fp32_path" in line:
+            line["fp64_plain"]["fp32_path_over_fp64_plain"] = round(line["fp32_path"]["run_steps_per_s"] / fp64_sps, 2)
     # the 3-D CVD workload (256 x 256 x 64): the mixed path (four sweeps per step: row
     # kernel along n, m-axis pass, column kernel along l, inverse m-axis pass) and the
     # plain FP64 path

@@ -102,6 +102,24 @@ def test_3d_set_fields_roundtrip():
     assert np.abs(r.fields()[0] - o.fields()[0]).max() <= 1e-6
 
 
+def test_3d_creation_sequences():
+    """The run creations on which an earlier, since removed, 3-D build faulted: a first
+    run at 64 x 64 x 32, and 256 x 128 x 64 after a 128 x 128 x 64 run was created,
+    stepped and destroyed (the index arithmetic of all four kernels is replayed on the
+    CPU for these shapes in test_index_replay.py).  Each steps, keeps its mass and has
+    finite fields."""
+    for shape in ((64, 64, 32), (128, 128, 64), (256, 128, 64)):
+        r = run3(*shape)
+        m0 = r.means()
+        r.advance(5, analysis=True)
+        phi, con = r.fields_f32()
+        assert np.isfinite(phi).all() and np.isfinite(con).all()
+        assert r.means() == m0
+        e, _ = r.energy()
+        assert np.isfinite(e)
+        r.close()
+
+
 def test_3d_fused_limits():
     with pytest.raises(P.PfcError):
         run3(64, 64, 16, precision=P.FP32)  # the FP32 path is 2-D
