@@ -467,7 +467,28 @@ def step_roofline(P, batch, G, B, names, reps=20):
         prof = profiled_kernel(names[name])
         if prof and prof.get("fp64_pipe_active_pct") is not None:
             out[name]["fp64_pipe_active_pct_profiled"] = prof["fp64_pipe_active_pct"]
+        n64 = (prof or {}).get("fp64_warp_insts_per_run", {}).get(str(G))
+        if n64:
+            # FP64 pipe: 2 warp instructions per cycle per SM (64 lanes); peak at the clock seen
+            sms, mhz = sm_info()
+            ach = n64 * B / (ms_k / 1000.0)
+            peak = 2.0 * sms * mhz * 1e6
+            out[name]["fp64_pipe"] = {"warp_insts_per_launch": n64 * B, "achieved_warp_insts_per_s": round(ach, 0),
+                                      "peak_warp_insts_per_s": round(peak, 0), "frac": round(ach / peak, 4),
+                                      "clock_mhz": mhz}
     return out
+
+
+def sm_info():
+    """SM count and the SM clock (MHz) the FP64 roofline is taken at: the median clock
+    sampled during the timed region when known, else the device's maximum."""
+    import torch
+    props = torch.cuda.get_device_properties(torch.cuda.current_device())
+    mhz = _CLOCK_SEEN.get("sm_mhz") or _CLOCK_SEEN.get("sm_max_mhz") or 1965.0
+    return props.multi_processor_count, float(mhz)
+
+
+_CLOCK_SEEN = {}
 
 
 def elastic_bench(P, dev, G=1024, steps=500):
@@ -528,6 +549,8 @@ def run_ours(args):
     clocks.start()
     ms = batch.advance_timed(args.steps)
     clk = clocks.stop()
+    if isinstance(clk, dict):
+        _CLOCK_SEEN.update({k: clk.get(k) for k in ("sm_mhz", "sm_max_mhz")})
     ms_max = dist.max(ms)
     total_run_steps = dist.sum(B * args.steps)
     value = total_run_steps / (ms_max / 1000.0)
@@ -598,6 +621,10 @@ def run_ours(args):
         "gpu_launches": 2 * args.steps,
         "clocks": clk,
     }
+    if "fp64_pipe" in kern[dom]:
+        # the mixed kernels compute in FP64: the bound that holds them is the FP64 pipe's issue
+        # rate (and its latency), which this fraction reports beside the HBM one
+        line["roofline"]["fp64_pipe"] = kern[dom]["fp64_pipe"]
     batch.close()
     for r in runs:
         r.close()
