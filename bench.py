@@ -471,10 +471,10 @@ def step_roofline(P, batch, G, B, names, reps=20):
         if n64:
             # FP64 pipe: 2 warp instructions per cycle per SM (64 lanes); peak at the clock seen
             sms, mhz = sm_info()
-            ach = n64 * B / (ms_k / 1000.0)
-            peak = 2.0 * sms * mhz * 1e6
-            out[name]["fp64_pipe"] = {"warp_insts_per_launch": n64 * B, "achieved_warp_insts_per_s": round(ach, 0),
-                                      "peak_warp_insts_per_s": round(peak, 0), "frac": round(ach / peak, 4),
+            ach64 = n64 * B / (ms_k / 1000.0)
+            peak64 = 2.0 * sms * mhz * 1e6
+            out[name]["fp64_pipe"] = {"warp_insts_per_launch": n64 * B, "achieved_warp_insts_per_s": round(ach64, 0),
+                                      "peak_warp_insts_per_s": round(peak64, 0), "frac": round(ach64 / peak64, 4),
                                       "clock_mhz": mhz}
     return out
 
