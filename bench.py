@@ -653,9 +653,10 @@ def run_ours(args):
         ms64 = r64.advance_timed(n64)
         r64.close()
         fp64_sps = n64 / (ms64 / 1000.0)
-        # 13 complex-double 3-D DFTs per step, each 3 axis passes reading and writing 16 B per
-        # point, plus the pointwise kernels' 14 reads and writes of complex doubles per point
-        fp64_bytes = G * G * (13 * 3 * 2 * 16 + 14 * 16)
+        # 13 complex-double 3-D DFTs per step, each one pass per axis of length > 1 (two on a
+        # 2-D grid) reading and writing 16 B per point, plus the pointwise kernels' 14 reads
+        # and writes of complex doubles per point
+        fp64_bytes = G * G * (13 * 2 * 2 * 16 + 14 * 16)
         ach64 = fp64_bytes / (ms64 / n64 / 1000.0) / 1e9
         line["fp64_plain"] = {"steps_per_s": round(fp64_sps, 2), "ms_per_step": round(ms64 / n64, 4),
                               "what": "one Misfit run, plain FP64 path (13 complex-double 3-D DFTs + pointwise "
@@ -666,6 +667,18 @@ def run_ours(args):
                               "batched_over_fp64_plain": round(value / dist.world / fp64_sps, 2)}
         if "fp32_path" in line:
             line["fp64_plain"]["fp32_path_over_fp64_plain"] = round(line["fp32_path"]["run_steps_per_s"] / fp64_sps, 2)
+    # one run alone (the single-run form of the 1024^2 workload): what a single simulation
+    # gets, against the batch's per-run share
+    if not args.no_fp64_plain:
+        r1 = P.Run(P.default_params(P.MODEL_MISFIT, L=G, M=G, N=1, seed=1000, device=dev, precision=P.MIXED))
+        r1.advance(5)
+        n1 = 200
+        ms1 = r1.advance_timed(n1)
+        r1.close()
+        sps1 = n1 / (ms1 / 1000.0)
+        line["single_run"] = {"steps_per_s": round(sps1, 2), "ms_per_step": round(ms1 / n1, 4),
+                              "over_fp64_plain": round(sps1 / line["fp64_plain"]["steps_per_s"], 2),
+                              "what": "one Misfit 1024^2 run on the mixed path, CUDA events over 200 steps"}
     # the 3-D CVD workload (256 x 256 x 64): the mixed path (four sweeps per step: row
     # kernel along n, m-axis pass, column kernel along l, inverse m-axis pass) and the
     # plain FP64 path
