@@ -727,7 +727,7 @@ extern "C" int pfc_run_create(const pfc_run_params *p, pfc_run **out) { return r
 // speed, not results.  On the first run of a grid and precision on a device, each
 // candidate width (the default, a quarter, half and twice it, where the tile fits:
 // col_tile_candidates, mixed_col_tile_candidates) runs a batch of Misfit runs of at
-// least 2 M points in all (4 to 16 runs) with each staging method: 3 warm-up steps,
+// least 8 M points in all (4 to 16 runs) with each staging method: 3 warm-up steps,
 // then 8 steps of the row and column sweeps timed with CUDA events.  The fastest pair
 // is kept for the rest of the process.  PFC_AUTOTUNE=0 in the environment keeps the
 // default width with bulk-copy staging; pfc_set_tile_width and pfc_set_col_staging fix
@@ -750,10 +750,13 @@ static std::mutex g_tile_mu;
 static std::map<std::tuple<int, int, int, int>, TileChoice> g_tile;  // (device, L, M, precision)
 
 // Device time of 8 steps of a trial batch with tile width ct, for each staging method
-// (ms[COL_STAGE_ASYNC], ms[COL_STAGE_BULK]).
+// (ms[COL_STAGE_ASYNC], ms[COL_STAGE_BULK]).  The batch holds at least 8 M points (8 runs
+// at 1024^2, 4 to 16 runs): with fewer, the wide tiles' column kernel (one CTA per SM)
+// has too few items per CTA, and the trial would rank the widths differently from the
+// batches it tunes for.
 static int time_tile_width(int device, int L, int M, int prec, int ct, float ms[2]) {
     const long pts = (long)L * M;
-    const int nruns = (int)std::max(4L, std::min(16L, (2L << 20) / pts));
+    const int nruns = (int)std::max(4L, std::min(16L, (8L << 20) / pts));
     std::vector<pfc_run *> runs;
     int rc = PFC_OK;
     for (int i = 0; i < nruns && rc == PFC_OK; ++i) {

@@ -11,7 +11,7 @@
 namespace pfc {
 
 template <int M> struct MRowCfg {
-    static constexpr int RPC = (MROW_TILE / 2) / M >= 1 ? (MROW_TILE / 2) / M : 1;  // rows per CTA
+    static constexpr int RPC = mrow_rpc(M);  // rows per CTA
     static constexpr int NB = 2 * RPC;
     static constexpr int NT = (NB * M / 16) < 512 ? (NB * M / 16) : 512;  // one radix-16 butterfly per thread
     static constexpr int MINB = 512 / NT;  // 128 registers per thread

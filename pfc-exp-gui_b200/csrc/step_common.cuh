@@ -19,6 +19,12 @@ constexpr bool col_tile_ok(int L, int C) { return C >= 1 && C <= COL_TILE_MAX &&
 // complex values (its shared buffers hold double2).
 constexpr bool mcol_tile_ok(int L, int C) { return C >= 1 && C <= COL_TILE_MAX && C * L >= 512 && C * L <= 4096; }
 constexpr int MROW_TILE = 2048;  // complex doubles per mixed row-kernel CTA (row step: 2 sequences per row)
+// Rows per mixed row-kernel CTA: MROW_TILE/2 points of rows, and at least two rows up to
+// M = 1024, so that a CTA's loads of a width-2 column tile are whole 32-byte sectors.
+constexpr int mrow_rpc(int M) {
+    const int a = (MROW_TILE / 2) / M, b = 2048 / M < 2 ? 2048 / M : 2;
+    return a > b ? a : (b > 1 ? b : 1);
+}
 
 template <int L, int C> struct ColCfg {
     static constexpr int NT = (C * L / 16) < 32 ? 32 : (C * L / 16);

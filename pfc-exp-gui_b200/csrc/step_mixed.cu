@@ -21,7 +21,8 @@
 // The k = 0 modes stay in FP64 per run, as on the FP32 path.
 //
 // HBM traffic is that of the FP32 path, 56 bytes per grid point per step.  Shared
-// memory holds double2 values, so the tiles are half as long (MROW_TILE, MCOL_TILE).
+// memory holds double2 values, so the tiles are half as long (MROW_TILE, MCOL_TILE),
+// except that a row-kernel CTA takes two rows of M = 1024 (mrow_rpc).
 // Column-kernel work items are ordered tile-major (all runs of one tile, then the next
 // tile) and each CTA takes a contiguous range, so a tile of the shared coefficient
 // table is read once from HBM and then from L2 by the other runs of a batch.
@@ -180,8 +181,7 @@ cudaError_t prepare_rows_mixed(int M) {
 }
 
 int analysis_partials_mixed(int L, int M) {
-    int rpc = (MROW_TILE / 2) / M;
-    if (rpc < 1) rpc = 1;
+    const int rpc = mrow_rpc(M);
     return (L + rpc - 1) / rpc;
 }
 

@@ -60,7 +60,7 @@ def test_row_kernels_stay_inside_layout_a(L, M, N):
     assert ct >= 1
     R, H = L * M, N // 2
     lct = ct.bit_length() - 1
-    rpc = max(1, (MROW_TILE // 2) // N)
+    rpc = max((MROW_TILE // 2) // N, min(2, 2048 // N), 1)  # mrow_rpc (step_common.cuh)
     lrpc = rpc.bit_length() - 1
     nt = min(2 * rpc * N // 16, 512)
     grid = -(-R // rpc)
