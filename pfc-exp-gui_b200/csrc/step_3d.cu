@@ -20,38 +20,77 @@ namespace pfc {
 
 template <int M, int C> struct MPassCfg {
     static constexpr int NT = (M * C / 16) < 32 ? 32 : (M * C / 16);  // one radix-16 butterfly per thread
+    // padded double2 transform buffer + the unpadded FP32 staging buffer
+    static constexpr int SMEM = (int)sizeof(double2) * padded_len<M * C>::value + (int)sizeof(float2) * M * C;
+    static constexpr int FIT = (228 * 1024) / (SMEM + 1024);  // CTAs per SM the shared memory leaves room for
+    static constexpr int MINB = FIT > 4 ? 4 : (FIT < 1 ? 1 : FIT);
 };
 
+__device__ __forceinline__ void mpass_cp8(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
+// All threads: start the copies of item `item` into the staging buffer q, one commit
+// group.  Forward: the A block, contiguous.  Inverse: the item's CT-value chunk of every
+// km of layout B.  Element m of sequence c lands at m*C + c, the transform's input order.
+template <int M, int C, int NT, bool FWD>
+__device__ __forceinline__ void mpass_issue(const MPassArgs &a, long item, float2 *q) {
+    const long per_arr = (long)a.Tn * a.L;
+    const int arr = (int)(item / per_arr);
+    const int rem = (int)(item % per_arr);
+    const int t = rem / a.L, l = rem % a.L;
+    const float2 *src = a.src[arr];
+    if (FWD) {
+        const float2 *g = src + ((long)t * a.L + l) * M * C;
+        for (int i = threadIdx.x; i < M * C / 2; i += NT) cp_async16(q + 2 * i, g + 2 * i);
+    } else if (C >= 2) {  // 16-byte pieces within a chunk (C is even)
+        for (int i = threadIdx.x; i < M * C / 2; i += NT) {
+            const int e = 2 * i, km = e / C, c = e % C;
+            cp_async16(q + e, src + (((long)t * M + km) * a.L + l) * C + c);
+        }
+    } else {
+        for (int i = threadIdx.x; i < M; i += NT) mpass_cp8(q + i, src + ((long)t * M + i) * a.L + l);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+// a transform's hook: start the next item's copies once the first stage has read q
+template <int M, int C, int NT, bool FWD> struct MPassPrefetch {
+    const MPassArgs *a;
+    long next, items;
+    float2 *q;
+    __device__ __forceinline__ void operator()() const {
+        if (next < items) mpass_issue<M, C, NT, FWD>(*a, next, q);
+    }
+};
+
+// Persistent over items (array, t, l): the item's input is staged (FP32) by cp.async into
+// q, which the transform's first stage reads directly; the next item's copies are issued
+// as soon as that stage has read q, so they stream in while the transform and the
+// output stores of this item run.
 template <int M, int C, bool FWD>
-__global__ void __launch_bounds__(MPassCfg<M, C>::NT) k_mpass(MPassArgs a, const double2 *__restrict__ tw) {
+__global__ void __launch_bounds__(MPassCfg<M, C>::NT, MPassCfg<M, C>::MINB)
+    k_mpass(MPassArgs a, const double2 *__restrict__ tw) {
     constexpr int NT = MPassCfg<M, C>::NT;
-    extern __shared__ double2 sd[];
-    const int L = a.L, Tn = a.Tn;
-    const long per_arr = (long)Tn * L, items = (long)a.narr * per_arr;
-    for (long item = blockIdx.x; item < items; item += gridDim.x) {
+    typedef RegOut<M, C, NT, double2> RO;
+    extern __shared__ __align__(16) double2 sd[];
+    float2 *q = reinterpret_cast<float2 *>(sd + padded_len<M * C>::value);  // 16-byte aligned
+    const int L = a.L;
+    const long per_arr = (long)a.Tn * L, items = (long)a.narr * per_arr;
+    long item = blockIdx.x;
+    if (item >= items) return;
+    double2 last[RO::PER_T][RO::R];
+    mpass_issue<M, C, NT, FWD>(a, item, q);
+    for (; item < items; item += gridDim.x) {
         const int arr = (int)(item / per_arr);
         const int rem = (int)(item % per_arr);
         const int t = rem / L, l = rem % L;
-        const float2 *__restrict__ src = a.src[arr];
         float2 *__restrict__ dst = a.dst[arr];
-        const long blockA = ((long)t * L + l) * M * C;  // the (t, l) tile in layout A
-        __syncthreads();  // the previous item's stores have read sd
-        if (FWD) {
-            const float4 *g = reinterpret_cast<const float4 *>(src + blockA);
-            for (int i = threadIdx.x; i < M * C / 2; i += NT) {
-                const float4 v = g[i];
-                sd[spad(2 * i)] = make_double2(v.x, v.y);
-                sd[spad(2 * i + 1)] = make_double2(v.z, v.w);
-            }
-        } else {
-            for (int i = threadIdx.x; i < M * C; i += NT) {
-                const int km = i / C, c = i % C;
-                const float2 v = src[(((long)t * M + km) * L + l) * C + c];
-                sd[spad(i)] = make_double2(v.x, v.y);
-            }
-        }
-        __syncthreads();
-        fft_smem<M, C, NT, FWD>(sd, tw);  // sequences c interleaved: element m of c at m*C + c
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        __syncthreads();  // every thread's copies have landed; the previous item's stores have read sd
+        // sequences c interleaved: element m of c at m*C + c
+        fft<M, C, NT, FWD, SP_GLOBAL, SP_SMEM>(q, sd, sd, tw, last, Identity(),
+                                               MPassPrefetch<M, C, NT, FWD>{&a, item + gridDim.x, items, q});
         if (FWD) {
             for (int i = threadIdx.x; i < M * C; i += NT) {
                 const int km = i / C, c = i % C;
@@ -59,24 +98,25 @@ __global__ void __launch_bounds__(MPassCfg<M, C>::NT) k_mpass(MPassArgs a, const
                 dst[(((long)t * M + km) * L + l) * C + c] = make_float2((float)v.x, (float)v.y);
             }
         } else {
-            float4 *g = reinterpret_cast<float4 *>(dst + blockA);
+            float4 *g = reinterpret_cast<float4 *>(dst + ((long)t * L + l) * M * C);
             for (int i = threadIdx.x; i < M * C / 2; i += NT) {
                 const double2 u = sd[spad(2 * i)], v = sd[spad(2 * i + 1)];
                 g[i] = make_float4((float)u.x, (float)u.y, (float)v.x, (float)v.y);
             }
         }
     }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");  // the last item issues no copy
 }
 
 template <int M, int C>
 static cudaError_t mpass_impl(const MPassArgs &a, bool fwd, const TwiddleSet &tw, cudaStream_t s) {
     constexpr int NT = MPassCfg<M, C>::NT;
-    constexpr size_t smem = sizeof(double2) * padded_len<M * C>::value;
+    constexpr size_t smem = MPassCfg<M, C>::SMEM;
     static unsigned mask_f = 0, mask_i = 0;
     cudaError_t e = fwd ? set_smem(k_mpass<M, C, true>, smem, mask_f) : set_smem(k_mpass<M, C, false>, smem, mask_i);
     if (e != cudaSuccess) return e;
     const long items = (long)a.narr * a.Tn * a.L;
-    const long cap = 8L * sm_count();
+    const long cap = (long)MPassCfg<M, C>::MINB * sm_count();
     const unsigned grid = (unsigned)(items < cap ? items : cap);
     if (fwd)
         k_mpass<M, C, true><<<grid, NT, smem, s>>>(a, tw.f64[log2i(M)]);
@@ -85,7 +125,7 @@ static cudaError_t mpass_impl(const MPassArgs &a, bool fwd, const TwiddleSet &tw
     return cudaGetLastError();
 }
 
-// M * C <= 4096 complex doubles (69.6 KB of padded shared memory per CTA)
+// M * C <= 4096 complex doubles (101.6 KB of shared memory per CTA with the staging buffer)
 template <int M>
 static cudaError_t mpass_width(const MPassArgs &a, bool fwd, const TwiddleSet &tw, cudaStream_t s) {
     switch (a.CT) {

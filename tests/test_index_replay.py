@@ -111,7 +111,14 @@ def test_m_axis_passes_map_layout_a_onto_layout_b(L, M, N):
     assert np.array_equal(np.sort(src_a.ravel()), np.arange(E))
     assert np.array_equal(np.sort(dst_b.ravel()), np.arange(E))
     assert spad(M * ct - 1) < padded_len(M * ct)
-    assert 16 * padded_len(M * ct) <= 227 * 1024
+    # the padded transform buffer, then the unpadded FP32 staging buffer (16-byte aligned)
+    assert (16 * padded_len(M * ct)) % 16 == 0
+    assert 16 * padded_len(M * ct) + 8 * M * ct <= 227 * 1024
+    # the inverse pass's staged copies: CT-value chunks of B, 16-byte pieces when CT is even
+    if ct >= 2:
+        e = np.arange(0, M * ct, 2)
+        src = ((0 * M + e // ct) * L + 0) * ct + e % ct
+        assert (src % 2 == 0).all() and (e // ct == (e + 1) // ct).all()
 
 
 @pytest.mark.parametrize("L,M,N", SHAPES)
