@@ -9,10 +9,12 @@
 //     the semi-implicit update with k^2 = kl^2 + km^2 + kn^2 (the 3-D table);
 //   this kernel, inverse: psi', con', c2a, c2b (and the gradients at checkpoints), B -> A.
 // Layouts (pfc_internal.h, MPassArgs): A puts each (t, l) M x CT tile in one block, B each
-// (t, km) L x CT tile.  A work item is one (array, t, l): the A block is read (or the B
-// chunks of CT values gathered), transformed along m in shared memory in FP64, and written
-// as CT-value chunks of B (or as the contiguous A block).  The inverse is unnormalised;
-// the 1/(L*M) of both l and m inverses is folded into the column kernel's factors.
+// (t, km) L x CT tile.  A work item is one (array, t, l): the A block is copied (or the B
+// chunks of CT values gathered) by cp.async into an FP32 staging buffer, transformed along
+// m in FP64 (the first stage reads the staging buffer, shared memory holds the rest), and
+// written as CT-value chunks of B (or as the contiguous A block); the next item's copies
+// run behind the current transform.  The inverse is unnormalised; the 1/(L*M) of both l
+// and m inverses is folded into the column kernel's factors.
 #include "pfc_b200.h"
 #include "step_common.cuh"
 

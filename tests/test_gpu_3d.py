@@ -36,7 +36,8 @@ def test_3d_initial_condition_matches_oracle():
     assert np.array_equal(con, ocon.astype(np.float32))
 
 
-@pytest.mark.parametrize("L,M,N,steps", [(64, 64, 16, 20), (32, 32, 8, 20), (128, 128, 64, 20), (64, 128, 32, 10)])
+@pytest.mark.parametrize("L,M,N,steps", [(64, 64, 16, 20), (32, 32, 8, 20), (128, 128, 64, 20), (64, 128, 32, 10),
+                                         (2048, 32, 16, 5)])
 def test_3d_mixed_matches_pure_fp64_oracle(L, M, N, steps):
     r = run3(L, M, N)
     o = O.Run(O.default_params(O.MODEL_CVD, L=L, M=M, N=N, exact=0))

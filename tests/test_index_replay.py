@@ -51,7 +51,9 @@ def geometry(L, M, N):
     return ct, hp, hp // ct, L * M * hp
 
 
-SHAPES = [(64, 64, 32), (128, 128, 64), (256, 128, 64), (256, 256, 64), (32, 32, 8), (64, 128, 32), (128, 64, 16)]
+# the last two run at column tile widths 16 and 1 (the inverse m-axis pass's 8-byte copies)
+SHAPES = [(64, 64, 32), (128, 128, 64), (256, 128, 64), (256, 256, 64), (32, 32, 8), (64, 128, 32), (128, 64, 16),
+          (32, 64, 16), (2048, 32, 16)]
 
 
 @pytest.mark.parametrize("L,M,N", SHAPES)
