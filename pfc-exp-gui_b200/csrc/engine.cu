@@ -747,7 +747,9 @@ struct TileChoice {
     }
 };
 static std::mutex g_tile_mu;
-static std::map<std::tuple<int, int, int, int>, TileChoice> g_tile;  // (device, L, M, precision)
+// (device, L, M, precision) of 2-D grids; a 3-D run takes tile_width_3d(L, M) and never
+// consults it
+static std::map<std::tuple<int, int, int, int>, TileChoice> g_tile;
 
 // Device time of 8 steps of a trial batch with tile width ct, for each staging method
 // (ms[COL_STAGE_ASYNC], ms[COL_STAGE_BULK]).  The batch holds at least 8 M points (8 runs
