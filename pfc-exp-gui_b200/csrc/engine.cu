@@ -528,7 +528,7 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
     int ct = tile_default(p->L, p->precision), stage = COL_STAGE_BULK;
     if (d3) {
         ct = tile_width_3d(p->L, p->M);
-        stage = COL_STAGE_ASYNC;
+        stage = COL_STAGE_BULK;  // 1 % faster than cp.async at 256 x 256 x 64
     } else if (fused) {
         if (ct_force > 0) {
             ct = ct_force;
