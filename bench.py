@@ -320,7 +320,29 @@ def drain_engine(P, eng, n, timeout_s=900.0):
 PREC_NAMES = {0: "fp32", 1: "fp64", 2: "fp64-pure", 3: "mixed"}
 
 
-def sweep_bench(P, dev, precision, nruns=64, steps=2000, master_seed=4242, reps=3):
+def cpu_sweep_estimate(grids, steps, extra=3):
+    """The sweep as the GUI runs it on the CPU: the reference program once per run, one
+    after another (MainWindow.cpp:3453-3522).  Each grid's binary is timed once with 1 and
+    once with 1+extra steps; a run costs time(1 step) + (steps - 1) x the per-step time.
+    None when a grid's reference binary is missing."""
+    import tempfile
+    per = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for g in grids:
+            exe = ref_binary(g)
+            if exe is None:
+                return None
+            t1 = time_reference_process(exe, 1, os.path.join(tmp, f"g{g}_1"))
+            tn = time_reference_process(exe, 1 + extra, os.path.join(tmp, f"g{g}_n"))
+            per[g] = (t1, (tn - t1) / extra)
+    total = sum(n * (per[g][0] + (steps - 1) * per[g][1]) for g, n in grids.items())
+    return {"estimate_s": round(total, 1), "runs_per_hour": round(sum(grids.values()) / total * 3600.0, 2),
+            "step_s": {f"{g}^2": round(v[1], 5) for g, v in sorted(per.items())},
+            "sample": f"each grid's reference pfc-exp-cli (built from its sources; FFTW unavailable, project "
+                      f"FFTW-API shim FFT) timed once at 1 and once at {1 + extra} steps on one core"}
+
+
+def sweep_bench(P, dev, precision, nruns=64, steps=2000, master_seed=4242, reps=3, cpu_reference=False):
     """64 Misfit runs of mixed grids {128, 256, 512}^2, u0 and con0 from the GUI's value
     lists, drawn with splitmix64 from a master seed; 2000 steps, one checkpoint (mod 2000),
     at the given precision.  Timed as one engine sweep (all submitted at once) and as
@@ -369,7 +391,9 @@ def sweep_bench(P, dev, precision, nruns=64, steps=2000, master_seed=4242, reps=
     grids = {}
     for p in jobs:
         grids[p.L] = grids.get(p.L, 0) + 1
+    cpu = cpu_sweep_estimate(grids, steps) if cpu_reference else None
     return {"runs": nruns, "steps": steps, "precision": PREC_NAMES[precision],
+            **({"cpu_reference_sequential": cpu} if cpu else {}),
             "grids": {f"{g}^2": n for g, n in sorted(grids.items())},
             "master_seed": master_seed,
             "batched_s": round(wall_b, 3), "sequential_gpu_s": round(wall_s, 3),
@@ -724,7 +748,7 @@ def run_ours(args):
     if not args.no_sweep:
         # the sweep workload names FP32 arithmetic with FP64 reductions (the FP32 path);
         # the same sweep on the default mixed-precision path beside it
-        line["sweep"] = sweep_bench(P, dev, P.FP32)
+        line["sweep"] = sweep_bench(P, dev, P.FP32, cpu_reference=dist.rank == 0 and not args.no_cpu_baseline)
         line["sweep"]["mixed_precision"] = sweep_bench(P, dev, P.MIXED)
     if not args.no_serve:
         line["serving"] = serve_bench(P, dev, n_req=args.serve_requests, seed=777 + dist.rank)
