@@ -144,6 +144,14 @@ int pfc_run_set_fields_f32(pfc_run *r, const float *phi, const float *con);
  * energy.txt (MIS:1081-1085).  Valid after pfc_run_advance(..., analysis=1). */
 int pfc_run_energy(pfc_run *r, double *e_over_p, double *mass_over_p);
 
+/* n time steps, each followed by the energy analysis, as n calls of
+ * pfc_run_advance(r, 1, 1) + pfc_run_energy (the same kernels and values); the n
+ * energies and masses (e_over_p[i], mass_over_p[i] after step i + 1) come back with one
+ * synchronisation.  CVD writes ENERGYC2 of every step to energy.txt (CVD:442, 979-1039).
+ * Returns PFC_E_NONFINITE, with the arrays written all the same, when the run's
+ * non-finite flag is set (see pfc_run_nonfinite; the flag stays set). */
+int pfc_run_advance_energies(pfc_run *r, int n, double *e_over_p, double *mass_over_p);
+
 /* Whether a fused-path (mixed or FP32) run has met a non-finite nonlinear term since it
  * was created or since the last call (*flag = 1: its fields hold NaN or Inf).  Waits for
  * the run's queued steps.  The engine fails such a run alone (PFC_EV_FAILED with

@@ -600,11 +600,24 @@ int run_cvd_cli(int argc, char **argv) {
         const int rc = resume_run(r, o, o.resume, o.resume + 1);
         if (rc != 0) return rc;
     }
-    for (int t = o.resume >= 0 ? o.resume + 1 : 0; t < o.steps; t++) {
-        fprintf(stderr, "PFC_PROGRESS step=%d total=%d\n", t + 1, o.steps);
+    // ENERGYC2 runs every step (CVD:442): the steps up to the next checkpoint (or the
+    // last step) run as one pfc_run_advance_energies call, whose per-step energies are
+    // those of a step-by-step loop, read back with one synchronisation
+    std::vector<double> es, ms;
+    for (int t = o.resume >= 0 ? o.resume + 1 : 0; t < o.steps;) {
+        const int next_kd = (t % o.mod) == 0 ? t : t + (o.mod - t % o.mod);
+        const int last = std::min(std::min(next_kd, o.steps - 1), t + 1023);
+        const int n = last - t + 1;
+        es.resize(n);
+        ms.resize(n);
+        // a run whose fields went non-finite goes on, as the reference does (its files
+        // then hold the NaN values)
+        const int rc = pfc_run_advance_energies(r, n, es.data(), ms.data());
+        if (rc != PFC_OK && rc != PFC_E_NONFINITE) return gpu_fail("time step");
+        for (int i = t; i <= last; ++i) fprintf(stderr, "PFC_PROGRESS step=%d total=%d\n", i + 1, o.steps);
         fflush(stderr);
-        // ENERGYC2 runs every step (CVD:442), so every step ends with the analysis
-        if (pfc_run_advance(r, 1, 1) != PFC_OK) return gpu_fail("time step");
+        for (int i = 0; i < n - 1; ++i) append_energy_line(o.outdir, t + i, es[i], ms[i]);
+        t = last;
         if ((t % o.mod) == 0) {
             const int kd = t;
             if (pfc_run_get_fields_f32(r, phi.data(), con.data()) != PFC_OK) return gpu_fail("checkpoint fields");
@@ -626,7 +639,8 @@ int run_cvd_cli(int argc, char **argv) {
                 log.flush();
             }
         }
-        if (append_energy(r, o, t) != 0) return 2;
+        append_energy_line(o.outdir, t, es[n - 1], ms[n - 1]);
+        ++t;
     }
     return 0;
 }

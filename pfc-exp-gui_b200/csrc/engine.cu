@@ -489,6 +489,7 @@ static void free_run(pfc_run *r) {
     release_kcoef(r);
     if (r->dev_mem) cudaFree(r->dev_mem);
     if (r->h_nonfinite) cudaFreeHost((void *)r->h_nonfinite);
+    if (r->d_eslots) cudaFree(r->d_eslots);
     if (r->f64) fp64_destroy(r->f64);
     delete r;
 }
@@ -1154,7 +1155,10 @@ extern "C" int pfc_run_destroy(pfc_run *r) {
     return PFC_OK;
 }
 
-static int fused_advance(pfc_run *r, int nsteps, int analysis) {
+// nsteps fused steps; with analysis, the last ends with the checkpoint column mode and
+// the analysis row kernel, whose (energy sum, mass sum) go to red_out (the run's scratch
+// when null).
+static int fused_advance(pfc_run *r, int nsteps, int analysis, double *red_out = nullptr) {
     const int prec = r->p.precision;
     for (int i = 0; i < nsteps; ++i) {
         const bool last = i == nsteps - 1;
@@ -1178,7 +1182,8 @@ static int fused_advance(pfc_run *r, int nsteps, int analysis) {
     r->energy_valid = false;
     if (analysis) {
         PFC_CUDA_TRY(launch_row_analysis(r->d_desc, 1, r->rows, r->rowlen, prec, r->ctx->tw, r->stream));
-        PFC_CUDA_TRY(launch_reduce_fixed(r->desc.partials, r->nparts, 2, 2, r->d_scratch, r->stream));
+        PFC_CUDA_TRY(launch_reduce_fixed(r->desc.partials, r->nparts, 2, 2, red_out ? red_out : r->d_scratch,
+                                         r->stream));
         r->fields_valid = true;
         r->energy_valid = true;
     }
@@ -1191,6 +1196,50 @@ extern "C" int pfc_run_advance(pfc_run *r, int nsteps, int analysis) {
     PFC_CUDA_TRY(cudaSetDevice(r->p.device));
     if (!fused_path(r->p.precision)) return fp64_advance(r, nsteps);
     return fused_advance(r, nsteps, analysis);
+}
+
+extern "C" int pfc_run_advance_energies(pfc_run *r, int nsteps, double *e_over_p, double *mass_over_p) {
+    if (!r || nsteps < 0 || (nsteps > 0 && (!e_over_p || !mass_over_p)))
+        return set_error(PFC_E_INVALID, "bad run, step count or output arrays");
+    if (nsteps == 0) return PFC_OK;
+    PFC_CUDA_TRY(cudaSetDevice(r->p.device));
+    if (!fused_path(r->p.precision)) {  // the FP64 path computes the energy with every step
+        for (int i = 0; i < nsteps; ++i) {
+            int rc = fp64_advance(r, 1);
+            if (rc == PFC_OK) rc = fp64_energy(r, e_over_p + i, mass_over_p + i);
+            if (rc != PFC_OK) return rc;
+        }
+        return PFC_OK;
+    }
+    if (r->eslots_cap < nsteps) {
+        PFC_CUDA_TRY(cudaStreamSynchronize(r->stream));
+        if (r->d_eslots) cudaFree(r->d_eslots);
+        r->d_eslots = nullptr;
+        r->eslots_cap = 0;
+        cudaError_t e = cudaMalloc(&r->d_eslots, sizeof(double) * 2 * (size_t)nsteps);
+        if (e != cudaSuccess) {
+            r->d_eslots = nullptr;
+            return set_error(PFC_E_NOMEM, std::string("cudaMalloc energy slots: ") + cudaGetErrorString(e));
+        }
+        r->eslots_cap = nsteps;
+    }
+    // each step as pfc_run_advance(r, 1, 1): the same launches, its sums in its own slot
+    for (int i = 0; i < nsteps; ++i) {
+        const int rc = fused_advance(r, 1, 1, r->d_eslots + 2 * i);
+        if (rc != PFC_OK) return rc;
+    }
+    PFC_CUDA_TRY(cudaMemcpyAsync(r->d_scratch, r->d_eslots + 2 * (nsteps - 1), 2 * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, r->stream));  // pfc_run_energy's last step
+    std::vector<double> h(2 * (size_t)nsteps);
+    PFC_CUDA_TRY(cudaMemcpyAsync(h.data(), r->d_eslots, h.size() * sizeof(double), cudaMemcpyDeviceToHost, r->stream));
+    PFC_SYNC_CHECKED(r->ctx, r->stream);
+    for (int i = 0; i < nsteps; ++i) {
+        e_over_p[i] = h[2 * i] / r->L / r->M / r->N;
+        mass_over_p[i] = h[2 * i + 1] / r->L / r->M / r->N;
+    }
+    if (*r->h_nonfinite != 0)  // the values are written all the same; the flag stays set for pfc_run_nonfinite
+        return set_error(PFC_E_NONFINITE, "non-finite fields (a NaN or Inf nonlinear term)");
+    return PFC_OK;
 }
 
 extern "C" int pfc_run_advance_timed(pfc_run *r, int nsteps, float *ms) {

@@ -72,6 +72,9 @@ struct pfc_run {
     pfc::RunDesc *d_desc = nullptr;
     float *d_krefn = nullptr;
     double *d_scratch = nullptr;
+    // pfc_run_advance_energies: per-step (energy sum, mass sum) slots on the device
+    double *d_eslots = nullptr;
+    int eslots_cap = 0;
     double psi_mean = 0.0, con_mean = 0.0;
     int t = 0;
     int step_ctr_init = -1;  // host staging of the device step counter

@@ -165,6 +165,7 @@ def lib():
         "pfc_set_col_staging": ([C.c_int, C.c_int, C.c_int, C.c_int, C.c_int], C.c_int),
         "pfc_selftest_tile_stage": ([C.c_int, C.c_int, C.c_int, C.c_double, P(C.c_int), P(C.c_int), dp], C.c_int),
         "pfc_selftest_log": ([C.c_int, dp, dp, C.c_int], C.c_int),
+        "pfc_run_advance_energies": ([vp, C.c_int, dp, dp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -267,6 +268,13 @@ class Run:
         e, d = C.c_double(), C.c_double()
         _check(lib().pfc_run_energy(self.h, C.byref(e), C.byref(d)), "pfc_run_energy")
         return e.value, d.value
+
+    def advance_energies(self, n):
+        """n steps, each followed by the energy analysis; returns (e/P, mass/P) per step as
+        float64 arrays of length n (pfc_run_advance_energies)."""
+        e, d = np.empty(n, np.float64), np.empty(n, np.float64)
+        _check(lib().pfc_run_advance_energies(self.h, n, _dp(e), _dp(d)), "pfc_run_advance_energies")
+        return e, d
 
     def nonfinite(self) -> bool:
         """True when the run met a NaN / Inf nonlinear term since creation or the last call."""

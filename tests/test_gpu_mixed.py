@@ -253,3 +253,25 @@ def test_mixed_noise_is_deterministic_and_has_the_reference_power():
     print("shell power mixed / oracle:", pg / po)
     assert np.all(np.abs(pg / po - 1.0) < 0.25)
     assert abs(pg.sum() / po.sum() - 1.0) < 0.12
+
+
+@pytest.mark.parametrize("L,M,N,precision", [(64, 64, 1, P.MIXED), (32, 32, 8, P.MIXED), (64, 64, 1, P.FP64)])
+def test_advance_energies_matches_step_by_step(L, M, N, precision):
+    """pfc_run_advance_energies (the CVD CLI's loop between checkpoints) against the same
+    steps taken one at a time with the energy read after each: energies, masses and
+    fields bit for bit."""
+    a = P.Run(P.default_params(P.MODEL_CVD, L=L, M=M, N=N, precision=precision))
+    b = P.Run(P.default_params(P.MODEL_CVD, L=L, M=M, N=N, precision=precision))
+    ea, ma = [], []
+    for _ in range(12):
+        a.advance(1, analysis=True)
+        e, m = a.energy()
+        ea.append(e)
+        ma.append(m)
+    eb, mb = b.advance_energies(7)
+    eb2, mb2 = b.advance_energies(5)
+    assert np.array_equal(np.array(ea), np.concatenate([eb, eb2]))
+    assert np.array_equal(np.array(ma), np.concatenate([mb, mb2]))
+    assert b.energy() == (ea[-1], ma[-1])
+    fa, fb = a.fields_f32(), b.fields_f32()
+    assert np.array_equal(fa[0], fb[0]) and np.array_equal(fa[1], fb[1])
