@@ -92,14 +92,65 @@ __global__ void k_sum_partials(const float *__restrict__ a, long n, double *__re
     }
 }
 
-// out[j] = sum_i partials[i * stride + j] for j < width, one thread per j, fixed order.
-__global__ void k_reduce_fixed(const double *__restrict__ partials, int count, int stride, int width,
-                               double *__restrict__ out) {
-    const int j = threadIdx.x;
-    if (j >= width) return;
+// out[j] = sum_i partials[i * stride + j] for j < width (width <= stride), the additions in
+// index order, one thread per j.  The CTA stages the partials chunk by chunk into shared
+// memory with coalesced loads, so the ordered sum waits on shared-memory reads rather
+// than on one global load per term.
+constexpr int REDUCE_NT = 256, REDUCE_CHUNK = 4096;  // threads; doubles staged at a time
+__device__ __forceinline__ void ordered_sums(const double *__restrict__ partials, int count, int stride, int width,
+                                             double *__restrict__ out) {
+    __shared__ double buf[REDUCE_CHUNK];
+    const long total = (long)count * stride;
+    const int rows = REDUCE_CHUNK / stride;  // whole rows of `stride` doubles per chunk
     double s = 0.0;
-    for (int i = 0; i < count; ++i) s += partials[(long)i * stride + j];
-    out[j] = s;
+    for (long base = 0; base < total; base += (long)rows * stride) {
+        const int n = (int)(total - base < (long)rows * stride ? total - base : (long)rows * stride);
+        __syncthreads();  // the previous chunk's sums are done
+        for (int i = threadIdx.x; i < n; i += blockDim.x) buf[i] = partials[base + i];
+        __syncthreads();
+        if (threadIdx.x < width)
+            for (int i = threadIdx.x; i < n; i += stride) s += buf[i];
+    }
+    if (threadIdx.x < width) out[threadIdx.x] = s;
+}
+
+__global__ void __launch_bounds__(REDUCE_NT) k_reduce_fixed(const double *__restrict__ partials, int count, int stride,
+                                                            int width, double *__restrict__ out) {
+    ordered_sums(partials, count, stride, width, out);
+}
+
+// out[j] = sum_i partials[i * stride + j] for j < width <= 2, by a tree of fixed shape: thread
+// t of the REDUCE_NT threads sums rows t, t + REDUCE_NT, ... in index order, then the 32
+// lanes of each warp by shuffles (halving offsets) and the warps' sums in warp order.  The
+// result does not depend on scheduling, and a run's sums are the same alone and in a batch
+// (k_reduce_runs calls the same function); the rows are read in parallel.
+__device__ __forceinline__ void tree_sums(const double *__restrict__ partials, int count, int stride, int width,
+                                          double *__restrict__ out) {
+    __shared__ double red[2][REDUCE_NT / 32];
+    double acc[2] = {0.0, 0.0};
+    for (int i = threadIdx.x; i < count; i += REDUCE_NT)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+            if (j < width) acc[j] += partials[(long)i * stride + j];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+        double v = acc[j];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) red[j][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < width) {
+        double t = 0.0;
+        for (int w = 0; w < REDUCE_NT / 32; ++w) t += red[threadIdx.x][w];
+        out[threadIdx.x] = t;
+    }
+}
+
+__global__ void __launch_bounds__(REDUCE_NT) k_reduce_tree(const double *__restrict__ partials, int count, int stride,
+                                                           int width, double *__restrict__ out) {
+    tree_sums(partials, count, stride, width, out);
 }
 
 cudaError_t launch_init_misfit(float *psi, float *con, int L, int M, int N, float u0, float con0, float dx,
@@ -125,29 +176,27 @@ cudaError_t launch_init_cvd(float *psi, float *con, int L, int M, int N, float u
 // Deterministic FP64 sum of n floats.  scratch must hold `blocks` doubles.
 cudaError_t launch_sum_f32(const float *a, long n, double *scratch, int blocks, double *out, cudaStream_t s) {
     k_sum_partials<<<blocks, 256, 0, s>>>(a, n, scratch);
-    k_reduce_fixed<<<1, 32, 0, s>>>(scratch, blocks, 1, 1, out);
+    k_reduce_fixed<<<1, REDUCE_NT, 0, s>>>(scratch, blocks, 1, 1, out);
     return cudaGetLastError();
 }
 
+// Sums of the analysis partials (energy, mass): the fixed-shape tree of tree_sums.
 cudaError_t launch_reduce_fixed(const double *partials, int count, int stride, int width, double *out,
                                 cudaStream_t s) {
-    k_reduce_fixed<<<1, 32, 0, s>>>(partials, count, stride, width, out);
+    if (stride < 1 || width > stride || width > 2) return cudaErrorInvalidValue;
+    k_reduce_tree<<<1, REDUCE_NT, 0, s>>>(partials, count, stride, width, out);
     return cudaGetLastError();
 }
 
 // k_reduce_fixed(partials, count, 2, 2, ...) for run blockIdx.x of a batch.
-__global__ void k_reduce_runs(const RunDesc *__restrict__ runs, int count, int slot) {
+__global__ void __launch_bounds__(REDUCE_NT) k_reduce_runs(const RunDesc *__restrict__ runs, int count, int slot) {
     const RunDesc &d = runs[blockIdx.x];
-    const int j = threadIdx.x;
-    if (j >= 2) return;
-    double s = 0.0;
-    for (int i = 0; i < count; ++i) s += d.partials[(long)i * 2 + j];
-    d.ehist[2 * slot + j] = s;
+    tree_sums(d.partials, count, 2, 2, d.ehist + 2 * slot);
 }
 
 cudaError_t launch_reduce_runs(const RunDesc *d_runs, int nruns, int nparts, int slot, cudaStream_t s) {
     if (nruns <= 0) return cudaSuccess;
-    k_reduce_runs<<<nruns, 32, 0, s>>>(d_runs, nparts, slot);
+    k_reduce_runs<<<nruns, REDUCE_NT, 0, s>>>(d_runs, nparts, slot);
     return cudaGetLastError();
 }
 

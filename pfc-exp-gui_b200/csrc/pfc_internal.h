@@ -144,9 +144,9 @@ cudaError_t launch_row_forward_mixed(const RunDesc *d_runs, int nruns, int L, in
 cudaError_t launch_row_analysis_mixed(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw,
                                       cudaStream_t s);
 
-// For each of nruns runs: (sum, in CTA order, of the analysis row kernel's nparts
-// partial pairs) -> runs[i].ehist[2*slot], [2*slot+1]; the same additions in the same
-// order as the single-run reduction (launch_reduce_fixed), so the sums are identical.
+// For each of nruns runs: (sum of the analysis row kernel's nparts partial pairs) ->
+// runs[i].ehist[2*slot], [2*slot+1]; the same additions in the same fixed order as the
+// single-run reduction (launch_reduce_fixed), so the sums are identical.
 cudaError_t launch_reduce_runs(const RunDesc *d_runs, int nruns, int nparts, int slot, cudaStream_t s);
 
 // Build the per k-point coefficient table of one run (layout and values as RunDesc::kcoef).
