@@ -170,11 +170,16 @@ __global__ void __launch_bounds__(MRowCfg<M>::NT) k_mrow_forward(const RunDesc *
 // density (ENERGYC2, MIS:1043-1092, every term in double, the grao2-twice gradient of
 // MIS:915) and mass summed in double.
 // ---------------------------------------------------------------------------
+// the analysis transforms three sequences per row: one radix-16 butterfly per thread
+template <int M> struct MRowACfg {
+    static constexpr int NT = (3 * MRowCfg<M>::RPC * M / 16) < 1024 ? (3 * MRowCfg<M>::RPC * M / 16) : 1024;
+    static constexpr int MINB = 768 / NT >= 1 ? 768 / NT : 1;  // 768 threads per SM (85 registers)
+};
 template <int M>
-__global__ void __launch_bounds__(MRowCfg<M>::NT) k_mrow_analysis(const RunDesc *__restrict__ runs,
+__global__ void __launch_bounds__(MRowACfg<M>::NT, MRowACfg<M>::MINB) k_mrow_analysis(const RunDesc *__restrict__ runs,
                                                                   const double2 *__restrict__ tw,
                                                                   const double2 *__restrict__ lt) {
-    constexpr int RPC = MRowCfg<M>::RPC, NT = MRowCfg<M>::NT, H = M / 2;
+    constexpr int RPC = MRowCfg<M>::RPC, NT = MRowACfg<M>::NT, H = M / 2;
     constexpr int NB = 3 * RPC;
     extern __shared__ double2 sd[];
     __shared__ double red[2][32];
@@ -279,7 +284,7 @@ static cudaError_t mrow_forward_impl(const RunDesc *d_runs, int nruns, int L, co
 template <int M>
 static cudaError_t mrow_analysis_impl(const RunDesc *d_runs, int nruns, int L, const TwiddleSet &tw,
                                       cudaStream_t st) {
-    constexpr int RPC = MRowCfg<M>::RPC, NT = MRowCfg<M>::NT;
+    constexpr int RPC = MRowCfg<M>::RPC, NT = MRowACfg<M>::NT;
     constexpr size_t smem = dsmem_bytes<3 * RPC * M>();
     static unsigned mask = 0;
     cudaError_t e = set_smem(k_mrow_analysis<M>, smem, mask);
