@@ -923,10 +923,18 @@ using namespace pfc;
 // C ABI (host buffers in, host buffers out)
 // ---------------------------------------------------------------------------
 namespace {
+// A device buffer of one host-array call, taken from the device's default memory pool in
+// stream order and returned to it the same way (the pool keeps freed memory, so repeated
+// calls do not map and unmap device memory; get_context sets that).
 struct DevBuf {
     void *p = nullptr;
+    cudaStream_t st = nullptr;
+    cudaError_t alloc(size_t bytes, cudaStream_t s) {
+        st = s;
+        return cudaMallocAsync(&p, bytes, s);
+    }
     ~DevBuf() {
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, st);
     }
 };
 int host_ctx(cudaStream_t *st) {
@@ -955,8 +963,8 @@ extern "C" int pfc_phimax_misfit(const float *phi, const float *con, int L, int 
     if (rc != PFC_OK) return rc;
     const long P = (long)L * M;
     DevBuf f, o;
-    ATRY(cudaMalloc(&f.p, 2 * P * sizeof(float)));
-    ATRY(cudaMalloc(&o.p, (size_t)(cap > 0 ? cap : 1) * 5 * sizeof(double)));
+    ATRY(f.alloc(2 * P * sizeof(float), st));
+    ATRY(o.alloc((size_t)(cap > 0 ? cap : 1) * 5 * sizeof(double), st));
     float *dphi = (float *)f.p, *dcon = dphi + P;
     ATRY(cudaMemcpyAsync(dphi, phi, P * sizeof(float), cudaMemcpyHostToDevice, st));
     ATRY(cudaMemcpyAsync(dcon, con, P * sizeof(float), cudaMemcpyHostToDevice, st));
@@ -976,8 +984,8 @@ extern "C" int pfc_phimax_elastic(const float *phi, int L, int M, int N, float d
     if (rc != PFC_OK) return rc;
     const long P = (long)L * M * N;
     DevBuf f, o;
-    ATRY(cudaMalloc(&f.p, P * sizeof(float)));
-    ATRY(cudaMalloc(&o.p, (size_t)(cap > 0 ? cap : 1) * 4 * sizeof(double)));
+    ATRY(f.alloc(P * sizeof(float), st));
+    ATRY(o.alloc((size_t)(cap > 0 ? cap : 1) * 4 * sizeof(double), st));
     ATRY(cudaMemcpyAsync(f.p, phi, P * sizeof(float), cudaMemcpyHostToDevice, st));
     rc = phimax_elastic_dev((const float *)f.p, L, M, N, dx, (double *)o.p, cap, count, st);
     if (rc != PFC_OK) return rc;
@@ -996,8 +1004,8 @@ extern "C" int pfc_cvd_atoms(const float *phi, int L, int M, int N, float dx, fl
     if (rc != PFC_OK) return rc;
     const long P = (long)L * M * N;
     DevBuf f, o;
-    ATRY(cudaMalloc(&f.p, P * sizeof(float)));
-    ATRY(cudaMalloc(&o.p, (size_t)cap * 4 * sizeof(double)));
+    ATRY(f.alloc(P * sizeof(float), st));
+    ATRY(o.alloc((size_t)cap * 4 * sizeof(double), st));
     ATRY(cudaMemcpyAsync(f.p, phi, P * sizeof(float), cudaMemcpyHostToDevice, st));
     float stats[2];
     rc = cvd_atoms_dev((const float *)f.p, L, M, N, dx, u0, (double *)o.p, cap, count, stats, st);
@@ -1018,7 +1026,7 @@ extern "C" int pfc_cvd_atoms(const float *phi, int L, int M, int N, float dx, fl
 }
 
 static int upload_records(const float *x, const float *y, const float *z, int n, DevBuf &b, cudaStream_t st) {
-    ATRY(cudaMalloc(&b.p, (size_t)3 * n * sizeof(float) + 16));
+    ATRY(b.alloc((size_t)3 * n * sizeof(float) + 16, st));
     float *d = (float *)b.p;
     ATRY(cudaMemcpyAsync(d, x, n * sizeof(float), cudaMemcpyHostToDevice, st));
     ATRY(cudaMemcpyAsync(d + n, y, n * sizeof(float), cudaMemcpyHostToDevice, st));
@@ -1039,7 +1047,7 @@ extern "C" int pfc_cvd_gr_hist(const float *x, const float *y, const float *z, i
     DevBuf r, h;
     rc = upload_records(x, y, z, n > 0 ? n : 1, r, st);
     if (rc != PFC_OK) return rc;
-    ATRY(cudaMalloc(&h.p, sizeof(unsigned) * (size_t)(mb > 0 ? mb : 1)));
+    ATRY(h.alloc(sizeof(unsigned) * (size_t)(mb > 0 ? mb : 1), st));
     const float *d = (const float *)r.p;
     const int nn = n > 0 ? n : 1;
     rc = cvd_gr_dev(d, d + nn, d + 2 * nn, n, L, M, N, dx, (unsigned *)h.p, mb, st);
@@ -1064,7 +1072,7 @@ extern "C" int pfc_cvd_q6(const float *x, const float *y, const float *z, int n,
     DevBuf r, o;
     rc = upload_records(x, y, z, n, r, st);
     if (rc != PFC_OK) return rc;
-    ATRY(cudaMalloc(&o.p, (size_t)n * (sizeof(unsigned) + sizeof(float))));
+    ATRY(o.alloc((size_t)n * (sizeof(unsigned) + sizeof(float)), st));
     const float *d = (const float *)r.p;
     unsigned *dnb = (unsigned *)o.p;
     float *dql = (float *)(dnb + n);
@@ -1084,7 +1092,7 @@ extern "C" int pfc_elastic3d(const double *x, const double *y, const double *z, 
     int rc = host_ctx(&st);
     if (rc != PFC_OK) return rc;
     DevBuf b;
-    ATRY(cudaMalloc(&b.p, (size_t)n * (4 * sizeof(double) + sizeof(uint32_t))));
+    ATRY(b.alloc((size_t)n * (4 * sizeof(double) + sizeof(uint32_t)), st));
     double *dx_ = (double *)b.p, *dy = dx_ + n, *dz = dy + n, *ds = dz + n;
     uint32_t *dnb = (uint32_t *)(ds + n);
     ATRY(cudaMemcpyAsync(dx_, x, n * sizeof(double), cudaMemcpyHostToDevice, st));
@@ -1106,7 +1114,7 @@ extern "C" int pfc_cryst_order(const double *x, const double *y, const double *z
     int rc = host_ctx(&st);
     if (rc != PFC_OK) return rc;
     DevBuf b;
-    ATRY(cudaMalloc(&b.p, (size_t)n * 5 * sizeof(double)));
+    ATRY(b.alloc((size_t)n * 5 * sizeof(double), st));
     double *dx_ = (double *)b.p, *dy = dx_ + n, *dz = dy + n, *d4 = dz + n, *d6 = d4 + n;
     ATRY(cudaMemcpyAsync(dx_, x, n * sizeof(double), cudaMemcpyHostToDevice, st));
     ATRY(cudaMemcpyAsync(dy, y, n * sizeof(double), cudaMemcpyHostToDevice, st));

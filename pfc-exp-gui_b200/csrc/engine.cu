@@ -77,6 +77,15 @@ int get_context(int device, Context **out) {
         return set_error(PFC_E_CUDA, std::string("no CUDA device available: ") + cudaGetErrorString(e));
     if (device < 0 || device >= ndev) return set_error(PFC_E_INVALID, "device ordinal out of range");
     PFC_CUDA_TRY(cudaSetDevice(device));
+    // memory freed in stream order (the analysis calls' buffers) stays in this process's
+    // default pool for the next call instead of being unmapped at each synchronisation
+    {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     Context *c = new Context();
     c->device = device;
     PFC_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));

@@ -439,7 +439,7 @@ def phimax_misfit(phi, con, dx=0.125, con0=0.2):
     con = np.ascontiguousarray(con, np.float32)
     L, M = phi.shape[0], phi.shape[1]
     cap = L * M + 1
-    out = np.zeros((cap, 5), np.float64)
+    out = np.empty((cap, 5), np.float64)  # only the first n rows are written and read
     n = C.c_int()
     _check(lib().pfc_phimax_misfit(_fp(phi), _fp(con), L, M, dx, con0, _dp(out), cap, C.byref(n)), "pfc_phimax_misfit")
     return out[: n.value].copy()
@@ -449,7 +449,7 @@ def phimax_elastic(phi, dx=0.125):
     phi = np.ascontiguousarray(phi, np.float32)
     L, M, N = phi.shape
     cap = L * M * N + 1
-    out = np.zeros((cap, 4), np.float64)
+    out = np.empty((cap, 4), np.float64)  # only the first n rows are written and read
     n = C.c_int()
     _check(lib().pfc_phimax_elastic(_fp(phi), L, M, N, dx, _dp(out), cap, C.byref(n)), "pfc_phimax_elastic")
     return out[: n.value].copy()
@@ -480,7 +480,7 @@ def cvd_atoms(phi, u0, dx=0.125):
     phi = np.ascontiguousarray(phi, np.float32)
     L, M, N = phi.shape
     cap = L * M * N + 1
-    out = np.zeros((cap, 4), np.float32)
+    out = np.empty((cap, 4), np.float32)  # only the first n rows are written and read
     n, phic, pmax = C.c_int(), C.c_float(), C.c_float()
     _check(lib().pfc_cvd_atoms(_fp(phi), L, M, N, dx, u0, _fp(out), cap, C.byref(n), C.byref(phic), C.byref(pmax)),
            "pfc_cvd_atoms")
