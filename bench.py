@@ -750,7 +750,8 @@ def run_ours(args):
     if not args.no_sweep:
         # the sweep workload names FP32 arithmetic with FP64 reductions (the FP32 path);
         # the same sweep on the default mixed-precision path beside it
-        line["sweep"] = sweep_bench(P, dev, P.FP32, cpu_reference=dist.rank == 0 and not args.no_cpu_baseline)
+        line["sweep"] = sweep_bench(P, dev, P.FP32,
+                                    cpu_reference=dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline)
         line["sweep"]["mixed_precision"] = sweep_bench(P, dev, P.MIXED)
     if not args.no_serve:
         line["serving"] = serve_bench(P, dev, n_req=args.serve_requests, seed=777 + dist.rank)
