@@ -50,8 +50,9 @@ extern "C" {
  * (misfit_uniform_time_seed_fftw_early.cpp:17-35, 125-143; cvd.cpp:111-125, 33-53). */
 typedef struct pfc_run_params {
     int model;      /* PFC_MODEL_MISFIT or PFC_MODEL_CVD */
-    int L, M, N;    /* grid; L, M powers of two in [32, 2048]; N = 1 (2-D) on the fused
-                       (FP32, mixed) paths, a power of two <= 2048 on the FP64 paths (3-D CVD runs) */
+    int L, M, N;    /* grid; L, M powers of two in [32, 2048]; N = 1 (2-D), or for 3-D CVD
+                       runs a power of two: 8 <= N <= 2048 on the mixed path, N <= 2048 on
+                       the FP64 paths (the FP32 path takes 2-D grids only) */
     float u0, con0, sig, dt, dx, axx;
     int grainx, grainy, grainz; /* Misfit initial grains */
     uint32_t seed;

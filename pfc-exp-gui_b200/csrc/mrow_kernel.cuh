@@ -25,6 +25,7 @@ struct TermsD {
 };
 struct CoefsD {
     double niu, ksi, w, alpha, inv_c0, inv_1mc0;
+    double ksi_3, mniu_2;  // ksi / 3 and -niu / 2
 };
 __device__ __forceinline__ CoefsD coefs_d(const ModelCoefs &k) {
     CoefsD c;
@@ -34,21 +35,36 @@ __device__ __forceinline__ CoefsD coefs_d(const ModelCoefs &k) {
     c.alpha = k.para_alpha;
     c.inv_c0 = 1.0 / (double)k.para_c0;
     c.inv_1mc0 = 1.0 / (1.0 - (double)k.para_c0);
+    c.ksi_3 = c.ksi / 3.0;
+    c.mniu_2 = -0.5 * c.niu;
     return c;
 }
+// Pointwise arithmetic of the mixed path is written as explicit fma() and the __d*_rn
+// operations, which the compiler never fuses or splits.  Left as a*b + c, the choice of
+// fusing is the compiler's for each inlined copy (a thread evaluates several points
+// through unrolled copies), so equal inputs could round differently from point to point.
+// With every rounding fixed, equal inputs give equal terms: a 3-D state that does not
+// depend on n (the CVD initial condition) stays exactly independent of n, as in the
+// reference, whose row transforms of a constant row are exact.
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+// 1 - 3 c^2 + 2 c^3 = 1 + c^2 (2 c - 3), c2 = c^2
+__device__ __forceinline__ double cubic_d(double c, double c2) { return fma(c2, fma(2.0, c, -3.0), 1.0); }
 __device__ __forceinline__ TermsD point_terms_d(const CoefsD &k, double psi, double c, double a, double b,
                                               const double2 *__restrict__ lt) {
-    const double psi2 = psi * psi;
-    const double in1 = -k.niu * psi2 * 0.5 + k.ksi * psi2 * psi * (1.0 / 3.0);
-    const double lc = log_tab(c * k.inv_c0, lt);
-    const double omc = 1.0 - c;
-    const double l1c = log_tab(omc * k.inv_1mc0, lt);
-    const double in2 = k.w * (c * lc + omc * l1c);
-    const double c2 = c * c, omc2 = omc * omc;
-    const double in3 = -(1.0 - 3.0 * c2 + 2.0 * c2 * c) * a - (1.0 - 3.0 * omc2 + 2.0 * omc2 * omc) * b;
+    const double psi2 = dmul(psi, psi);
+    const double in1 = dmul(psi2, fma(k.ksi_3, psi, k.mniu_2));  // -niu psi^2 / 2 + ksi psi^3 / 3
+    const double lc = log_tab(dmul(c, k.inv_c0), lt);
+    const double omc = dsub(1.0, c);
+    const double l1c = log_tab(dmul(omc, k.inv_1mc0), lt);
+    const double in2 = dmul(k.w, fma(c, lc, dmul(omc, l1c)));
+    const double c2 = dmul(c, c), omc2 = dmul(omc, omc);
+    const double in3 = -fma(cubic_d(c, c2), a, dmul(cubic_d(omc, omc2), b));
     TermsD t;
-    t.inn = in1 + in2 + in3;
-    t.inc = k.w * (psi + 1.0) * (lc - l1c) - 3.0 * psi * (a - b) * (c2 - c);
+    t.inn = dadd(dadd(in1, in2), in3);
+    // w (psi + 1)(lc - l1c) - 3 psi (a - b)(c^2 - c)
+    t.inc = fma(dmul(-3.0, dmul(psi, dsub(a, b))), dsub(c2, c), dmul(dmul(k.w, dadd(psi, 1.0)), dsub(lc, l1c)));
     return t;
 }
 
@@ -106,8 +122,8 @@ __global__ void __launch_bounds__(MRowCfg<M>::NT, MRowCfg<M>::MINB)
         if (w < RPC * M) {
             const int r = w % RPC, m = w / RPC;
             const double2 z1 = sd[spad(m * NB + 2 * r)], z2 = sd[spad(m * NB + 2 * r + 1)];
-            const TermsD t =
-                point_terms_d(kc, z1.x * invM + d.psi_mean, z1.y * invM + d.con_mean, z2.x * invM, z2.y * invM, lt);
+            const TermsD t = point_terms_d(kc, fma(z1.x, invM, d.psi_mean), fma(z1.y, invM, d.con_mean),
+                                           dmul(z2.x, invM), dmul(z2.y, invM), lt);
             out[q] = make_double2(t.inn, t.inc);
             bad |= !(isfinite(t.inn) && isfinite(t.inc));
         }
@@ -211,19 +227,22 @@ __global__ void __launch_bounds__(MRowACfg<M>::NT, MRowACfg<M>::MINB) k_mrow_ana
         if (l >= L) continue;
         const double2 z1 = sd[spad(m * NB + 3 * r)], z2 = sd[spad(m * NB + 3 * r + 1)],
                       z3 = sd[spad(m * NB + 3 * r + 2)];
-        const double dpsi = z1.x * invM;
-        const double psi = dpsi + d.psi_mean, c = z1.y * invM + d.con_mean;
-        const double a = z2.x * invM, b = z2.y * invM, gx = z3.x * invM, gy = z3.y * invM;
+        // explicit roundings, as in point_terms_d: equal inputs give equal outputs
+        const double dpsi = dmul(z1.x, invM);
+        const double psi = dadd(dpsi, d.psi_mean), c = fma(z1.y, invM, d.con_mean);
+        const double a = dmul(z2.x, invM), b = dmul(z2.y, invM), gx = dmul(z3.x, invM), gy = dmul(z3.y, invM);
         d.psi_real[(size_t)l * M + m] = (float)psi;
         d.con_real[(size_t)l * M + m] = (float)c;
-        const double psi2 = psi * psi;
-        const double e_id = psi2 * 0.5 - kc.niu * psi2 * psi * (1.0 / 6.0) + kc.ksi * psi2 * psi2 * (1.0 / 12.0);
-        const double lc = log_tab(c * kc.inv_c0, lt), omc = 1.0 - c, l1c = log_tab(omc * kc.inv_1mc0, lt);
-        const double e_mix = (psi + 1.0) * kc.w * (c * lc + omc * l1c);
-        const double c2 = c * c, omc2 = omc * omc;
-        const double in3 = -(1.0 - 3.0 * c2 + 2.0 * c2 * c) * a - (1.0 - 3.0 * omc2 + 2.0 * omc2 * omc) * b;
-        const double e_ex = 0.5 * psi * in3 + kc.alpha * (gx * gx + gy * gy + gy * gy);
-        acc_e += e_id + e_mix + e_ex;
+        const double psi2 = dmul(psi, psi);
+        // psi^2 / 2 - niu psi^3 / 6 + ksi psi^4 / 12 = psi^2 (1/2 + psi (ksi psi / 12 - niu / 6))
+        const double e_id = dmul(psi2, fma(psi, fma(dmul(kc.ksi_3, 0.25), psi, dmul(kc.mniu_2, 1.0 / 3.0)), 0.5));
+        const double lc = log_tab(dmul(c, kc.inv_c0), lt), omc = dsub(1.0, c), l1c = log_tab(dmul(omc, kc.inv_1mc0), lt);
+        const double e_mix = dmul(dmul(dadd(psi, 1.0), kc.w), fma(c, lc, dmul(omc, l1c)));
+        const double c2 = dmul(c, c), omc2 = dmul(omc, omc);
+        const double in3 = -fma(cubic_d(c, c2), a, dmul(cubic_d(omc, omc2), b));
+        const double grad2 = fma(gx, gx, dmul(2.0, dmul(gy, gy)));  // gx^2 + gy^2 + gy^2
+        const double e_ex = fma(dmul(0.5, psi), in3, dmul(kc.alpha, grad2));
+        acc_e += dadd(dadd(e_id, e_mix), e_ex);
         acc_m += dpsi;
     }
 #pragma unroll
