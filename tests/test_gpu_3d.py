@@ -152,35 +152,38 @@ def test_3d_cvd_state_stays_independent_of_n(precision):
         assert n_spread(r) == 0.0, f"step {target}"
 
 
-def test_3d_long_run_statistics():
-    """CVD 256 x 256 x 64, steps 1000 and 2000, mixed path against pure FP64.
 
-    The run stores its state in FP32, and this CVD state amplifies small differences by
-    ~1e4 between steps 20 and 100 (a 1e-10 perturbation of phi at step 20 is 7e-7 there),
-    so the fields separate from pure FP64 by ~1e-3 at step 100 and, once an interface has
-    moved by a lattice spacing, by O(1) locally (0.8 at step 1000); rounding the pure-FP64
-    run's real fields to FP32 after every step does the same.  What stays: the energy (within
-    5e-4 relative at step 1000, 2e-3 at 2000), the conserved means exactly, the independence
-    of n exactly, and the 2-D run of the same plane (a state independent of n evolves as
-    the 2-D state)."""
-    shape = dict(L=256, M=256, N=64)
-    a = run3(**shape)
-    b = P.Run(P.default_params(P.MODEL_CVD, precision=P.FP64_PURE, **shape))
-    a2 = P.Run(P.default_params(P.MODEL_CVD, L=256, M=256, N=1))
+@pytest.mark.parametrize("u0,checkpoints", [(0.05, ((250, 5e-5), (1000, 5e-5), (5000, 5e-4))),
+                                            (0.01, ((1000, 2e-3), (2000, 5e-3)))])
+def test_3d_long_run_statistics(u0, checkpoints):
+    """CVD 256 x 256 x 64 with con0 0.2 over a long run, mixed path against pure FP64: u0 0.05
+    is the C3 run (5000 steps, checkpoints every 250), u0 0.01 the CLI default.
+
+    The run stores its state in FP32, and CVD amplifies small differences (at u0 0.01 a
+    1e-10 perturbation of phi at step 20 is 7e-7 at step 100), so the fields separate from
+    pure FP64 by ~1e-3 within 100 steps and, once an interface has moved by a lattice
+    spacing, by O(1) locally; the reference's own float roundings (the FP64 path) do the
+    same (0.94 at step 5000 of C3, where the mixed path is at 0.02).  What stays: the energy
+    per point within max(floor, 2 x the reference's own deviation), the conserved means
+    exactly, the independence of n exactly, and the 2-D run of the same plane (a state
+    independent of n evolves as the 2-D state) within 1e-3."""
+    kw = dict(L=256, M=256, u0=u0, con0=0.2)
+    a = run3(N=64, **kw)
+    b = run3(N=64, precision=P.FP64_PURE, **kw)
+    c = run3(N=64, precision=P.FP64, **kw)
+    a2 = P.Run(P.default_params(P.MODEL_CVD, N=1, **kw))
     m0 = a.means()
     done = 0
-    for target, rel in ((1000, 2e-3), (2000, 5e-3)):
-        a.advance(target - done, analysis=True)
-        a2.advance(target - done, analysis=True)
-        b.advance(target - done)
+    for target, floor in checkpoints:
+        for r in (a, a2, b, c):
+            r.advance(target - done, analysis=True)
         done = target
-        ea, da = a.energy()
-        eb, db = b.energy()
-        e2, d2 = a2.energy()
-        print(f"CVD 256x256x64 step {target}: e/P mixed {ea:.9e}, pure FP64 {eb:.9e} (rel {abs(ea - eb) / abs(eb):.2e}), "
-              f"2-D mixed {e2:.9e}; mass {da:.12f} vs {db:.12f}")
-        assert abs(ea - eb) <= rel * abs(eb)
-        assert abs(ea - e2) <= 1e-4 * abs(e2)
+        (ea, da), (eb, db), (ec, _), (e2, _) = a.energy(), b.energy(), c.energy(), a2.energy()
+        rel, ref = abs(ea - eb) / abs(eb), abs(ec - eb) / abs(eb)
+        print(f"CVD 256x256x64 u0 {u0} step {target}: e/P mixed {ea:.9e}, pure FP64 {eb:.9e} (rel {rel:.2e}; the "
+              f"reference's roundings {ref:.2e}), 2-D mixed {e2:.9e}; mass {da:.12f} vs {db:.12f}")
+        assert rel <= max(floor, 2.0 * ref)
+        assert abs(ea - e2) <= 1e-3 * abs(e2)
         assert a.means() == m0
         assert abs(da - db) <= 1e-9
         assert n_spread(a) == 0.0
