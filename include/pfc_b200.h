@@ -205,8 +205,9 @@ int pfc_phimax_misfit(const float *phi, const float *con, int L, int M, float dx
  * atoms are written and *count is set.  *count is the number of atoms found, which
  * may exceed cap; only the first cap records are written.
  *
- * The first call on a device looks up the scratch array's device address; make
- * that first call before any stream capture.  All calls on a device share the
+ * Every call synchronises `stream` (it reads the atom count back to the host), so
+ * it cannot be part of a CUDA graph: never call it while `stream`, or the legacy
+ * default stream, is being captured.  All calls on a device share the scratch
  * array, so calls that overlap on the GPU (from several host threads or streams)
  * race: serialise them. */
 int pfc_phimax_misfit_noalloc(const float *d_phi, const float *d_con, int L, int M, float dx, float con0,
