@@ -476,7 +476,9 @@ void cvd_usage(const char *argv0) {
          << "  --seed <uint>       Random seed base (default: 20200604)\n"
          << "  --outdir <path>     Output directory (default: current dir)\n"
          << "  --grid <LxMxN>      Grid (default: 256x256x1)\n"
-         << "  --precision <p>     mixed, fp32, fp64 or fp64-pure (default: mixed; fp64 on 3-D grids it does not take)\n"
+         << "  --precision <p>     mixed, fp32, fp64 or fp64-pure (default: mixed; fp64 on 3-D grids it does not take;\n"
+         << "                      fp64 keeps the reference's own float roundings, so a run follows the reference's\n"
+         << "                      trajectory, which FP32 storage leaves after ~100 steps at u0 0.01)\n"
          << "  --resume <kd>       Continue from checkpoint kd in --outdir\n"
          << "  -h, --help          Show this help\n";
 }
