@@ -1167,12 +1167,17 @@ extern "C" int pfc_run_destroy(pfc_run *r) {
 // nsteps fused steps; with analysis, the last ends with the checkpoint column mode and
 // the analysis row kernel, whose (energy sum, mass sum) go to red_out (the run's scratch
 // when null).
-static int fused_advance(pfc_run *r, int nsteps, int analysis, double *red_out = nullptr) {
+// row_done: the first step's row work (inn, inc) was done by the analysis that ended the
+// previous call; next_row (mixed path, with analysis): the closing analysis also does the
+// next step's row work, so that the next call passes row_done.
+static int fused_advance(pfc_run *r, int nsteps, int analysis, double *red_out = nullptr, bool row_done = false,
+                         bool next_row = false) {
     const int prec = r->p.precision;
     for (int i = 0; i < nsteps; ++i) {
         const bool last = i == nsteps - 1;
         const int mode = (last && analysis) ? COL_STEP_CHECKPOINT : COL_STEP;
-        PFC_CUDA_TRY(launch_row_step(r->d_desc, 1, r->rows, r->rowlen, prec, r->ctx->tw, r->stream));
+        if (i > 0 || !row_done)
+            PFC_CUDA_TRY(launch_row_step(r->d_desc, 1, r->rows, r->rowlen, prec, r->ctx->tw, r->stream));
         if (r->d3) {
             const RunDesc &dc = r->desc_col;
             PFC_CUDA_TRY(launch_mpass(mpass_args(r, {0, 1, 4, 5}, true), true, r->ctx->tw, r->stream));
@@ -1190,7 +1195,10 @@ static int fused_advance(pfc_run *r, int nsteps, int analysis, double *red_out =
     r->fields_valid = false;
     r->energy_valid = false;
     if (analysis) {
-        PFC_CUDA_TRY(launch_row_analysis(r->d_desc, 1, r->rows, r->rowlen, prec, r->ctx->tw, r->stream));
+        if (next_row)
+            PFC_CUDA_TRY(launch_row_analysis_step_mixed(r->d_desc, 1, r->rows, r->rowlen, r->ctx->tw, r->stream));
+        else
+            PFC_CUDA_TRY(launch_row_analysis(r->d_desc, 1, r->rows, r->rowlen, prec, r->ctx->tw, r->stream));
         PFC_CUDA_TRY(launch_reduce_fixed(r->desc.partials, r->nparts, 2, 2, red_out ? red_out : r->d_scratch,
                                          r->stream));
         r->fields_valid = true;
@@ -1232,9 +1240,13 @@ extern "C" int pfc_run_advance_energies(pfc_run *r, int nsteps, double *e_over_p
         }
         r->eslots_cap = nsteps;
     }
-    // each step as pfc_run_advance(r, 1, 1): the same launches, its sums in its own slot
+    // each step as pfc_run_advance(r, 1, 1), its sums in its own slot.  On the mixed path
+    // the analysis of step i (but the last) also does step i + 1's row work: the same
+    // operations as the row kernel's, so the same bits, with one launch and one read of
+    // the row-space arrays fewer per step.
+    const bool fuse = r->p.precision == PFC_PRECISION_MIXED;
     for (int i = 0; i < nsteps; ++i) {
-        const int rc = fused_advance(r, 1, 1, r->d_eslots + 2 * i);
+        const int rc = fused_advance(r, 1, 1, r->d_eslots + 2 * i, fuse && i > 0, fuse && i + 1 < nsteps);
         if (rc != PFC_OK) return rc;
     }
     PFC_CUDA_TRY(cudaMemcpyAsync(r->d_scratch, r->d_eslots + 2 * (nsteps - 1), 2 * sizeof(double),

@@ -40,15 +40,18 @@ __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_doub
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+// The FP64 products are explicit fma() and __dmul_rn (never fused or split by the
+// compiler), so a butterfly rounds the same way in every kernel that inlines it: two
+// kernels that transform the same sequence give the same bits.
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+    return make_double2(fma(a.x, b.x, -__dmul_rn(a.y, b.y)), fma(a.x, b.y, __dmul_rn(a.y, b.x)));
 }
 // multiply by conj(b)
 __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
     return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
 __device__ __forceinline__ double2 cmulc(double2 a, double2 b) {
-    return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+    return make_double2(fma(a.x, b.x, __dmul_rn(a.y, b.y)), fma(a.y, b.x, -__dmul_rn(a.x, b.y)));
 }
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
@@ -135,6 +138,12 @@ template <bool FWD, typename C> __device__ __forceinline__ void dft8(C *a) {
     a[7] = csub(e3, o3);
 }
 
+// (a.x c + a.y s, a.y c - a.x s): a rotated by exp(-i theta), c = cos, s = sin
+__device__ __forceinline__ float2 rot(float2 a, float c, float s) { return mk(a.x * c + a.y * s, a.y * c - a.x * s); }
+__device__ __forceinline__ double2 rot(double2 a, double c, double s) {
+    return mk(fma(a.x, c, __dmul_rn(a.y, s)), fma(a.y, c, -__dmul_rn(a.x, s)));
+}
+
 // multiply by w16^j (j = n2*k1 in 0..9), w16 = exp(-+2 pi i / 16)
 template <bool FWD, typename C> __device__ __forceinline__ C w16(C a, int j) {
     typedef typename real_of<C>::T R;
@@ -153,7 +162,7 @@ template <bool FWD, typename C> __device__ __forceinline__ C w16(C a, int j) {
         default: c = -c1; s = -s1; break;  // 9
     }
     if (!FWD) s = -s;
-    return mk(a.x * c + a.y * s, a.y * c - a.x * s);
+    return rot(a, c, s);
 }
 
 template <bool FWD, typename C> __device__ __forceinline__ void dft16(C *a) {

@@ -190,18 +190,26 @@ __global__ void __launch_bounds__(MRowCfg<M>::NT) k_mrow_forward(const RunDesc *
 template <int M> struct MRowACfg {
     static constexpr int NT = (3 * MRowCfg<M>::RPC * M / 16) < 1024 ? (3 * MRowCfg<M>::RPC * M / 16) : 1024;
     static constexpr int MINB = 768 / NT >= 1 ? 768 / NT : 1;  // 768 threads per SM (85 registers)
+    // the analysis with the next step's row work (STEP): about 112 registers per thread
+    static constexpr int MINB_STEP = 65536 / (NT * 112) >= 1 ? 65536 / (NT * 112) : 1;
 };
-template <int M>
-__global__ void __launch_bounds__(MRowACfg<M>::NT, MRowACfg<M>::MINB) k_mrow_analysis(const RunDesc *__restrict__ runs,
-                                                                  const double2 *__restrict__ tw,
-                                                                  const double2 *__restrict__ lt) {
+// STEP = false: the analysis of the state.  STEP = true: the same analysis (the same
+// arithmetic, so the same sums), and then the next step's row work from the transforms it
+// already holds: the pointwise terms, their forward transform and the inn/inc row-space
+// arrays, as k_mrow_step computes them (the same operations in the same order, so the same
+// bits).  The next step then starts at its m-axis pass (3-D) or column kernel (2-D).
+template <int M, bool STEP>
+__global__ void __launch_bounds__(MRowACfg<M>::NT, STEP ? MRowACfg<M>::MINB_STEP : MRowACfg<M>::MINB)
+    k_mrow_analysis(const RunDesc *__restrict__ runs, const double2 *__restrict__ tw, const double2 *__restrict__ lt) {
     constexpr int RPC = MRowCfg<M>::RPC, NT = MRowACfg<M>::NT, H = M / 2;
     constexpr int NB = 3 * RPC;
+    constexpr int PTS = (RPC * M + NT - 1) / NT;
     extern __shared__ double2 sd[];
     __shared__ double red[2][32];
     const RunDesc &d = runs[blockIdx.y];
     const int L = d.L;
     const int l0 = blockIdx.x * RPC;
+    if (STEP && d.noise_amp != 0.0f && blockIdx.x == 0 && threadIdx.x == 0) *d.step_ctr += 1;
     ROW_TILE_LOOP(RPC, H, NT, {
         float2 z[6] = {};
         if (l < L) {
@@ -222,7 +230,13 @@ __global__ void __launch_bounds__(MRowACfg<M>::NT, MRowACfg<M>::MINB) k_mrow_ana
     const double invM = 1.0 / (double)M;
     const CoefsD kc = coefs_d(d.k);
     double acc_e = 0.0, acc_m = 0.0;
-    for (int w = threadIdx.x; w < RPC * M; w += NT) {
+    double2 out[STEP ? PTS : 1];
+    bool bad = false;
+#pragma unroll
+    for (int q = 0; q < PTS; ++q) {
+        const int w = threadIdx.x + q * NT;
+        if (STEP) out[q] = make_double2(0.0, 0.0);
+        if (w >= RPC * M) continue;
         const int r = w % RPC, m = w / RPC, l = l0 + r;
         if (l >= L) continue;
         const double2 z1 = sd[spad(m * NB + 3 * r)], z2 = sd[spad(m * NB + 3 * r + 1)],
@@ -244,6 +258,12 @@ __global__ void __launch_bounds__(MRowACfg<M>::NT, MRowACfg<M>::MINB) k_mrow_ana
         const double e_ex = fma(dmul(0.5, psi), in3, dmul(kc.alpha, grad2));
         acc_e += dadd(dadd(e_id, e_mix), e_ex);
         acc_m += dpsi;
+        if constexpr (STEP) {
+            // the row step's inputs: psi as k_mrow_step forms it (one rounding), c, a, b as above
+            const TermsD t = point_terms_d(kc, fma(z1.x, invM, d.psi_mean), c, a, b, lt);
+            out[q] = make_double2(t.inn, t.inc);
+            bad |= !(isfinite(t.inn) && isfinite(t.inc));
+        }
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
@@ -265,6 +285,27 @@ __global__ void __launch_bounds__(MRowACfg<M>::NT, MRowACfg<M>::MINB) k_mrow_ana
         const int lrows = (L - l0) < RPC ? (L - l0) : RPC;
         d.partials[2 * blockIdx.x] = se;
         d.partials[2 * blockIdx.x + 1] = sm + d.psi_mean * (double)lrows * (double)M;
+    }
+    if constexpr (STEP) {
+        // every thread has read the inverse transforms (the barrier above); a non-finite
+        // term marks the run
+        if (__syncthreads_or(bad) && threadIdx.x == 0) *d.nonfinite = 1;
+#pragma unroll
+        for (int q = 0; q < PTS; ++q) {
+            const int w = threadIdx.x + q * NT;
+            if (w < RPC * M) sd[spad(w)] = out[q];  // w = m*RPC + r: RPC interleaved sequences
+        }
+        __syncthreads();
+        fft_smem<M, RPC, NT, true>(sd, tw);
+        ROW_TILE_LOOP(RPC, H, NT, {
+            if (l < L) {
+                double2 X, Y;
+                separate_d(sd[spad(k * RPC + r)], sd[spad(((M - k) & (M - 1)) * RPC + r)], X, Y);
+                const long o = rs_index(d, l, k);
+                d.inn[o] = narrow(X);
+                d.inc[o] = narrow(Y);
+            }
+        })
     }
 }
 
@@ -300,16 +341,16 @@ static cudaError_t mrow_forward_impl(const RunDesc *d_runs, int nruns, int L, co
     return cudaGetLastError();
 }
 
-template <int M>
+template <int M, bool STEP>
 static cudaError_t mrow_analysis_impl(const RunDesc *d_runs, int nruns, int L, const TwiddleSet &tw,
                                       cudaStream_t st) {
     constexpr int RPC = MRowCfg<M>::RPC, NT = MRowACfg<M>::NT;
     constexpr size_t smem = dsmem_bytes<3 * RPC * M>();
     static unsigned mask = 0;
-    cudaError_t e = set_smem(k_mrow_analysis<M>, smem, mask);
+    cudaError_t e = set_smem(k_mrow_analysis<M, STEP>, smem, mask);
     if (nruns == 0 || e != cudaSuccess) return e;
     dim3 grid((L + RPC - 1) / RPC, nruns);
-    k_mrow_analysis<M><<<grid, NT, smem, st>>>(d_runs, tw.f64[log2i(M)], tw.logt);
+    k_mrow_analysis<M, STEP><<<grid, NT, smem, st>>>(d_runs, tw.f64[log2i(M)], tw.logt);
     return cudaGetLastError();
 }
 
@@ -318,7 +359,8 @@ cudaError_t launch_mrow_M(int kind, const RunDesc *d_runs, int nruns, int L, con
     switch (kind) {
         case MROW_STEP: return mrow_step_impl<M>(d_runs, nruns, L, tw, s);
         case MROW_FORWARD: return mrow_forward_impl<M>(d_runs, nruns, L, tw, s);
-        case MROW_ANALYSIS: return mrow_analysis_impl<M>(d_runs, nruns, L, tw, s);
+        case MROW_ANALYSIS: return mrow_analysis_impl<M, false>(d_runs, nruns, L, tw, s);
+        case MROW_ANALYSIS_STEP: return mrow_analysis_impl<M, true>(d_runs, nruns, L, tw, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -124,7 +124,7 @@ cudaError_t launch_col_mixed_L(const RunDesc *d_runs, int nruns, int tiles, int 
 cudaError_t launch_col_step_mixed_tiles(const RunDesc *d_runs, int nruns, int L, int tiles, int C, int stage,
                                         int mode, const TwiddleSet &tw, cudaStream_t s);
 // The mixed-precision row kernels of one row length M (instantiated per M in row_inst.cu).
-enum MRowKind : int { MROW_STEP = 0, MROW_FORWARD = 1, MROW_ANALYSIS = 2 };
+enum MRowKind : int { MROW_STEP = 0, MROW_FORWARD = 1, MROW_ANALYSIS = 2, MROW_ANALYSIS_STEP = 3 };
 template <int M>
 cudaError_t launch_mrow_M(int kind, const RunDesc *d_runs, int nruns, int L, const TwiddleSet &tw, cudaStream_t s);
 // The FP32 and mixed-precision kernels behind them.
@@ -143,6 +143,11 @@ cudaError_t launch_row_forward_mixed(const RunDesc *d_runs, int nruns, int L, in
                                      cudaStream_t s);
 cudaError_t launch_row_analysis_mixed(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw,
                                       cudaStream_t s);
+// The analysis followed by the next step's row work (k_mrow_analysis<M, true>): the
+// energy sums of the current state, and inn/inc for the next step, whose row kernel is
+// then not launched.
+cudaError_t launch_row_analysis_step_mixed(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw,
+                                           cudaStream_t s);
 
 // For each of nruns runs: (sum of the analysis row kernel's nparts partial pairs) ->
 // runs[i].ehist[2*slot], [2*slot+1]; the same additions in the same fixed order as the

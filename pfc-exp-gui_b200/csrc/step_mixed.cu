@@ -162,6 +162,10 @@ cudaError_t launch_row_analysis_mixed(const RunDesc *d_runs, int nruns, int L, i
                                       cudaStream_t s) {
     PFC_MROW_SWITCH(M, launch_mrow_M, MROW_ANALYSIS, d_runs, nruns, L, tw, s)
 }
+cudaError_t launch_row_analysis_step_mixed(const RunDesc *d_runs, int nruns, int L, int M, const TwiddleSet &tw,
+                                           cudaStream_t s) {
+    PFC_MROW_SWITCH(M, launch_mrow_M, MROW_ANALYSIS_STEP, d_runs, nruns, L, tw, s)
+}
 cudaError_t launch_col_step_mixed(const RunDesc *d_runs, int nruns, int L, int M, int C, int stage, int mode,
                                   const TwiddleSet &tw, cudaStream_t s) {
     const int tiles = (M / 2 + 1 + C - 1) / C;
@@ -177,6 +181,7 @@ cudaError_t prepare_rows_mixed(int M) {
     cudaError_t e;
     if ((e = launch_row_step_mixed(nullptr, 0, 0, M, none, 0)) != cudaSuccess) return e;
     if ((e = launch_row_forward_mixed(nullptr, 0, 0, M, none, 0)) != cudaSuccess) return e;
+    if ((e = launch_row_analysis_step_mixed(nullptr, 0, 0, M, none, 0)) != cudaSuccess) return e;
     return launch_row_analysis_mixed(nullptr, 0, 0, M, none, 0);
 }
 
