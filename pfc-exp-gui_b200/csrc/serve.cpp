@@ -263,15 +263,21 @@ int build_cohorts(pfc_engine *e) {
 
 // One regular step of a cohort: Misfit row + column sweeps; CVD the same with the
 // energy analysis that ends every CVD step, its sums going to energy slot `slot`.
-int cohort_step(pfc_engine *e, Cohort &c, int slot, cudaStream_t st) {
+// row_done: the step's row work was done by the previous step's analysis; next_row
+// (mixed-precision CVD cohorts): the analysis also does the next step's row work (the
+// same operations as the row kernel, so the same bits).
+int cohort_step(pfc_engine *e, Cohort &c, int slot, cudaStream_t st, bool row_done = false, bool next_row = false) {
     const int n = (int)c.jobs.size();
     const TwiddleSet &tw = e->ctx->tw;
-    PFC_CUDA_TRY(launch_row_step(c.d_descs, n, c.L, c.M, c.prec, tw, st));
+    if (!row_done) PFC_CUDA_TRY(launch_row_step(c.d_descs, n, c.L, c.M, c.prec, tw, st));
     if (c.model == PFC_JOB_MISFIT) {
         PFC_CUDA_TRY(launch_col_step(c.d_descs, n, c.L, c.M, c.CT, c.stage, COL_STEP, c.prec, tw, st));
     } else {
         PFC_CUDA_TRY(launch_col_step(c.d_descs, n, c.L, c.M, c.CT, c.stage, COL_STEP_CHECKPOINT, c.prec, tw, st));
-        PFC_CUDA_TRY(launch_row_analysis(c.d_descs, n, c.L, c.M, c.prec, tw, st));
+        if (next_row)
+            PFC_CUDA_TRY(launch_row_analysis_step_mixed(c.d_descs, n, c.L, c.M, tw, st));
+        else
+            PFC_CUDA_TRY(launch_row_analysis(c.d_descs, n, c.L, c.M, c.prec, tw, st));
         PFC_CUDA_TRY(launch_reduce_runs(c.d_descs, n, analysis_partials(c.L, c.M, c.prec), slot, st));
     }
     return PFC_OK;
@@ -284,8 +290,9 @@ int enqueue_steps(pfc_engine *e, int len) {
     for (size_t i = 0; i < e->cohorts.size(); ++i) {
         Cohort &c = e->cohorts[i];
         PFC_CUDA_TRY(cudaStreamWaitEvent(c.stream, e->fork_event, 0));
+        const bool fuse = c.model == PFC_JOB_CVD && c.prec == PFC_PRECISION_MIXED;
         for (int s = 0; s < len; ++s) {
-            const int rc = cohort_step(e, c, s, c.stream);
+            const int rc = cohort_step(e, c, s, c.stream, fuse && s > 0, fuse && s + 1 < len);
             if (rc != PFC_OK) return rc;
         }
         PFC_CUDA_TRY(cudaEventRecord(e->join_events[i], c.stream));
