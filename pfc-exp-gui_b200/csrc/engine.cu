@@ -391,8 +391,10 @@ static size_t run_state_bytes(int L, int M, int N, int prec, int ct) {
     const size_t real = (size_t)L * M * N * sizeof(float);
     const size_t ktab = (size_t)(L + M + N + 1) * sizeof(float);  // k-vectors + the step counter
     const size_t kdtab = prec == PFC_PRECISION_MIXED ? (size_t)(L + M + N) * sizeof(double) : 0;
-    const int parts_n = !fused ? analysis_partials(L, M, PFC_PRECISION_FP32)
-                               : (d3 ? analysis_partials(L * M, N, prec) : analysis_partials(L, M, prec));
+    // mixed path: one (energy, 0) pair per spectral column follows the analysis partials
+    const int gtiles = prec != PFC_PRECISION_MIXED ? 0 : (d3 ? (N / 2 + 1) * M : M / 2 + 1);
+    const int parts_n = gtiles + (!fused ? analysis_partials(L, M, PFC_PRECISION_FP32)
+                                         : (d3 ? analysis_partials(L * M, N, prec) : analysis_partials(L, M, prec)));
     const size_t parts = (size_t)(2 * parts_n + 4096) * sizeof(double);
     return (fused ? (d3 ? 16 : 8) * rs : 0) + 2 * real + round_up((int)ktab, 256) + round_up((int)kdtab, 256) + parts +
            2 * sizeof(RunDesc) + 1024;
@@ -574,8 +576,13 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
     // device memory: 8 row-space arrays + 2 real fields + k tables + partials + result
     const size_t rs = (size_t)r->rows * r->Hp * sizeof(float2);
     const size_t real = (size_t)r->P * sizeof(float);
-    const int nparts = fused ? analysis_partials(r->rows, r->rowlen, p->precision)
-                             : analysis_partials(r->L, r->M, PFC_PRECISION_FP32);
+    const int nrow = fused ? analysis_partials(r->rows, r->rowlen, p->precision)
+                           : analysis_partials(r->L, r->M, PFC_PRECISION_FP32);
+    // mixed path: the checkpoint column kernel's (energy, 0) pair per spectral column (the
+    // energy's gradient term summed in k-space; km in 2-D, kn*M + km in 3-D, so that the
+    // count and the order do not depend on the tile width) follows the analysis partials
+    const int gtiles = p->precision != PFC_PRECISION_MIXED ? 0 : (d3 ? (p->N / 2 + 1) * p->M : p->M / 2 + 1);
+    const int nparts = nrow + gtiles;
     r->nparts = nparts;
     const size_t ktab = (size_t)(r->L + r->M + r->N + 1) * sizeof(float);
     const size_t kdtab = p->precision == PFC_PRECISION_MIXED ? (size_t)(r->L + r->M + r->N) * sizeof(double) : 0;
@@ -636,6 +643,9 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
         d.kdn = kd + r->L + r->M;
     }
     d.partials = (double *)m;
+    d.gpart_off = nrow;
+    // alpha / (P S^2): S = 1/L (2-D), 1/(L*M) (the 3-D column view)
+    d.gscale = (double)r->k.para_alpha * (d3 ? (double)r->L * (double)r->M / (double)r->N : (double)r->L / (double)r->M);
     r->d_scratch = (double *)m + 2 * nparts;
     m += parts;
     r->d_desc = (RunDesc *)m;
@@ -1183,9 +1193,8 @@ static int fused_advance(pfc_run *r, int nsteps, int analysis, double *red_out =
             PFC_CUDA_TRY(launch_mpass(mpass_args(r, {0, 1, 4, 5}, true), true, r->ctx->tw, r->stream));
             PFC_CUDA_TRY(launch_col_step_mixed_tiles(r->d_desc_col, 1, r->L, dc.T, dc.CT, dc.stage, mode,
                                                      r->ctx->tw, r->stream));
-            PFC_CUDA_TRY(launch_mpass(mode == COL_STEP_CHECKPOINT ? mpass_args(r, {0, 1, 2, 3, 6, 7}, false)
-                                                                  : mpass_args(r, {0, 1, 2, 3}, false),
-                                      false, r->ctx->tw, r->stream));
+            // (the checkpoint mode's gradient term is a k-space sum: no gx, gy to carry back)
+            PFC_CUDA_TRY(launch_mpass(mpass_args(r, {0, 1, 2, 3}, false), false, r->ctx->tw, r->stream));
         } else {
             PFC_CUDA_TRY(launch_col_step(r->d_desc, 1, r->L, r->M, r->desc.CT, r->desc.stage, mode, prec,
                                          r->ctx->tw, r->stream));

@@ -48,18 +48,6 @@ __device__ __forceinline__ double col_k2(const RunDesc &d, int b, int km0, int k
     const double km = d.kdm[km3], kz = kn <= d.N / 2 ? d.kdn[kn] : 0.0;
     return km * km + kz * kz;
 }
-// -i k P along l (which = 0) or m (which = 1), double k-vectors.  A 2-D tile's columns
-// are km = km0 + b (0 past M/2: padding); a 3-D column view's tile has one km (km3, all M
-// values occur, signed through kdm) and its columns are kn.
-struct GradientOfD {
-    const double *kdl, *kdm;
-    int km0, H, which, km3;
-    __device__ __forceinline__ double2 operator()(int e, int b, double2 v) const {
-        const int km = km3 >= 0 ? km3 : (km0 + b <= H ? km0 + b : 0);
-        const double kv = which == 0 ? kdl[e] : kdm[km];
-        return make_double2(kv * v.y, -kv * v.x);
-    }
-};
 // padded shared double2 tile -> FP32 tile in HBM (16-byte stores)
 template <int L, int C, int NT> __device__ __forceinline__ void tile_out_d(const double2 *sm, float2 *__restrict__ g) {
     float4 *g4 = reinterpret_cast<float4 *>(g);
@@ -206,10 +194,44 @@ __global__ void __launch_bounds__(MColCfg<L, C>::NT, MColCfg<L, C>::MINB)
         fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b);
         tile_out_d<L, C, NT>(s, d.con + tile);
         if (MODE == COL_STEP_CHECKPOINT) {
-            fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, GradientOfD{d.kdl, d.kdm, km0, H, 0, km3});
-            tile_out_d<L, C, NT>(s, d.gx + tile);
-            fft<L, C, NT, false, SP_SMEM, SP_SMEM>(Pk, s, s, tw, b, GradientOfD{d.kdl, d.kdm, km0, H, 1, km3});
-            tile_out_d<L, C, NT>(s, d.gy + tile);
+            // The energy's gradient term alpha sum_x (gx^2 + 2 gy^2) of the new c (ENERGYC2
+            // with grao2 twice, MIS:915), as a k-space sum (Parseval): Pk = S C^ (S the
+            // inverse-transform scale), so sum_x gx^2 = sum_k w kl^2 |Pk|^2 / (P S^2) over this
+            // half spectrum, w = 1 on the self-conjugate column (km = 0, M/2 in 2-D; kn = 0,
+            // N/2 in 3-D), 2 on the others.  The reference keeps the real part of the complex
+            // inverse transform of -i k C^, which has no derivative along an axis at that
+            // axis's Nyquist index: kl = 0 at l = L/2, the m wavenumber 0 at M/2.
+            // One partial per spectral column, summed in an order that does not depend on the
+            // tile width: a column's L/16 threads take rows t, t + L/16, ... in turn (thread
+            // t*C + b of column b), and one thread adds their sums in t order.
+            const int b0 = threadIdx.x % C;
+            const int kc0 = km3 >= 0 ? (tile_i / d.M) * C + b0 : km0 + b0;  // the half-spectrum column
+            const int hc = km3 >= 0 ? d.N / 2 : H;
+            const int kmi = km3 >= 0 ? km3 : kc0;                            // its m index
+            const double ky = (kc0 > hc || kmi == d.M / 2) ? 0.0 : d.kdm[kmi];
+            const double ky2 = dmul(2.0, dmul(ky, ky));
+            double g = 0.0;
+            for (int e = threadIdx.x; e < L * C; e += NT) {
+                const int l = e / C;
+                const double kl = l == L / 2 ? 0.0 : kl_of(l, dkl);
+                const double2 v = Pk[spad(e)];
+                g = fma(fma(kl, kl, ky2), fma(v.x, v.x, dmul(v.y, v.y)), g);
+            }
+            double *gs = reinterpret_cast<double *>(s);  // s is free: con' has been stored
+            __syncthreads();
+            gs[threadIdx.x] = g;
+            __syncthreads();
+            if (threadIdx.x < C) {
+                const int kc = km3 >= 0 ? (tile_i / d.M) * C + threadIdx.x : km0 + threadIdx.x;
+                if (kc <= hc) {
+                    double t = 0.0;
+                    for (int i = 0; i < NT / C; ++i) t = dadd(t, gs[i * C + threadIdx.x]);
+                    const double w = (kc == 0 || kc == hc) ? 1.0 : 2.0;
+                    const int col = km3 >= 0 ? kc * d.M + km3 : kc;  // (kn, km) in 3-D, km in 2-D
+                    d.partials[2 * (d.gpart_off + col)] = dmul(dmul(t, w), d.gscale);
+                    d.partials[2 * (d.gpart_off + col) + 1] = 0.0;
+                }
+            }
         }
     }
     st.finish();  // every copy issued has been waited for: the last item issues none

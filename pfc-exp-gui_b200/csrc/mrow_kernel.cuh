@@ -46,9 +46,6 @@ __device__ __forceinline__ CoefsD coefs_d(const ModelCoefs &k) {
 // With every rounding fixed, equal inputs give equal terms: a 3-D state that does not
 // depend on n (the CVD initial condition) stays exactly independent of n, as in the
 // reference, whose row transforms of a constant row are exact.
-__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
-__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
-__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
 // 1 - 3 c^2 + 2 c^3 = 1 + c^2 (2 c - 3), c2 = c^2
 __device__ __forceinline__ double cubic_d(double c, double c2) { return fma(c2, fma(2.0, c, -3.0), 1.0); }
 __device__ __forceinline__ TermsD point_terms_d(const CoefsD &k, double psi, double c, double a, double b,
@@ -183,15 +180,16 @@ __global__ void __launch_bounds__(MRowCfg<M>::NT) k_mrow_forward(const RunDesc *
 
 // ---------------------------------------------------------------------------
 // Analysis row kernel (checkpoints): real fields (rounded once to FP32), and the energy
-// density (ENERGYC2, MIS:1043-1092, every term in double, the grao2-twice gradient of
-// MIS:915) and mass summed in double.
+// density (ENERGYC2, MIS:1043-1092, every term in double) and mass summed in double.  The
+// gradient term (the grao2-twice gradient of MIS:915) is summed in k-space by the
+// checkpoint column kernel; its per-tile partials follow this kernel's.
 // ---------------------------------------------------------------------------
-// the analysis transforms three sequences per row: one radix-16 butterfly per thread
+// the analysis transforms two sequences per row (psi + i con, c2a + i c2b): one radix-16
+// butterfly per thread
 template <int M> struct MRowACfg {
-    static constexpr int NT = (3 * MRowCfg<M>::RPC * M / 16) < 1024 ? (3 * MRowCfg<M>::RPC * M / 16) : 1024;
-    static constexpr int MINB = 768 / NT >= 1 ? 768 / NT : 1;  // 768 threads per SM (85 registers)
-    // the analysis with the next step's row work (STEP): about 112 registers per thread
-    static constexpr int MINB_STEP = 65536 / (NT * 112) >= 1 ? 65536 / (NT * 112) : 1;
+    static constexpr int NT = (2 * MRowCfg<M>::RPC * M / 16) < 1024 ? (2 * MRowCfg<M>::RPC * M / 16) : 1024;
+    static constexpr int MINB = 512 / NT >= 1 ? 512 / NT : 1;  // 128 registers per thread, as the step kernel
+    static constexpr int MINB_STEP = MINB;                      // the analysis with the next step's row work
 };
 // STEP = false: the analysis of the state.  STEP = true: the same analysis (the same
 // arithmetic, so the same sums), and then the next step's row work from the transforms it
@@ -202,7 +200,7 @@ template <int M, bool STEP>
 __global__ void __launch_bounds__(MRowACfg<M>::NT, STEP ? MRowACfg<M>::MINB_STEP : MRowACfg<M>::MINB)
     k_mrow_analysis(const RunDesc *__restrict__ runs, const double2 *__restrict__ tw, const double2 *__restrict__ lt) {
     constexpr int RPC = MRowCfg<M>::RPC, NT = MRowACfg<M>::NT, H = M / 2;
-    constexpr int NB = 3 * RPC;
+    constexpr int NB = 2 * RPC;
     constexpr int PTS = (RPC * M + NT - 1) / NT;
     extern __shared__ double2 sd[];
     __shared__ double red[2][32];
@@ -211,19 +209,16 @@ __global__ void __launch_bounds__(MRowACfg<M>::NT, STEP ? MRowACfg<M>::MINB_STEP
     const int l0 = blockIdx.x * RPC;
     if (STEP && d.noise_amp != 0.0f && blockIdx.x == 0 && threadIdx.x == 0) *d.step_ctr += 1;
     ROW_TILE_LOOP(RPC, H, NT, {
-        float2 z[6] = {};
+        float2 z[4] = {};
         if (l < L) {
             const long o = rs_index(d, l, k);
             z[0] = d.psi[o];
             z[1] = d.con[o];
             z[2] = d.ca[o];
             z[3] = d.cb[o];
-            z[4] = d.gx[o];
-            z[5] = d.gy[o];
         }
-        build_pair_d(sd, NB, 3 * r, k, M, wide(z[0]), wide(z[1]));
-        build_pair_d(sd, NB, 3 * r + 1, k, M, wide(z[2]), wide(z[3]));
-        build_pair_d(sd, NB, 3 * r + 2, k, M, wide(z[4]), wide(z[5]));
+        build_pair_d(sd, NB, 2 * r, k, M, wide(z[0]), wide(z[1]));
+        build_pair_d(sd, NB, 2 * r + 1, k, M, wide(z[2]), wide(z[3]));
     })
     __syncthreads();
     fft_smem<M, NB, NT, false>(sd, tw);
@@ -239,12 +234,11 @@ __global__ void __launch_bounds__(MRowACfg<M>::NT, STEP ? MRowACfg<M>::MINB_STEP
         if (w >= RPC * M) continue;
         const int r = w % RPC, m = w / RPC, l = l0 + r;
         if (l >= L) continue;
-        const double2 z1 = sd[spad(m * NB + 3 * r)], z2 = sd[spad(m * NB + 3 * r + 1)],
-                      z3 = sd[spad(m * NB + 3 * r + 2)];
+        const double2 z1 = sd[spad(m * NB + 2 * r)], z2 = sd[spad(m * NB + 2 * r + 1)];
         // explicit roundings, as in point_terms_d: equal inputs give equal outputs
         const double dpsi = dmul(z1.x, invM);
         const double psi = dadd(dpsi, d.psi_mean), c = fma(z1.y, invM, d.con_mean);
-        const double a = dmul(z2.x, invM), b = dmul(z2.y, invM), gx = dmul(z3.x, invM), gy = dmul(z3.y, invM);
+        const double a = dmul(z2.x, invM), b = dmul(z2.y, invM);
         d.psi_real[(size_t)l * M + m] = (float)psi;
         d.con_real[(size_t)l * M + m] = (float)c;
         const double psi2 = dmul(psi, psi);
@@ -254,8 +248,9 @@ __global__ void __launch_bounds__(MRowACfg<M>::NT, STEP ? MRowACfg<M>::MINB_STEP
         const double e_mix = dmul(dmul(dadd(psi, 1.0), kc.w), fma(c, lc, dmul(omc, l1c)));
         const double c2 = dmul(c, c), omc2 = dmul(omc, omc);
         const double in3 = -fma(cubic_d(c, c2), a, dmul(cubic_d(omc, omc2), b));
-        const double grad2 = fma(gx, gx, dmul(2.0, dmul(gy, gy)));  // gx^2 + gy^2 + gy^2
-        const double e_ex = fma(dmul(0.5, psi), in3, dmul(kc.alpha, grad2));
+        // the gradient term alpha (gx^2 + 2 gy^2) is summed in k-space by the checkpoint
+        // column kernel (its per-tile partials follow this kernel's in d.partials)
+        const double e_ex = dmul(dmul(0.5, psi), in3);
         acc_e += dadd(dadd(e_id, e_mix), e_ex);
         acc_m += dpsi;
         if constexpr (STEP) {
@@ -345,7 +340,7 @@ template <int M, bool STEP>
 static cudaError_t mrow_analysis_impl(const RunDesc *d_runs, int nruns, int L, const TwiddleSet &tw,
                                       cudaStream_t st) {
     constexpr int RPC = MRowCfg<M>::RPC, NT = MRowACfg<M>::NT;
-    constexpr size_t smem = dsmem_bytes<3 * RPC * M>();
+    constexpr size_t smem = dsmem_bytes<2 * RPC * M>();
     static unsigned mask = 0;
     cudaError_t e = set_smem(k_mrow_analysis<M, STEP>, smem, mask);
     if (nruns == 0 || e != cudaSuccess) return e;

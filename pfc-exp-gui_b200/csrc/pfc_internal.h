@@ -75,8 +75,14 @@ struct RunDesc {
     // set to 1 (device-visible, mapped pinned host memory) by a row-step kernel that met a
     // non-finite nonlinear term (NaN / Inf in the run's fields); the engine fails the run
     int *nonfinite;
-    // per-CTA partial sums written by the analysis row kernel: [2 * L] doubles
+    // per-CTA partial sums written by the analysis row kernel: [2 * L] doubles; on the
+    // mixed path followed, from pair gpart_off on, by one (energy, 0) pair per spectral
+    // column (km in 2-D, kn*M + km in 3-D) that the checkpoint column kernel writes: the
+    // gradient term of the energy summed in k-space, times gscale = alpha / (P S^2) (S the
+    // column view's inverse-transform scale)
     double *partials;
+    int gpart_off;
+    double gscale;
     // batched runs only: slots of (energy sum, mass sum) that launch_reduce_runs fills
     double *ehist;
     // stochastic noise (axx > 0): amplitude dt * b0 (0 = off), stream key, and the

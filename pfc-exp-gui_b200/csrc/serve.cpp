@@ -278,7 +278,7 @@ int cohort_step(pfc_engine *e, Cohort &c, int slot, cudaStream_t st, bool row_do
             PFC_CUDA_TRY(launch_row_analysis_step_mixed(c.d_descs, n, c.L, c.M, tw, st));
         else
             PFC_CUDA_TRY(launch_row_analysis(c.d_descs, n, c.L, c.M, c.prec, tw, st));
-        PFC_CUDA_TRY(launch_reduce_runs(c.d_descs, n, analysis_partials(c.L, c.M, c.prec), slot, st));
+        PFC_CUDA_TRY(launch_reduce_runs(c.d_descs, n, c.jobs[0]->run->nparts, slot, st));  // the runs' shared count
     }
     return PFC_OK;
 }

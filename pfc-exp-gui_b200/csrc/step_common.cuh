@@ -44,6 +44,13 @@ __device__ __forceinline__ float c2_ref(const C2Params &p, float ks) {
     return (float)(exp(-(double)p.q2 * (double)p.q2) * exp(-(d * d) / (double)p.gg2));
 }
 
+// Double products and sums that the compiler never fuses into an fma or splits (the mixed
+// path writes its pointwise arithmetic with these and explicit fma(), so that equal inputs
+// round equally in every kernel and every inlined copy).
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+
 // Natural logarithm in double for the mixed path's pointwise terms, by the table-driven
 // method of P. T. P. Tang (ACM TOMS 16(4):378-400, 1990): x = 2^e m with m in [1, 2),
 // F = 1 + j/128 the breakpoint nearest m (j = 0 .. 128), and
