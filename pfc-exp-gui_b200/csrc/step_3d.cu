@@ -7,7 +7,8 @@
 //   this kernel, forward: psi, con, inn, inc transformed along m, layout A -> B;
 //   the mixed column kernel on the (n-tile, km) tiles of layout B: transforms along l and
 //     the semi-implicit update with k^2 = kl^2 + km^2 + kn^2 (the 3-D table);
-//   this kernel, inverse: psi', con', c2a, c2b (and the gradients at checkpoints), B -> A.
+//   this kernel, inverse: psi', con', c2a, c2b, B -> A (at checkpoints too: the column
+//     kernel sums the energy's gradient term in k-space).
 // Layouts (pfc_internal.h, MPassArgs): A puts each (t, l) M x CT tile in one block, B each
 // (t, km) L x CT tile.  A work item is one (array, t, l): the A block is copied (or the B
 // chunks of CT values gathered) by cp.async into an FP32 staging buffer, transformed along

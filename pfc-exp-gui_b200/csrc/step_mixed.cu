@@ -9,7 +9,8 @@
 //     forward row FFT of inn+i*inc;
 //   column kernel: forward column FFTs of psi, inn, con, inc; the semi-implicit update
 //     MAINEQUATIONC2_NOI / C2MIX (MIS:983-1014, CVD:865-886); inverse column FFTs of
-//     psi', C2A psi', C2B psi', con' (and the -i k gradients of con' at checkpoints).
+//     psi', C2A psi', C2B psi', con'; at checkpoints also the energy's gradient term of
+//     con' as a k-space sum (one partial per spectral column).
 //
 // Every value is widened to double when it is loaded and rounded to float once, when it
 // is stored: the transforms, the pointwise terms and the update run in FP64, and the
