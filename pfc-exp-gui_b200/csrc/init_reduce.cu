@@ -128,7 +128,23 @@ __device__ __forceinline__ void tree_sums(const double *__restrict__ partials, i
                                           double *__restrict__ out) {
     __shared__ double red[2][REDUCE_NT / 32];
     double acc[2] = {0.0, 0.0};
-    for (int i = threadIdx.x; i < count; i += REDUCE_NT)
+    // a thread adds partials tid, tid + NT, tid + 2 NT, ... in that order; eight of them are
+    // loaded ahead of their additions, so that the loads overlap
+    constexpr int U = 8;
+    int i = threadIdx.x;
+    for (; i + (U - 1) * REDUCE_NT < count; i += U * REDUCE_NT) {
+        double v[U][2];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) v[u][j] = j < width ? partials[(long)(i + u * REDUCE_NT) * stride + j] : 0.0;
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+                if (j < width) acc[j] += v[u][j];
+    }
+    for (; i < count; i += REDUCE_NT)
 #pragma unroll
         for (int j = 0; j < 2; ++j)
             if (j < width) acc[j] += partials[(long)i * stride + j];
