@@ -396,8 +396,11 @@ static size_t run_state_bytes(int L, int M, int N, int prec, int ct) {
     const int parts_n = gtiles + (!fused ? analysis_partials(L, M, PFC_PRECISION_FP32)
                                          : (d3 ? analysis_partials(L * M, N, prec) : analysis_partials(L, M, prec)));
     const size_t parts = (size_t)(2 * parts_n + 4096) * sizeof(double);
-    return (fused ? (d3 ? 16 : 8) * rs : 0) + 2 * real + round_up((int)ktab, 256) + round_up((int)kdtab, 256) + parts +
-           2 * sizeof(RunDesc) + 1024;
+    // row-space arrays: psi, con, ca, cb, inn, inc, and gx, gy on the FP32 path only (the
+    // mixed path sums the energy's gradient term in k-space)
+    const int narr = prec == PFC_PRECISION_MIXED ? 6 : 8;
+    return (fused ? (d3 ? 2 * narr : narr) * rs : 0) + 2 * real + round_up((int)ktab, 256) + round_up((int)kdtab, 256) +
+           parts + 2 * sizeof(RunDesc) + 1024;
 }
 
 // Column tile width of a 3-D mixed run: the widest up to the 2-D default whose column
@@ -600,14 +603,17 @@ static int run_create(const pfc_run_params *p, int ct_force, int stage_force, pf
     RunDesc &dc = r->desc_col;
     std::memset(&dc, 0, sizeof(dc));
     if (fused) {
+        // gx, gy (the last two) on the FP32 path only, as in run_state_bytes; the mixed
+        // path's stay null
+        const int narr = p->precision == PFC_PRECISION_MIXED ? 6 : 8;
         float2 **arrs[8] = {&d.psi, &d.con, &d.ca, &d.cb, &d.inn, &d.inc, &d.gx, &d.gy};
-        for (int i = 0; i < 8; ++i) {
+        for (int i = 0; i < narr; ++i) {
             *arrs[i] = (float2 *)m;
             m += rs;
         }
         if (d3) {  // the layout-B arrays of the column view
             float2 **b[8] = {&dc.psi, &dc.con, &dc.ca, &dc.cb, &dc.inn, &dc.inc, &dc.gx, &dc.gy};
-            for (int i = 0; i < 8; ++i) {
+            for (int i = 0; i < narr; ++i) {
                 *b[i] = (float2 *)m;
                 m += rs;
             }
@@ -1093,12 +1099,12 @@ static int init_real_fields(pfc_run *r) {
 }
 
 // m-pass arguments of a 3-D run for the arrays `which` (0 psi, 1 con, 2 c2a, 3 c2b, 4 inn,
-// 5 inc, 6 gx, 7 gy): forward reads layout A (the row view's arrays) and writes layout B
-// (the column view's), inverse the other way.
+// 5 inc): forward reads layout A (the row view's arrays) and writes layout B (the column
+// view's), inverse the other way.
 static MPassArgs mpass_args(const pfc_run *r, std::initializer_list<int> which, bool forward) {
     const RunDesc &a = r->desc, &b = r->desc_col;
-    float2 *A[8] = {a.psi, a.con, a.ca, a.cb, a.inn, a.inc, a.gx, a.gy};
-    float2 *B[8] = {b.psi, b.con, b.ca, b.cb, b.inn, b.inc, b.gx, b.gy};
+    float2 *A[6] = {a.psi, a.con, a.ca, a.cb, a.inn, a.inc};
+    float2 *B[6] = {b.psi, b.con, b.ca, b.cb, b.inn, b.inc};
     MPassArgs m{};
     for (int w : which) {
         m.src[m.narr] = forward ? A[w] : B[w];
