@@ -43,8 +43,10 @@ extern "C" {
 #define PFC_PRECISION_FP64 1 /* plain FP64 path with the reference's float roundings */
 #define PFC_PRECISION_FP64_PURE 2 /* plain FP64 path, every intermediate in double */
 #define PFC_PRECISION_MIXED 3 /* fused path: the FP32 path's FP32 complex arrays in HBM, FP64
-                                 arithmetic and the pure-FP64 operator in the kernels (within
-                                 1e-5 of pure FP64 after 200 steps); the default */
+                                 arithmetic and the pure-FP64 operator in the kernels (Misfit
+                                 within 1e-5 of pure FP64 after 200 steps; CVD amplifies the FP32
+                                 storage roundings, and PFC_PRECISION_FP64 follows the reference's
+                                 own trajectory); the default */
 
 /* Parameters of one run.  Field meanings and defaults follow the reference CLI
  * (misfit_uniform_time_seed_fftw_early.cpp:17-35, 125-143; cvd.cpp:111-125, 33-53). */
