@@ -9,8 +9,9 @@ formulas as the kernels (csrc/mrow_kernel.cuh: ROW_TILE_LOOP, build_pair_d, the 
 pointwise and forward stores; csrc/step_3d.cu: k_mpass; csrc/mcol_kernel.cuh:
 k_mcol_step's items, tiles, table planes and k-vector reads), and checked: every index
 inside the buffer it addresses, the row walk visiting each (row, kn <= N/2) once, the
-m-axis passes mapping layout A onto layout B one to one, and the shared buffers inside
-the CTA's dynamic shared memory.  The grid shapes include the three on which an earlier,
+m-axis passes mapping layout A onto layout B one to one, the shared buffers inside
+the CTA's dynamic shared memory, and the checkpoint column kernel's gradient partials
+covering each spectral column once, from rows that do not depend on the tile width.  The grid shapes include the three on which an earlier,
 since removed, 3-D build faulted at run creation.
 """
 import numpy as np
@@ -155,3 +156,61 @@ def test_column_kernel_items_stay_inside_layout_b_and_tables(L, M, N):
     assert q_off % 16 == 0 and t_off % 16 == 0 and (8 * L * ct) % 16 == 0
     # table planes: 4 planes of T3*L*CT doubles, 16-byte aligned tile starts
     assert (tiles * L * ct * 8 % 16 == 0).all()
+
+
+def column_partials(L, M, N, ct, three_d):
+    """The checkpoint column kernel's gradient partials (csrc/mcol_kernel.cuh, COL_STEP_CHECKPOINT):
+    for each tile, thread b < C writes partial pair gpart_off + col for its column kc when
+    kc <= hc; col = kc*M + km3 in the 3-D column view (tile t*M + km3, kc = t*CT + b, hc = N/2),
+    col = kc in 2-D (tile t, kc = t*CT + b, hc = M/2).  Returns the written cols, and the
+    per-thread sum's rows for every column (thread t_c*C + b takes rows t_c + j*L/16)."""
+    nt = ct * L // 16
+    if three_d:
+        hp = -(-(N // 2 + 1) // ct) * ct
+        tiles = (hp // ct) * M
+        hc = N // 2
+    else:
+        hp = -(-(M // 2 + 1) // ct) * ct
+        tiles = hp // ct
+        hc = M // 2
+    cols = []
+    for tile in range(tiles):
+        for b in range(ct):
+            if three_d:
+                kc, km3 = (tile // M) * ct + b, tile % M
+                if kc <= hc:
+                    cols.append(kc * M + km3)
+            else:
+                kc = tile * ct + b
+                if kc <= hc:
+                    cols.append(kc)
+    rows = {}
+    for tid in range(nt):
+        b, tc = tid % ct, tid // ct
+        rows[(b, tc)] = [(tid + j * nt) // ct for j in range((L * ct) // nt)]
+        assert all((tid + j * nt) % ct == b for j in range((L * ct) // nt))
+    return np.array(cols), rows, nt
+
+
+@pytest.mark.parametrize("L,M,N", SHAPES)
+def test_gradient_partials_cover_each_spectral_column_once_3d(L, M, N):
+    ct, hp, tn, E = geometry(L, M, N)
+    cols, rows, nt = column_partials(L, M, N, ct, True)
+    gcols = (N // 2 + 1) * M  # engine.cu: the pairs allotted after the analysis partials
+    assert len(cols) == gcols and np.array_equal(np.sort(cols), np.arange(gcols))
+    # a column's threads take the same rows whatever the tile width: t_c + j*L/16
+    for (b, tc), rr in rows.items():
+        assert rr == [tc + j * (L // 16) for j in range(16)]
+
+
+@pytest.mark.parametrize("L,M", [(64, 64), (256, 256), (1024, 1024), (32, 256), (2048, 64)])
+def test_gradient_partials_do_not_depend_on_tile_width_2d(L, M):
+    gcols = M // 2 + 1
+    widths = [c for c in (1, 2, 4, 8, 16) if mcol_tile_ok(L, c)]
+    assert widths
+    for ct in widths:
+        cols, rows, nt = column_partials(L, M, 1, ct, False)
+        assert nt == ct * L // 16 and nt % ct == 0
+        assert len(cols) == gcols and np.array_equal(np.sort(cols), np.arange(gcols))
+        for (b, tc), rr in rows.items():
+            assert rr == [tc + j * (L // 16) for j in range(16)]
