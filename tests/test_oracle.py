@@ -192,3 +192,21 @@ def test_oracle_cvd_checkpoint_analysis(name):
         else:
             assert not os.path.exists(os.path.join(d, f"Ql_{kd}.txt"))
     assert phimax_txt == text(os.path.join(d, "phimax.txt"))
+
+
+def test_cvd_3d_state_stays_independent_of_n():
+    """The CVD initial condition (INITIAL_C2, cvd.cpp:587-642) does not depend on n, and the
+    reference keeps it so exactly: its own 32 x 32 x 8 run's checkpoints, and the oracle in
+    both modes over 60 steps, have no spread along n at all.  (A constant row transforms to
+    one bin and back without rounding, and equal points give equal terms; the GPU path's
+    tests hold it to the same.)"""
+    _, _, fields = golden_case("cvd_32x32x8")
+    for key, v in fields.items():
+        a = v.reshape(32, 32, 8)
+        assert (a.max(axis=2) - a.min(axis=2)).max() == 0.0, key
+    for exact in (1, 0):
+        o = O.Run(O.default_params(O.MODEL_CVD, L=32, M=32, N=8, exact=exact))
+        o.step(60)
+        for a in o.fields():
+            a = a.reshape(32, 32, 8)
+            assert (a.max(axis=2) - a.min(axis=2)).max() == 0.0, exact
